@@ -1,0 +1,152 @@
+// Context: device, stream, device-memory arena, twiddle tables and the
+// host-side stop/deadline poll shared by every entry point.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/spk_b200.h"
+#include "common.cuh"
+
+struct spk_context {
+    int device {};
+    std::uint64_t cap_bytes {};
+    cudaStream_t stream {};
+    std::atomic<std::uint64_t> launches { 0 };
+    std::uint64_t bytes_in_use {};
+    struct Buffer {
+        void* ptr {};
+        std::size_t bytes {};
+    };
+    std::map<std::string, Buffer> device_buffers;
+    std::map<std::string, Buffer> host_buffers;  // pinned staging
+    std::map<std::pair<int, int>, void*> twiddles;  // (sizeof scalar, L) -> table
+    void* session {};                              // placement session (engine.cpp)
+};
+
+namespace spk {
+
+// Grows (never shrinks) a named device buffer; returns nullptr on failure.
+inline void* device_buffer(spk_context* ctx, const std::string& name, std::size_t bytes, int& status)
+{
+    auto& b = ctx->device_buffers[name];
+    if (b.bytes >= bytes && b.ptr) {
+        return b.ptr;
+    }
+    const std::uint64_t next = ctx->bytes_in_use - b.bytes + bytes;
+    if (ctx->cap_bytes && next > ctx->cap_bytes) {
+        status = kMemoryLimit;
+        return nullptr;
+    }
+    if (b.ptr) {
+        cudaFree(b.ptr);
+        ctx->bytes_in_use -= b.bytes;
+        b = {};
+    }
+    void* p {};
+    if (cudaMalloc(&p, bytes ? bytes : 1) != cudaSuccess) {
+        cudaGetLastError();
+        status = kAllocation;
+        return nullptr;
+    }
+    b.ptr = p;
+    b.bytes = bytes;
+    ctx->bytes_in_use += bytes;
+    return p;
+}
+
+inline void* host_buffer(spk_context* ctx, const std::string& name, std::size_t bytes, int& status)
+{
+    auto& b = ctx->host_buffers[name];
+    if (b.bytes >= bytes && b.ptr) {
+        return b.ptr;
+    }
+    if (b.ptr) {
+        cudaFreeHost(b.ptr);
+        b = {};
+    }
+    void* p {};
+    if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+        cudaGetLastError();
+        status = kAllocation;
+        return nullptr;
+    }
+    b.ptr = p;
+    b.bytes = bytes;
+    return p;
+}
+
+// exp(-2 pi i m / L) for m < L, FP64-computed, stored as T.
+template <typename T>
+const cplx_t<T>* twiddle_table(spk_context* ctx, int L, int& status)
+{
+    const auto key = std::make_pair(static_cast<int>(sizeof(T)), L);
+    auto it = ctx->twiddles.find(key);
+    if (it != ctx->twiddles.end()) {
+        return static_cast<const cplx_t<T>*>(it->second);
+    }
+    std::vector<cplx_t<T>> host(L);
+    const double pi = 3.14159265358979323846264338327950288;
+    for (int m = 0; m < L; ++m) {
+        // Exact values at the quarter points keep the table symmetric.
+        double c, s;
+        if (4 * m % L == 0) {
+            const int quadrant = 4 * m / L;
+            c = quadrant == 0 ? 1.0 : quadrant == 2 ? -1.0 : 0.0;
+            s = quadrant == 1 ? -1.0 : quadrant == 3 ? 1.0 : 0.0;
+        }
+        else {
+            const double angle = -2.0 * pi * static_cast<double>(m) / static_cast<double>(L);
+            c = std::cos(angle);
+            s = std::sin(angle);
+        }
+        host[m].x = static_cast<T>(c);
+        host[m].y = static_cast<T>(s);
+    }
+    void* p {};
+    if (cudaMalloc(&p, sizeof(cplx_t<T>) * L) != cudaSuccess) {
+        cudaGetLastError();
+        status = kAllocation;
+        return nullptr;
+    }
+    cudaMemcpy(p, host.data(), sizeof(cplx_t<T>) * L, cudaMemcpyHostToDevice);
+    ctx->twiddles[key] = p;
+    return static_cast<const cplx_t<T>*>(p);
+}
+
+std::int64_t monotonic_ns();
+
+// The reference polls stop first, then the deadline (operation_control.hpp:33-42).
+inline int poll(const spk_control* control)
+{
+    if (!control) {
+        return kOk;
+    }
+    if (control->stop_word && *control->stop_word) {
+        return kCancelled;
+    }
+    if (control->deadline_ns && monotonic_ns() >= control->deadline_ns) {
+        return kDeadline;
+    }
+    return kOk;
+}
+
+inline std::uint32_t next_pow2(std::uint64_t v)
+{
+    std::uint32_t p = 1;
+    while (p < v) {
+        p <<= 1;
+    }
+    return p;
+}
+
+}  // namespace spk

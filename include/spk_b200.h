@@ -1,0 +1,126 @@
+/*
+ * spk_b200.h - C ABI of the B200 spectral placement path.
+ *
+ * Plain pointers and sizes only.  Every entry point is noexcept, returns an
+ * int status (0 = ok) and reports failures as values; spk_status_code() maps
+ * a status to the reference's static string code (ADR 0015 convention,
+ * reference engine/pack_compute/include/spectrapack/compute/correlation.hpp:52-56).
+ * Buffers passed in are borrowed for the call; outputs go to caller buffers;
+ * device memory is owned by the context.  One host thread drives a context at
+ * a time (the reference's "one coordinator serialises calls" rule,
+ * correlation.hpp:78-79).
+ *
+ * Storage order everywhere is X-fastest: cell (x, y, z) of a field with shape
+ * (sx, sy, sz) lives at x + sx * (y + sy * z)  (correlation.hpp:20-21).
+ */
+#ifndef SPK_B200_H
+#define SPK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spk_context spk_context;
+
+/* Arithmetic used by the FFT correlation. */
+enum { SPK_FP32 = 0, SPK_FP64 = 1 };
+
+/* Reference: compute::CorrelationSpec, correlation.hpp:22-27. */
+typedef struct spk_correlation_spec {
+    uint32_t environment_shape[3];
+    uint32_t kernel_shape[3];
+    int64_t environment_first[3];
+    int64_t kernel_first[3];
+} spk_correlation_spec;
+
+/* Reference: compute::CorrelationLimits, correlation.hpp:29-36 (device bytes). */
+typedef struct spk_correlation_limits {
+    uint64_t max_working_bytes;
+    uint64_t reserved_bytes;
+    uint64_t max_padded_cells;
+    uint64_t max_direct_terms;
+} spk_correlation_limits;
+
+/* Reference: CorrelationResult metadata + NumericReport + CorrelationStats,
+ * correlation.hpp:38-72.  `padded_shape` is the FFT grid actually used. */
+typedef struct spk_correlation_result {
+    int64_t translation_first[3];
+    uint32_t shape[3];
+    double max_integer_residual;
+    double mass_residual;
+    double max_probe_error;
+    uint64_t padded_cells;
+    uint64_t working_bytes_peak;
+    uint64_t direct_terms;
+    uint32_t padded_shape[3];
+} spk_correlation_result;
+
+/* Reference: CorrelationEstimate, correlation.hpp:100-104. */
+typedef struct spk_correlation_estimate {
+    uint32_t padded_shape[3];
+    uint64_t padded_cells;
+    uint64_t working_bytes;
+} spk_correlation_estimate;
+
+/* Reference: runtime::OperationControl stop token and deadline
+ * (engine/common/include/spectrapack/runtime/operation_control.hpp:18-45).
+ * A nonzero *stop_word means user stop; deadline_ns is CLOCK_MONOTONIC
+ * nanoseconds, 0 for none.  Both are polled between device phases. */
+typedef struct spk_control {
+    const volatile uint32_t* stop_word;
+    int64_t deadline_ns;
+} spk_control;
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Opens a context on `device` with a device-memory cap (0 = no cap). */
+int spk_context_create(int device, uint64_t max_device_bytes, spk_context** out);
+void spk_context_destroy(spk_context* context);
+/* Static string for a status (e.g. "CORRELATION_NUMERIC"); never NULL. */
+const char* spk_status_code(int status);
+/* Number of kernels this library launched on the context (all entry points). */
+uint64_t spk_context_launches(const spk_context* context);
+
+/* ---- full-range correlation drop-in ----------------------------------- */
+
+/* Replaces compute::estimate_correlation_cpu (correlation.hpp:100-106,
+ * correlation.cpp:596-641) for the GPU path: FFT grid and device bytes. */
+int spk_estimate_correlation(const spk_correlation_spec* spec, uint32_t precision,
+                             spk_correlation_estimate* out);
+
+/* Replaces compute::correlate_binary_cpu (correlation.hpp:108-111,
+ * correlation.cpp:238-592,643-648).  Output: (E+K-1) per axis doubles,
+ * X-fastest, rounded to integers, with the reference's residual (<0.25),
+ * range, mass and 8-probe direct checks.  Host pointers. */
+int spk_correlate_binary(spk_context* context, const spk_correlation_spec* spec,
+                         const uint8_t* environment, const uint8_t* kernel,
+                         const spk_correlation_limits* limits, const spk_control* control,
+                         uint32_t precision, double* out_values, uint64_t out_capacity,
+                         spk_correlation_result* result);
+
+/* Replaces compute::correlate_proximity_cpu (correlation.hpp:113-117,
+ * correlation.cpp:650-655): f64 environment in [0,1], binary kernel. */
+int spk_correlate_proximity(spk_context* context, const spk_correlation_spec* spec,
+                            const double* environment, const uint8_t* kernel,
+                            const spk_correlation_limits* limits, const spk_control* control,
+                            uint32_t precision, double* out_values, uint64_t out_capacity,
+                            spk_correlation_result* result);
+
+/* ---- fields ------------------------------------------------------------ */
+
+/* Replaces solver::detail::build_proximity
+ * (engine/pack_solver/src/field_proximity.hpp:32-132): exact squared EDT to
+ * the nearest occupied cell, then exp(-sqrt(d2)/2), 0 where no cell is
+ * occupied.  Host pointers; returns kProximityShape (21) for shapes the
+ * reference rejects (field_proximity.hpp:13-27). */
+int spk_build_proximity(spk_context* context, const uint32_t shape[3], const uint8_t* occupied,
+                        double* values);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPK_B200_H */
