@@ -93,7 +93,7 @@ __device__ C* fft_lines_smem(C* a, C* b, const C* __restrict__ tw, int L, int li
 // axes 1 and 2, consecutive lines for axis 0) so global accesses coalesce.
 template <typename T>
 __global__ void fft_axis_kernel(cplx_t<T>* __restrict__ data, int Lx, int Ly, int Lz, int axis, int inverse,
-                                T scale, const cplx_t<T>* __restrict__ twiddles, int group)
+                                T scale, const cplx_t<T>* __restrict__ twiddles, int group, int store_limit)
 {
     using C = cplx_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -147,7 +147,7 @@ __global__ void fft_axis_kernel(cplx_t<T>* __restrict__ data, int Lx, int Ly, in
         }
     }
     else {
-        for (int e = threadIdx.x; e < group * L; e += blockDim.x) {
+        for (int e = threadIdx.x; e < group * store_limit; e += blockDim.x) {
             const int j = e % group;
             const int q = e / group;
             data[base + j + q * stride] = cscale(result[j * pitch + q], scale);
@@ -156,9 +156,10 @@ __global__ void fft_axis_kernel(cplx_t<T>* __restrict__ data, int Lx, int Ly, in
 }
 
 // Host-side launcher for one axis pass; returns the CUDA launch status.
+// store_limit (axes 1 and 2 only): positions q >= store_limit are not written back.
 template <typename T>
 cudaError_t fft_axis(cplx_t<T>* data, int Lx, int Ly, int Lz, int axis, bool inverse, T scale,
-                     const cplx_t<T>* twiddles, cudaStream_t stream)
+                     const cplx_t<T>* twiddles, cudaStream_t stream, int store_limit = -1)
 {
     using C = cplx_t<T>;
     const int L = axis == 0 ? Lx : axis == 1 ? Ly : Lz;
@@ -171,11 +172,16 @@ cudaError_t fft_axis(cplx_t<T>* data, int Lx, int Ly, int Lz, int axis, bool inv
         group >>= 1;
     }
     const size_t smem = sizeof(C) * (L + 2 * static_cast<size_t>(group) * (L + 1));
+    static bool attribute_set = false;
+    if (!attribute_set) {
+        cudaFuncSetAttribute(fft_axis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attribute_set = true;
+    }
     const int threads = 256;
     const long long blocks = lines / group;
     fft_axis_kernel<T><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(data, Lx, Ly, Lz, axis,
                                                                                   inverse ? 1 : 0, scale, twiddles,
-                                                                                  group);
+                                                                                  group, store_limit < 0 ? L : store_limit);
     return cudaGetLastError();
 }
 

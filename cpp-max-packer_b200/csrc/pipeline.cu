@@ -1,0 +1,970 @@
+// Spectral page pipeline kernels and host orchestration (see pipeline.hpp).
+//
+// Per environment (once per layout): Z = B + iP on an L^3 grid (B the u8
+// occupancy, P the FP32 proximity) and its forward FFT, scaled by 1/N.
+// Per oriented kernel (once per run): the kernel transformed along x and y,
+// kept for its K2 nonzero z-planes ("partial spectrum").
+// Per page request:
+//   pass A  - per (kx, ky) column: finish the kernel FFT along z, multiply by
+//             the conjugate into the environment spectrum, inverse FFT along
+//             z, keep the legal z outputs;
+//   pass B1 - inverse FFT along y, keep the legal y rows;
+//   pass B2 - inverse FFT along x, then the fused epilogue: real part = overlap
+//             count, imaginary part = proximity sum; threshold |b| < 0.5,
+//             approximate score, per-warp sorted top-32 of 64-bit keys
+//             (orderable score, legal linear index z-major) and a per-request
+//             pruning bound;
+//   merge   - per request, sort the surviving keys;
+//   exact   - per selected key, exact u8 overlap recount and the exact,
+//             correctly rounded FP64 proximity sum (superaccumulator).
+// The host then scores exactly, orders by (score, z, y, x), applies the
+// cursor and certifies that no excluded candidate could enter the page; an
+// uncertified page is recomputed in threshold mode (every candidate whose
+// approximate score is within the error bound of the page's last entry).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <tuple>
+#include <vector>
+
+#include "context.hpp"
+#include "edt.cuh"
+#include "fft.cuh"
+#include "pipeline.hpp"
+#include "superacc.cuh"
+
+namespace spk {
+
+namespace {
+
+constexpr std::int32_t kInf = INT32_MAX;
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kB2Rows = 8;
+constexpr int kColumnGroup = 16;
+
+int launch_blocks(long long n, int threads)
+{
+    const long long want = (n + threads - 1) / threads;
+    return static_cast<int>(std::min<long long>(std::max<long long>(want, 1), 148LL * 32));
+}
+
+__global__ void env_pack_kernel(float2* __restrict__ z, int L0, int L1, int L2, int E0, int E1, int E2,
+                                const std::uint8_t* __restrict__ occ, const std::int32_t* __restrict__ d2,
+                                const double* __restrict__ table, double* __restrict__ norm_partial)
+{
+    __shared__ double s[256];
+    const long long n = static_cast<long long>(L0) * L1 * L2;
+    double acc = 0;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % L0);
+        const long long r = i / L0;
+        const int y = static_cast<int>(r % L1);
+        const int w = static_cast<int>(r / L1);
+        float b = 0.f, p = 0.f;
+        if (x < E0 && y < E1 && w < E2) {
+            const long long e = x + static_cast<long long>(E0) * (y + static_cast<long long>(E1) * w);
+            b = occ[e] ? 1.f : 0.f;
+            const std::int32_t v = d2[e];
+            p = v == kInf ? 0.f : static_cast<float>(table[v]);
+        }
+        acc += static_cast<double>(b) * b + static_cast<double>(p) * p;
+        z[i] = make_float2(b, p);
+    }
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            s[threadIdx.x] += s[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        norm_partial[blockIdx.x] = s[0];
+    }
+}
+
+__global__ void kernel_pack_kernel(float2* __restrict__ kp, int L0, int L1, int K0, int K1, int K2,
+                                   const std::uint8_t* __restrict__ cells)
+{
+    const long long n = static_cast<long long>(L0) * L1 * K2;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % L0);
+        const long long r = i / L0;
+        const int y = static_cast<int>(r % L1);
+        const int w = static_cast<int>(r / L1);
+        float v = 0.f;
+        if (x < K0 && y < K1) {
+            v = cells[x + static_cast<long long>(K0) * (y + static_cast<long long>(K1) * w)] ? 1.f : 0.f;
+        }
+        kp[i] = make_float2(v, 0.f);
+    }
+}
+
+// Pass A: one block per group of 16 consecutive kx at one ky.
+__global__ void pass_a_kernel(const float2* __restrict__ spectrum, const float2* __restrict__ partial,
+                              float2* __restrict__ inter, int L0, int L1, int L2, int K2, int legal_z,
+                              const float2* __restrict__ twiddles)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int pitch = L2 + 1;
+    float2* tw = reinterpret_cast<float2*>(smem_raw);
+    float2* a = tw + L2;
+    float2* b = a + kColumnGroup * pitch;
+    float2* s = b + kColumnGroup * pitch;
+    for (int m = threadIdx.x; m < L2; m += blockDim.x) {
+        tw[m] = twiddles[m];
+    }
+    const int groups_x = L0 / kColumnGroup;
+    const int ky = blockIdx.x / groups_x;
+    const int kx0 = (blockIdx.x % groups_x) * kColumnGroup;
+    const long long plane = static_cast<long long>(L0) * L1;
+    const long long column = kx0 + static_cast<long long>(L0) * ky;
+    for (int e = threadIdx.x; e < kColumnGroup * L2; e += blockDim.x) {
+        const int j = e % kColumnGroup;
+        const int q = e / kColumnGroup;
+        const long long at = column + j + plane * q;
+        s[j * L2 + q] = spectrum[at];
+        a[j * pitch + q] = q < K2 ? partial[at] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    float2* k = fft_lines_smem(a, b, tw, L2, kColumnGroup, pitch, false);
+    float2* o = k == a ? b : a;
+    for (int e = threadIdx.x; e < kColumnGroup * L2; e += blockDim.x) {
+        const int j = e / L2;
+        const int q = e - j * L2;
+        o[j * pitch + q] = cmulconj(s[j * L2 + q], k[j * pitch + q]);
+    }
+    __syncthreads();
+    float2* w = fft_lines_smem(o, k, tw, L2, kColumnGroup, pitch, true);
+    for (int e = threadIdx.x; e < kColumnGroup * legal_z; e += blockDim.x) {
+        const int j = e % kColumnGroup;
+        const int q = e / kColumnGroup;
+        inter[column + j + plane * q] = w[j * pitch + q];
+    }
+}
+
+__device__ __forceinline__ unsigned long long make_key(double score, unsigned int index)
+{
+    const float f = __double2float_rd(score);
+    const unsigned int u = __float_as_uint(f);
+    const unsigned int k = (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+    return (static_cast<unsigned long long>(k) << 32) | index;
+}
+
+__device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, int lane)
+{
+    for (int k = 2; k <= 32; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const unsigned long long o = __shfl_xor_sync(kFull, v, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            v = (lower == up) ? (v < o ? v : o) : (v > o ? v : o);
+        }
+    }
+    return v;
+}
+
+// Sorts a bitonic 32-sequence held one key per lane (ascending).
+__device__ __forceinline__ unsigned long long warp_bitonic_finish(unsigned long long m, int lane)
+{
+    for (int j = 16; j > 0; j >>= 1) {
+        const unsigned long long o = __shfl_xor_sync(kFull, m, j);
+        m = ((lane & j) == 0) ? (m < o ? m : o) : (m > o ? m : o);
+    }
+    return m;
+}
+
+// Keeps the 64 smallest keys seen by the warp: lo holds ranks 0..31 and hi
+// ranks 32..63, each sorted ascending across lanes.
+__device__ __forceinline__ void warp_insert(unsigned long long& lo, unsigned long long& hi, unsigned long long key,
+                                            int lane)
+{
+    const unsigned long long worst = __shfl_sync(kFull, hi, 31);
+    if (!__any_sync(kFull, key < worst)) {
+        return;
+    }
+    key = warp_sort32(key, lane);
+    // split lo | key into the 32 smallest (new lo) and the 32 largest (spill)
+    unsigned long long rev = __shfl_sync(kFull, key, 31 - lane);
+    const unsigned long long small = lo < rev ? lo : rev;
+    const unsigned long long large = lo < rev ? rev : lo;
+    lo = warp_bitonic_finish(small, lane);
+    const unsigned long long spill = warp_bitonic_finish(large, lane);
+    // keep the 32 smallest of hi | spill
+    rev = __shfl_sync(kFull, spill, 31 - lane);
+    hi = warp_bitonic_finish(hi < rev ? hi : rev, lane);
+}
+
+// Pass B2: inverse FFT along x for 8 legal rows, then the fused epilogue.
+// mode 0: warp top-32 lists + pruning bound in *tau; mode 1: append every
+// candidate whose approximate score is <= threshold and count every candidate
+// past the cursor floor in *tau.
+__global__ void pass_b2_kernel(const float2* __restrict__ inter, int L0, int L1, int legal_x, int legal_y,
+                               int legal_z, const float2* __restrict__ twiddles, const double* __restrict__ t65,
+                               double inv_occ, int mode, double threshold, double cursor_floor,
+                               unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
+                               unsigned int cap, unsigned long long* __restrict__ tau,
+                               unsigned long long* __restrict__ resid)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int pitch = L0 + 1;
+    float2* tw = reinterpret_cast<float2*>(smem_raw);
+    float2* a = tw + L0;
+    float2* b = a + kB2Rows * pitch;
+    for (int m = threadIdx.x; m < L0; m += blockDim.x) {
+        tw[m] = twiddles[m];
+    }
+    const long long rows = static_cast<long long>(legal_y) * legal_z;
+    const long long row0 = static_cast<long long>(blockIdx.x) * kB2Rows;
+    for (int e = threadIdx.x; e < kB2Rows * L0; e += blockDim.x) {
+        const int j = e / L0;
+        const int q = e - j * L0;
+        const long long row = row0 + j;
+        float2 v = make_float2(0.f, 0.f);
+        if (row < rows) {
+            const long long y = row % legal_y;
+            const long long zz = row / legal_y;
+            v = inter[q + static_cast<long long>(L0) * (y + static_cast<long long>(L1) * zz)];
+        }
+        a[j * pitch + q] = v;
+    }
+    __syncthreads();
+    const float2* res = fft_lines_smem(a, b, tw, L0, kB2Rows, pitch, true);
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const long long row = row0 + warp;
+    if (warp >= kB2Rows || row >= rows) {
+        return;
+    }
+    const int y = static_cast<int>(row % legal_y);
+    const int zz = static_cast<int>(row / legal_y);
+    const double t65z = t65[zz];
+    unsigned long long list_lo = kEmptyKey, list_hi = kEmptyKey;
+    float residual = 0.f;
+    const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
+    for (int c = 0; c < legal_x; c += 32) {
+        const int x = c + lane;
+        unsigned long long key = kEmptyKey;
+        bool take = false;
+        if (x < legal_x) {
+            const float2 v = res[warp * pitch + x];
+            residual = fmaxf(residual, fabsf(v.x - rintf(v.x)));
+            if (fabsf(v.x) < 0.5f) {
+                const double score = t65z - 0.35 * (static_cast<double>(v.y) * inv_occ);
+                if (score >= cursor_floor) {
+                    key = make_key(score, row_index + x);
+                    take = mode == 1 && score <= threshold;
+                    if (mode == 1) {
+                        atomicAdd(tau, 1ULL);
+                    }
+                }
+            }
+        }
+        if (mode == 0) {
+            warp_insert(list_lo, list_hi, key, lane);
+        }
+        else {
+            const unsigned mask = __ballot_sync(kFull, take);
+            if (mask) {
+                unsigned int base = 0;
+                if (lane == 0) {
+                    base = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+                }
+                base = __shfl_sync(kFull, base, 0);
+                const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+                if (take && base + rank < cap) {
+                    keys[base + rank] = key;
+                }
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        residual = fmaxf(residual, __shfl_xor_sync(kFull, residual, o));
+    }
+    if (lane == 0 && residual > 0.f) {
+        atomicMax(resid, static_cast<unsigned long long>(__float_as_uint(residual)));
+    }
+    if (mode == 0) {
+        const unsigned long long bound = *reinterpret_cast<volatile unsigned long long*>(tau);
+        for (int half = 0; half < 2; ++half) {
+            const unsigned long long v = half ? list_hi : list_lo;
+            const bool take = v != kEmptyKey && v <= bound;
+            const unsigned mask = __ballot_sync(kFull, take);
+            if (mask) {
+                unsigned int base = 0;
+                if (lane == 0) {
+                    base = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+                }
+                base = __shfl_sync(kFull, base, 0);
+                const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+                if (take && base + rank < cap) {
+                    keys[base + rank] = v;
+                }
+            }
+        }
+        const unsigned long long worst = __shfl_sync(kFull, list_hi, 31);
+        if (lane == 0 && worst != kEmptyKey) {
+            atomicMin(tau, worst);
+        }
+    }
+}
+
+// Sorts up to kKeyCapacity keys of one request and keeps the smallest
+// kExactPerOrientation + 1 (padded with kEmptyKey).
+__global__ void merge_kernel(const unsigned long long* __restrict__ keys, const unsigned int* __restrict__ counts,
+                             unsigned long long* __restrict__ selected)
+{
+    __shared__ unsigned long long s[kKeyCapacity];
+    const int r = blockIdx.x;
+    const unsigned int n = min(counts[r], kKeyCapacity);
+    unsigned int size = 1;
+    while (size < n) {
+        size <<= 1;
+    }
+    for (unsigned int i = threadIdx.x; i < size; i += blockDim.x) {
+        s[i] = i < n ? keys[static_cast<long long>(r) * kKeyCapacity + i] : kEmptyKey;
+    }
+    __syncthreads();
+    for (unsigned int k = 2; k <= size; k <<= 1) {
+        for (unsigned int j = k >> 1; j > 0; j >>= 1) {
+            for (unsigned int i = threadIdx.x; i < size; i += blockDim.x) {
+                const unsigned int p = i ^ j;
+                if (p > i) {
+                    const bool up = (i & k) == 0;
+                    const unsigned long long x = s[i], y = s[p];
+                    if ((x > y) == up) {
+                        s[i] = y;
+                        s[p] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int i = threadIdx.x; i <= kExactPerOrientation; i += blockDim.x) {
+        selected[static_cast<long long>(r) * (kExactPerOrientation + 1) + i] =
+            static_cast<unsigned int>(i) < size ? s[i] : kEmptyKey;
+    }
+}
+
+struct ExactJob {
+    const std::int32_t* ones;
+    int ones_count;
+    int legal_x, legal_y;
+};
+
+// One block per selected key: exact overlap recount and exact proximity sum.
+__global__ void exact_kernel(const unsigned long long* __restrict__ selected, const ExactJob* __restrict__ jobs,
+                             int per_request, const std::uint8_t* __restrict__ occ,
+                             const std::int32_t* __restrict__ d2, const double* __restrict__ table, int E0, int E1,
+                             long long* __restrict__ out_count, double* __restrict__ out_p,
+                             int* __restrict__ range_error)
+{
+    const int request = static_cast<int>(blockIdx.x / per_request);
+    const unsigned long long key = selected[blockIdx.x];
+    if (key == kEmptyKey) {
+        if (threadIdx.x == 0) {
+            out_count[blockIdx.x] = -1;
+            out_p[blockIdx.x] = 0.0;
+        }
+        return;
+    }
+    const ExactJob job = jobs[request];
+    const unsigned int index = static_cast<unsigned int>(key & 0xffffffffULL);
+    const long long sx = index % job.legal_x;
+    const long long rest = index / job.legal_x;
+    const long long sy = rest % job.legal_y;
+    const long long sz = rest / job.legal_y;
+    const long long base = sx + E0 * (sy + static_cast<long long>(E1) * sz);
+    SuperAcc acc;
+    super_clear(acc);
+    long long overlap = 0;
+    bool ok = true;
+    for (int i = threadIdx.x; i < job.ones_count; i += blockDim.x) {
+        const long long cell = base + job.ones[i];
+        overlap += occ[cell];
+        const std::int32_t v = d2[cell];
+        ok &= super_add(acc, v == kInf ? 0.0 : table[v]);
+    }
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        overlap += __shfl_xor_sync(kFull, overlap, o);
+        for (int l = 0; l < kSuperLimbs; ++l) {
+            acc.limb[l] += __shfl_xor_sync(kFull, acc.limb[l], o);
+        }
+    }
+    __shared__ long long s_limbs[8][kSuperLimbs];
+    __shared__ long long s_overlap[8];
+    if (lane == 0) {
+        s_overlap[warp] = overlap;
+        for (int l = 0; l < kSuperLimbs; ++l) {
+            s_limbs[warp][l] = acc.limb[l];
+        }
+    }
+    if (!ok) {
+        atomicOr(range_error, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        SuperAcc total;
+        super_clear(total);
+        long long count = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) {
+            count += s_overlap[w];
+            for (int l = 0; l < kSuperLimbs; ++l) {
+                total.limb[l] += s_limbs[w][l];
+            }
+        }
+        out_count[blockIdx.x] = count;
+        out_p[blockIdx.x] = super_round(total);
+    }
+}
+
+double decode_key_score(unsigned long long key)
+{
+    const unsigned int k = static_cast<unsigned int>(key >> 32);
+    const unsigned int u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return static_cast<double>(f);
+}
+
+bool rank_less(const Candidate& l, const Candidate& r)
+{
+    if (l.score != r.score) {
+        return l.score < r.score;
+    }
+    if (l.orientation != r.orientation) {
+        return l.orientation < r.orientation;
+    }
+    return std::tie(l.t[2], l.t[1], l.t[0]) < std::tie(r.t[2], r.t[1], r.t[0]);
+}
+
+template <typename Kernel>
+void allow_large_smem(Kernel k)
+{
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+}  // namespace
+
+Pipeline::~Pipeline()
+{
+    for (auto& s : slots_) {
+        cudaFree(s.partial);
+        cudaFree(s.ones);
+        cudaFree(s.t65);
+    }
+}
+
+int Pipeline::set_geometry(const std::int64_t* env_first, const std::uint32_t* env_shape, const double* origin,
+                           double pitch, double container_min_z, double container_height)
+{
+    for (int a = 0; a != 3; ++a) {
+        if (env_shape[a] == 0) {
+            return kInvalidArgument;
+        }
+        E_[a] = static_cast<int>(env_shape[a]);
+        const std::uint32_t L = next_pow2(std::max<std::uint32_t>(env_shape[a], 16));
+        if (L > static_cast<std::uint32_t>(kMaxFftLength)) {
+            return kUnsupportedLength;
+        }
+        L_[a] = static_cast<int>(L);
+        env_first_[a] = env_first[a];
+        origin_[a] = origin[a];
+    }
+    pitch_ = pitch;
+    cmin_z_ = container_min_z;
+    height_ = container_height;
+    const long long cells = static_cast<long long>(E_[0]) * E_[1] * E_[2];
+    const long long grid = static_cast<long long>(L_[0]) * L_[1] * L_[2];
+    int status = kOk;
+    occ_ = static_cast<std::uint8_t*>(device_buffer(ctx_, "pipe.occ", cells, status));
+    d2_ = static_cast<std::int32_t*>(device_buffer(ctx_, "pipe.d2", cells * sizeof(std::int32_t), status));
+    spectrum_ = static_cast<float2*>(device_buffer(ctx_, "pipe.spectrum", grid * sizeof(float2), status));
+    if (!occ_ || !d2_ || !spectrum_) {
+        return status;
+    }
+    const std::uint32_t shape[3] = { env_shape[0], env_shape[1], env_shape[2] };
+    if (!proximity_shape_supported(shape)) {
+        return kProximityShape;
+    }
+    table_ = proximity_table(ctx_, max_squared_distance(shape), status);
+    return table_ ? kOk : status;
+}
+
+int Pipeline::set_occupancy(const std::uint8_t* d_occupancy)
+{
+    cudaStream_t st = ctx_->stream;
+    const long long cells = static_cast<long long>(E_[0]) * E_[1] * E_[2];
+    if (d_occupancy != occ_) {
+        cudaMemcpyAsync(occ_, d_occupancy, cells, cudaMemcpyDeviceToDevice, st);
+    }
+    const std::uint32_t shape[3] = { static_cast<std::uint32_t>(E_[0]), static_cast<std::uint32_t>(E_[1]),
+                                     static_cast<std::uint32_t>(E_[2]) };
+    int status = edt_squared(ctx_, occ_, d2_, shape, st);
+    if (status) {
+        return status;
+    }
+    const long long grid = static_cast<long long>(L_[0]) * L_[1] * L_[2];
+    const int blocks = launch_blocks(grid, 256);
+    auto* partial = static_cast<double*>(device_buffer(ctx_, "pipe.norm", blocks * sizeof(double), status));
+    if (!partial) {
+        return status;
+    }
+    env_pack_kernel<<<blocks, 256, 0, st>>>(spectrum_, L_[0], L_[1], L_[2], E_[0], E_[1], E_[2], occ_, d2_, table_,
+                                             partial);
+    ctx_->launches++;
+    for (int axis = 0; axis != 3; ++axis) {
+        const auto* tw = twiddle_table<float>(ctx_, L_[axis], status);
+        if (!tw) {
+            return status;
+        }
+        const float scale = axis == 2 ? static_cast<float>(1.0 / static_cast<double>(grid)) : 1.f;
+        if (fft_axis<float>(spectrum_, L_[0], L_[1], L_[2], axis, false, scale, tw, st) != cudaSuccess) {
+            return kCuda;
+        }
+        ctx_->launches++;
+    }
+    std::vector<double> host(blocks);
+    cudaMemcpyAsync(host.data(), partial, blocks * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        return kCuda;
+    }
+    double sum = 0;
+    for (double v : host) {
+        sum += v;
+    }
+    z_norm_ = std::sqrt(sum);
+    return kOk;
+}
+
+int Pipeline::add_kernel(std::uint64_t orientation, const std::int64_t* first, const std::uint32_t* shape,
+                         const std::uint8_t* cells, double max_z, std::uint64_t& slot_out)
+{
+    KernelSlot s;
+    s.orientation = orientation;
+    std::uint64_t n = 1;
+    for (int a = 0; a != 3; ++a) {
+        s.K[a] = static_cast<int>(shape[a]);
+        s.first[a] = first[a];
+        s.legal[a] = E_[a] >= s.K[a] ? E_[a] - s.K[a] + 1 : 0;
+        n *= shape[a];
+    }
+    s.max_z = max_z;
+    s.host_cells.assign(cells, cells + n);
+    std::vector<std::int32_t> ones;
+    for (int z = 0; z < s.K[2]; ++z) {
+        for (int y = 0; y < s.K[1]; ++y) {
+            for (int x = 0; x < s.K[0]; ++x) {
+                if (cells[x + static_cast<std::uint64_t>(s.K[0]) * (y + static_cast<std::uint64_t>(s.K[1]) * z)]) {
+                    ones.push_back(x + E_[0] * (y + E_[1] * z));
+                }
+            }
+        }
+    }
+    s.occupied = ones.size();
+    const bool fits = s.legal[0] && s.legal[1] && s.legal[2];
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
+    if (fits && !ones.empty()) {
+        // The kernel must fit the FFT period: K <= E <= L always holds here.
+        const long long partial_cells = static_cast<long long>(L_[0]) * L_[1] * s.K[2];
+        if (cudaMalloc(&s.partial, partial_cells * sizeof(float2)) != cudaSuccess ||
+            cudaMalloc(&s.ones, ones.size() * sizeof(std::int32_t)) != cudaSuccess ||
+            cudaMalloc(&s.t65, s.legal[2] * sizeof(double)) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(s.partial);
+            cudaFree(s.ones);
+            cudaFree(s.t65);
+            return kAllocation;
+        }
+        cudaMemcpyAsync(s.ones, ones.data(), ones.size() * sizeof(std::int32_t), cudaMemcpyHostToDevice, st);
+        std::vector<double> t65(s.legal[2]);
+        for (int zi = 0; zi < s.legal[2]; ++zi) {
+            const std::int64_t tz = env_first_[2] - s.first[2] + zi;
+            const double world_z = origin_[2] + pitch_ * static_cast<double>(tz);
+            const double top = (world_z + max_z - cmin_z_) / height_;
+            t65[zi] = .65 * top;
+        }
+        cudaMemcpyAsync(s.t65, t65.data(), t65.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+        auto* d_cells = static_cast<std::uint8_t*>(device_buffer(ctx_, "pipe.kcells", n, status));
+        if (!d_cells) {
+            return status;
+        }
+        cudaMemcpyAsync(d_cells, cells, n, cudaMemcpyHostToDevice, st);
+        kernel_pack_kernel<<<launch_blocks(partial_cells, 256), 256, 0, st>>>(s.partial, L_[0], L_[1], s.K[0],
+                                                                               s.K[1], s.K[2], d_cells);
+        ctx_->launches++;
+        for (int axis = 0; axis != 2; ++axis) {
+            const auto* tw = twiddle_table<float>(ctx_, L_[axis], status);
+            if (!tw) {
+                return status;
+            }
+            if (fft_axis<float>(s.partial, L_[0], L_[1], s.K[2], axis, false, 1.f, tw, st) != cudaSuccess) {
+                return kCuda;
+            }
+            ctx_->launches++;
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            return kCuda;
+        }
+    }
+    slot_out = slots_.size();
+    slots_.push_back(std::move(s));
+    return kOk;
+}
+
+double Pipeline::approx_epsilon(const KernelSlot& s) const
+{
+    // Error bound of the FP32 proximity sum: 2^-14 * log2(N) * |Z|_2 * sqrt(occ) / sqrt(N),
+    // checked at run time against every exactly rescored candidate.
+    const double n = static_cast<double>(L_[0]) * L_[1] * L_[2];
+    const double eps_p = std::ldexp(1.0, -14) * std::log2(n) * z_norm_ * std::sqrt(static_cast<double>(s.occupied)) /
+                         std::sqrt(n);
+    return .35 * eps_p / static_cast<double>(s.occupied);
+}
+
+double Pipeline::epsilon_p(const KernelSlot& s) const
+{
+    return approx_epsilon(s) * static_cast<double>(s.occupied) / .35;
+}
+
+double Pipeline::score(const KernelSlot& s, const std::int64_t* t, double p) const
+{
+    // spectral_pipeline.cpp:1794-1800, evaluated in the same order.
+    const double mean_proximity = p / static_cast<double>(s.occupied);
+    const double world_z = origin_[2] + pitch_ * static_cast<double>(t[2]);
+    const double top = (world_z + s.max_z - cmin_z_) / height_;
+    return .65 * top - .35 * mean_proximity;
+}
+
+int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, double cursor_floor,
+                              unsigned long long* keys, unsigned int* count, unsigned int cap,
+                              unsigned long long* tau, unsigned long long* resid)
+{
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
+    const std::size_t inter = static_cast<std::size_t>(L_[0]) * L_[1] * s.legal[2] * sizeof(float2);
+    if (inter > inter_bytes_) {
+        inter_ = static_cast<float2*>(device_buffer(ctx_, "pipe.inter", inter, status));
+        if (!inter_) {
+            return status;
+        }
+        inter_bytes_ = inter;
+    }
+    static bool configured = false;
+    if (!configured) {
+        allow_large_smem(pass_a_kernel);
+        allow_large_smem(pass_b2_kernel);
+        configured = true;
+    }
+    const auto* tw0 = twiddle_table<float>(ctx_, L_[0], status);
+    const auto* tw1 = twiddle_table<float>(ctx_, L_[1], status);
+    const auto* tw2 = twiddle_table<float>(ctx_, L_[2], status);
+    if (!tw0 || !tw1 || !tw2) {
+        return status;
+    }
+    const std::size_t smem_a = sizeof(float2) * (L_[2] + 2 * kColumnGroup * (L_[2] + 1) + kColumnGroup * L_[2]);
+    pass_a_kernel<<<(L_[0] / kColumnGroup) * L_[1], 256, smem_a, st>>>(spectrum_, s.partial, inter_, L_[0], L_[1],
+                                                                        L_[2], s.K[2], s.legal[2], tw2);
+    ctx_->launches++;
+    if (fft_axis<float>(inter_, L_[0], L_[1], s.legal[2], 1, true, 1.f, tw1, st, s.legal[1]) != cudaSuccess) {
+        return kCuda;
+    }
+    ctx_->launches++;
+    const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
+    const std::size_t smem_b = sizeof(float2) * (L_[0] + 2 * kB2Rows * (L_[0] + 1));
+    pass_b2_kernel<<<static_cast<unsigned>((rows + kB2Rows - 1) / kB2Rows), 32 * kB2Rows, smem_b, st>>>(
+        inter_, L_[0], L_[1], s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied),
+        mode, threshold, cursor_floor, keys, count, cap, tau, resid);
+    ctx_->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out)
+{
+    const int R = static_cast<int>(requests.size());
+    out.assign(R, {});
+    if (R == 0) {
+        return kOk;
+    }
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
+    const int per = kExactPerOrientation + 1;
+    auto* keys = static_cast<unsigned long long*>(
+        device_buffer(ctx_, "pipe.keys", static_cast<std::size_t>(R) * kKeyCapacity * 8, status));
+    auto* meta = static_cast<unsigned long long*>(device_buffer(ctx_, "pipe.meta", static_cast<std::size_t>(R) * 24,
+                                                                status));
+    auto* selected = static_cast<unsigned long long*>(
+        device_buffer(ctx_, "pipe.selected", static_cast<std::size_t>(R) * per * 8, status));
+    auto* jobs = static_cast<ExactJob*>(device_buffer(ctx_, "pipe.jobs", R * sizeof(ExactJob), status));
+    auto* counts_out = static_cast<long long*>(
+        device_buffer(ctx_, "pipe.ecount", static_cast<std::size_t>(R) * per * 8, status));
+    auto* p_out = static_cast<double*>(device_buffer(ctx_, "pipe.ep", static_cast<std::size_t>(R) * per * 8, status));
+    auto* range_error = static_cast<int*>(device_buffer(ctx_, "pipe.rangeerr", 16, status));
+    if (!keys || !meta || !selected || !jobs || !counts_out || !p_out || !range_error) {
+        return status;
+    }
+    // meta layout: tau[R] (u64), resid[R] (u64), count[R] (u32, in the last third as u64 slots)
+    unsigned long long* tau = meta;
+    unsigned long long* resid = meta + R;
+    auto* count = reinterpret_cast<unsigned int*>(meta + 2 * R);
+    std::vector<unsigned long long> init(3 * R, 0);
+    for (int r = 0; r < R; ++r) {
+        init[r] = kEmptyKey;
+    }
+    cudaMemcpyAsync(meta, init.data(), init.size() * 8, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(range_error, 0, 16, st);
+    std::vector<ExactJob> host_jobs(R);
+    std::vector<double> eps_s(R), floor(R);
+    for (int r = 0; r < R; ++r) {
+        const auto& s = slots_[requests[r].slot];
+        host_jobs[r] = { s.ones, static_cast<int>(s.occupied), std::max(s.legal[0], 1), std::max(s.legal[1], 1) };
+        if (!s.legal[0] || !s.legal[1] || !s.legal[2] || !s.occupied) {
+            continue;
+        }
+        eps_s[r] = approx_epsilon(s) + std::ldexp(1.0, -22);
+        floor[r] = requests[r].has_cursor ? requests[r].cursor.score - eps_s[r] : -INFINITY;
+        if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * kKeyCapacity,
+                                      count + r, kKeyCapacity, tau + r, resid + r))) {
+            return status;
+        }
+    }
+    cudaMemcpyAsync(jobs, host_jobs.data(), R * sizeof(ExactJob), cudaMemcpyHostToDevice, st);
+    merge_kernel<<<R, 1024, 0, st>>>(keys, count, selected);
+    exact_kernel<<<R * per, 256, 0, st>>>(selected, jobs, per, occ_, d2_, table_, E_[0], E_[1], counts_out, p_out,
+                                          range_error);
+    ctx_->launches += 2;
+    std::vector<unsigned long long> h_meta(3 * R), h_sel(static_cast<std::size_t>(R) * per);
+    std::vector<long long> h_count(static_cast<std::size_t>(R) * per);
+    std::vector<double> h_p(static_cast<std::size_t>(R) * per);
+    int h_range = 0;
+    cudaMemcpyAsync(h_meta.data(), meta, h_meta.size() * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h_sel.data(), selected, h_sel.size() * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h_count.data(), counts_out, h_count.size() * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h_p.data(), p_out, h_p.size() * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&h_range, range_error, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    if (h_range) {
+        return kNumericRange;
+    }
+    const auto* h_count32 = reinterpret_cast<const unsigned int*>(h_meta.data() + 2 * R);
+    for (int r = 0; r < R; ++r) {
+        const auto& req = requests[r];
+        const auto& s = slots_[req.slot];
+        auto& o = out[r];
+        if (!s.legal[0] || !s.legal[1] || !s.legal[2]) {
+            o.certified = true;  // kernel wider than the environment: complete, empty page
+            continue;
+        }
+        if (!s.occupied) {
+            o.status = kEmptyKernel;
+            continue;
+        }
+        std::uint32_t rbits = static_cast<std::uint32_t>(h_meta[R + r]);
+        float rf;
+        std::memcpy(&rf, &rbits, 4);
+        o.max_integer_residual = rf;
+        if (rf >= 0.25f) {
+            o.status = kNumeric;  // correlation.cpp:521-528 residual guard
+            continue;
+        }
+        const unsigned int n = h_count32[r];
+        const unsigned long long tau_r = h_meta[r];
+        std::vector<Candidate> all;
+        double max_error = 0;
+        const std::int64_t legal_first[3] = { env_first_[0] - s.first[0], env_first_[1] - s.first[1],
+                                              env_first_[2] - s.first[2] };
+        const int m = static_cast<int>(std::min<unsigned int>(n, kExactPerOrientation));
+        for (int i = 0; i < m; ++i) {
+            const unsigned long long key = h_sel[static_cast<std::size_t>(r) * per + i];
+            const long long overlap = h_count[static_cast<std::size_t>(r) * per + i];
+            const double p = h_p[static_cast<std::size_t>(r) * per + i];
+            const unsigned int index = static_cast<unsigned int>(key & 0xffffffffULL);
+            Candidate c {};
+            c.t[0] = legal_first[0] + index % s.legal[0];
+            c.t[1] = legal_first[1] + (index / s.legal[0]) % s.legal[1];
+            c.t[2] = legal_first[2] + index / (static_cast<unsigned int>(s.legal[0]) * s.legal[1]);
+            c.orientation = s.orientation;
+            c.score = score(s, c.t, p);
+            c.binary_overlap = static_cast<double>(overlap);
+            c.direct_zero = overlap == 0;
+            const double approx = decode_key_score(key);
+            max_error = std::max(max_error, std::fabs(approx - c.score));
+            ++o.rescored;
+            if (overlap != 0) {
+                continue;  // the reference's FFT rounding never admits these
+            }
+            if (req.has_cursor && !rank_less(req.cursor, c)) {
+                continue;
+            }
+            all.push_back(c);
+        }
+        o.max_score_error = max_error;
+        if (max_error > eps_s[r]) {
+            o.status = kNumeric;  // the FP32 bound did not hold: fail closed
+            continue;
+        }
+        std::sort(all.begin(), all.end(), rank_less);
+        if (all.size() > static_cast<std::size_t>(kPageSize)) {
+            all.resize(kPageSize);
+        }
+        unsigned long long excluded = kEmptyKey;
+        if (n > kKeyCapacity) {
+            excluded = 0;  // overflowed: nothing can be certified
+        }
+        else {
+            if (n > static_cast<unsigned int>(kExactPerOrientation)) {
+                excluded = h_sel[static_cast<std::size_t>(r) * per + kExactPerOrientation];
+            }
+            excluded = std::min(excluded, tau_r);
+        }
+        bool certified;
+        if (excluded == kEmptyKey) {
+            certified = true;
+        }
+        else if (all.size() == static_cast<std::size_t>(kPageSize)) {
+            certified = excluded != 0 && decode_key_score(excluded) - eps_s[r] > all.back().score;
+        }
+        else {
+            certified = false;
+        }
+        o.page = std::move(all);
+        o.certified = certified;
+        // Starting bound for a threshold pass over a page that is not full:
+        // the lowest excluded approximate score, or the last rescored one.
+        double start = m > 0 ? decode_key_score(h_sel[static_cast<std::size_t>(r) * per + m - 1]) : -INFINITY;
+        if (excluded != kEmptyKey && excluded != 0) {
+            start = std::max(start, decode_key_score(excluded));
+        }
+        o.excluded_score = start;
+        if (std::getenv("SPK_DEBUG_PAGES")) {
+            std::fprintf(stderr, "page r=%d n=%u tau=%llx m=%d page=%zu certified=%d eps=%g err=%g start=%.17g\n", r,
+                         n, tau_r, m, o.page.size(), certified ? 1 : 0, eps_s[r], max_error, start);
+        }
+    }
+    // Threshold passes for every uncertified page (each recomputes that
+    // orientation): collect every candidate whose approximate score is <= T,
+    // rescore all of them exactly, and widen T until the page is certified.
+    for (int r = 0; r < R; ++r) {
+        auto& o = out[r];
+        if (o.status || o.certified) {
+            continue;
+        }
+        const auto& req = requests[r];
+        const auto& s = slots_[req.slot];
+        const std::int64_t legal_first[3] = { env_first_[0] - s.first[0], env_first_[1] - s.first[1],
+                                              env_first_[2] - s.first[2] };
+        // Everything left out of a threshold pass has approximate score > T, so
+        // exact score > T - eps; T = S32 + 2 eps certifies a page whose 32nd
+        // entry did not get worse.
+        double threshold = o.page.size() == static_cast<std::size_t>(kPageSize)
+                               ? o.page.back().score + 2 * eps_s[r]
+                               : o.excluded_score + 2 * eps_s[r];
+        double widen = std::max(4 * eps_s[r], 1e-6);
+        unsigned int cap = kKeyCapacity;
+        for (int attempt = 0; attempt < 24 && !o.certified; ++attempt) {
+            auto* tkeys = static_cast<unsigned long long*>(device_buffer(ctx_, "pipe.tkeys", cap * 8ULL, status));
+            if (!tkeys) {
+                return status;
+            }
+            unsigned long long zero[3] = { 0, 0, 0 };
+            cudaMemcpyAsync(meta, zero, 24, cudaMemcpyHostToDevice, st);
+            if ((status = run_orientation(s, 1, threshold, floor[r], tkeys, reinterpret_cast<unsigned int*>(meta + 2),
+                                          cap, meta, meta + 1))) {
+                return status;
+            }
+            unsigned long long h[3];
+            cudaMemcpyAsync(h, meta, 24, cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) {
+                return kCuda;
+            }
+            const unsigned int n = static_cast<unsigned int>(h[2] & 0xffffffffULL);
+            const unsigned long long total = h[0];
+            if (n > cap) {
+                cap = n + 1024;
+                --attempt;
+                continue;
+            }
+            std::vector<Candidate> all;
+            if (n) {
+                auto* tcount = static_cast<long long*>(device_buffer(ctx_, "pipe.tcount", n * 8ULL, status));
+                auto* tp = static_cast<double*>(device_buffer(ctx_, "pipe.tp", n * 8ULL, status));
+                if (!tcount || !tp) {
+                    return status;
+                }
+                ExactJob job { s.ones, static_cast<int>(s.occupied), s.legal[0], s.legal[1] };
+                cudaMemcpyAsync(jobs, &job, sizeof(job), cudaMemcpyHostToDevice, st);
+                exact_kernel<<<n, 256, 0, st>>>(tkeys, jobs, static_cast<int>(n), occ_, d2_, table_, E_[0], E_[1],
+                                                tcount, tp, range_error);
+                ctx_->launches++;
+                std::vector<unsigned long long> hk(n);
+                std::vector<long long> cnt(n);
+                std::vector<double> pv(n);
+                cudaMemcpyAsync(hk.data(), tkeys, n * 8ULL, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(cnt.data(), tcount, n * 8ULL, cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(pv.data(), tp, n * 8ULL, cudaMemcpyDeviceToHost, st);
+                if (cudaStreamSynchronize(st) != cudaSuccess) {
+                    return kCuda;
+                }
+                for (unsigned int i = 0; i < n; ++i) {
+                    const unsigned int index = static_cast<unsigned int>(hk[i] & 0xffffffffULL);
+                    Candidate c {};
+                    c.t[0] = legal_first[0] + index % s.legal[0];
+                    c.t[1] = legal_first[1] + (index / s.legal[0]) % s.legal[1];
+                    c.t[2] = legal_first[2] + index / (static_cast<unsigned int>(s.legal[0]) * s.legal[1]);
+                    c.orientation = s.orientation;
+                    c.score = score(s, c.t, pv[i]);
+                    c.binary_overlap = static_cast<double>(cnt[i]);
+                    c.direct_zero = cnt[i] == 0;
+                    o.max_score_error = std::max(o.max_score_error, std::fabs(decode_key_score(hk[i]) - c.score));
+                    ++o.rescored;
+                    if (cnt[i] != 0 || (req.has_cursor && !rank_less(req.cursor, c))) {
+                        continue;
+                    }
+                    all.push_back(c);
+                }
+            }
+            if (o.max_score_error > eps_s[r]) {
+                o.status = kNumeric;
+                break;
+            }
+            std::sort(all.begin(), all.end(), rank_less);
+            if (all.size() > static_cast<std::size_t>(kPageSize)) {
+                all.resize(kPageSize);
+            }
+            const bool complete = n == total;
+            const bool full = all.size() == static_cast<std::size_t>(kPageSize);
+            o.page = std::move(all);
+            o.threshold_pass = true;
+            if (complete || (full && o.page.back().score < threshold - eps_s[r])) {
+                o.certified = true;
+                break;
+            }
+            if (std::getenv("SPK_DEBUG_PAGES")) {
+                std::fprintf(stderr, "threshold r=%d T=%.17g n=%u total=%llu page=%zu\n", r, threshold, n, total,
+                             o.page.size());
+            }
+            threshold = full ? std::max(o.page.back().score + 2 * eps_s[r], threshold + widen) : threshold + widen;
+            widen *= 4;
+        }
+        if (!o.certified && !o.status) {
+            o.status = kScratchLimit;
+        }
+    }
+    return kOk;
+}
+
+}  // namespace spk

@@ -1,0 +1,118 @@
+// Spectral page pipeline: legal-translation correlation of one environment
+// (occupancy + proximity) against many oriented kernels, fused threshold,
+// approximate score and top-k, then exact integer recount and exact FP64
+// proximity sums for the selected candidates.
+//
+// Reference behaviour restated (engine/pack_solver/src/spectral_pipeline.cpp):
+//   legal translations  first = env.first - kernel.first, extent E-K+1   :1618-1648
+//   score = .65 * (world_z + max_z - c_min_z) / H - .35 * prox / occ      :1794-1800
+//   ordinary pages keep round(binary) == 0, rank by (score, o, z, y, x),
+//   32 entries after an exclusive cursor                                  :1706-1824
+//   direct_zero_overlap = exact u8 recount of each page candidate         :1825-1857
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "../../include/spk_b200.h"
+#include "common.cuh"
+
+struct spk_context;
+
+namespace spk {
+
+constexpr int kPageSize = 32;
+constexpr int kExactPerOrientation = 64;
+constexpr unsigned kKeyCapacity = 4096;
+constexpr unsigned long long kEmptyKey = ~0ULL;
+
+struct Candidate {
+    std::int64_t t[3];
+    double score;
+    bool direct_zero;
+    std::uint64_t orientation;
+    double binary_overlap;
+};
+
+// One oriented kernel on the device, prepared for a fixed environment shape.
+struct KernelSlot {
+    std::uint64_t orientation {};
+    int K[3] {};
+    std::int64_t first[3] {};
+    std::uint64_t occupied {};
+    double max_z {};
+    float2* partial {};           // [z < K2][ky < L1][kx < L0], x and y transformed
+    std::int32_t* ones {};        // environment-relative offsets of kernel ones
+    double* t65 {};               // .65 * top(z) for each legal z
+    int legal[3] {};              // E - K + 1 per axis (0 when the kernel does not fit)
+    std::vector<std::uint8_t> host_cells;
+};
+
+struct PageRequest {
+    std::uint64_t slot {};
+    bool has_cursor {};
+    Candidate cursor {};
+};
+
+struct PageOutcome {
+    int status {};
+    std::vector<Candidate> page;
+    bool certified {};
+    bool threshold_pass {};
+    double max_integer_residual {};
+    double max_score_error {};
+    double excluded_score {};  // lowest approximate score of an unrescored candidate
+    std::uint64_t rescored {};
+};
+
+class Pipeline {
+public:
+    explicit Pipeline(spk_context* ctx) : ctx_(ctx) {}
+    ~Pipeline();
+
+    // Environment window (global first + shape) and lattice/container terms.
+    int set_geometry(const std::int64_t* env_first, const std::uint32_t* env_shape, const double* origin,
+                     double pitch, double container_min_z, double container_height);
+    // Device occupancy (u8, E^3): runs the exact EDT and the environment spectrum.
+    int set_occupancy(const std::uint8_t* d_occupancy);
+    // Adds an oriented kernel field (host cells, X-fastest); returns the slot.
+    int add_kernel(std::uint64_t orientation, const std::int64_t* first, const std::uint32_t* shape,
+                   const std::uint8_t* cells, double max_z, std::uint64_t& slot);
+    int pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out);
+
+    const std::uint8_t* occupancy() const { return occ_; }
+    const std::int32_t* d2() const { return d2_; }
+    const int* env_shape() const { return E_; }
+    const int* fft_shape() const { return L_; }
+    std::size_t kernels() const { return slots_.size(); }
+    const KernelSlot& slot(std::size_t i) const { return slots_[i]; }
+    double epsilon_p(const KernelSlot& s) const;
+
+private:
+    int run_orientation(const KernelSlot& s, int mode, double threshold, double cursor_floor, unsigned long long* keys,
+                        unsigned int* count, unsigned int cap, unsigned long long* tau,
+                        unsigned long long* resid);
+    double score(const KernelSlot& s, const std::int64_t* t, double p) const;
+    double approx_epsilon(const KernelSlot& s) const;
+
+    spk_context* ctx_;
+    int E_[3] {};
+    int L_[3] {};
+    std::int64_t env_first_[3] {};
+    double origin_[3] {};
+    double pitch_ {};
+    double cmin_z_ {};
+    double height_ {};
+    std::uint8_t* occ_ {};
+    std::int32_t* d2_ {};
+    float2* spectrum_ {};
+    float2* inter_ {};
+    std::size_t inter_bytes_ {};
+    const double* table_ {};
+    double z_norm_ {};  // sqrt(sum over cells of b^2 + p^2)
+    std::vector<KernelSlot> slots_;
+};
+
+}  // namespace spk

@@ -119,6 +119,66 @@ int spk_correlate_proximity(spk_context* context, const spk_correlation_spec* sp
 int spk_build_proximity(spk_context* context, const uint32_t shape[3], const uint8_t* occupied,
                         double* values);
 
+/* ---- spectral pages ---------------------------------------------------- */
+
+/* Reference: SpectralPipelineResult::RankedCandidate,
+ * engine/pack_solver/src/spectral_pipeline.hpp:26-32. */
+typedef struct spk_candidate {
+    int64_t translation[3];
+    double score;
+    int32_t direct_zero_overlap;
+    int32_t reserved;
+    uint64_t orientation_index;
+    double binary_overlap;
+} spk_candidate;
+
+/* Reference: CandidatePageQuery, spectral_pipeline.hpp:45-51.  mode 0 is
+ * CandidatePageMode::ordinary; low_overlap is not offered (SPK_INVALID_ARGUMENT). */
+typedef struct spk_page_query {
+    uint64_t orientation_index;
+    int32_t has_cursor;
+    int32_t mode;
+    spk_candidate exclusive_cursor;
+} spk_page_query;
+
+/* The environment window over which a layout is correlated
+ * (spectral_pipeline.cpp:107-140 window(), lattice, container z range). */
+typedef struct spk_page_scene {
+    int64_t environment_first[3];
+    uint32_t environment_shape[3];
+    double lattice_origin_mm[3];
+    double lattice_pitch_mm;
+    double container_min_z_mm;
+    double container_height_mm;
+} spk_page_scene;
+
+/* One oriented object field (voxelize_object window) and the oriented
+ * bounds' max z (physical_bounds.cpp:347) used by the score's top term. */
+typedef struct spk_page_kernel {
+    int64_t first[3];
+    uint32_t shape[3];
+    double object_max_z_mm;
+} spk_page_kernel;
+
+typedef struct spk_page_report {
+    double max_integer_residual;   /* largest |b - round(b)| over legal cells (FP32) */
+    double max_score_error;        /* largest |approximate - exact| score seen */
+    uint64_t rescored;             /* candidates rescored exactly */
+    int32_t certified;
+    int32_t threshold_pass;        /* an uncertified first pass was widened */
+} spk_page_report;
+
+/* One page of build_spectral_pipeline (spectral_pipeline.cpp:914-1876, page
+ * scan :1706-1824 and recount :1825-1857) for the layout whose blocked
+ * occupancy is `occupancy` (u8 over the scene window) and the oriented kernel
+ * `kernel_cells`.  Scores use the exact, correctly rounded proximity sum;
+ * page entries are ordered by (score, orientation, z, y, x).  Host pointers;
+ * `page` holds up to 32 entries. */
+int spk_spectral_page(spk_context* context, const spk_page_scene* scene, const uint8_t* occupancy,
+                      const spk_page_kernel* kernel, const uint8_t* kernel_cells,
+                      const spk_page_query* query, spk_candidate* page, uint32_t* count,
+                      spk_page_report* report);
+
 #ifdef __cplusplus
 }
 #endif

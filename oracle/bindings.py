@@ -282,3 +282,35 @@ class RefSession:
             raise RuntimeError(self.ref._error())
         n = placed.value
         return ori[:n], t[:n], scores[:n], rejected.value, seconds.value
+
+
+class OracleCandidate(ctypes.Structure):
+    _fields_ = [("t", ctypes.c_int64 * 3), ("score", ctypes.c_double), ("direct_zero", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("orientation", ctypes.c_uint64), ("binary_overlap", ctypes.c_double)]
+
+
+def oracle_page(c: C, env_first, env_shape, occupancy, proximity, kernel_first, kernel_shape, kernel, lattice,
+                max_z, cmin_z, height, orientation=0, cursor=None):
+    """The restated page (oracle_page in spk_oracle.c); cursor is (t, score, orientation) or None."""
+    ef = np.array(env_first, np.int64)
+    es = np.array(env_shape, np.uint32)
+    kf = np.array(kernel_first, np.int64)
+    ks = np.array(kernel_shape, np.uint32)
+    occ = np.ascontiguousarray(occupancy, np.uint8).reshape(-1)
+    prox = np.ascontiguousarray(proximity, np.float64).reshape(-1)
+    ker = np.ascontiguousarray(kernel, np.uint8).reshape(-1)
+    lat = np.array(lattice, np.float64)
+    page = (OracleCandidate * 32)()
+    cur = None
+    if cursor is not None:
+        cur = OracleCandidate()
+        for a in range(3):
+            cur.t[a] = int(cursor[0][a])
+        cur.score = cursor[1]
+        cur.orientation = cursor[2]
+    n = c.lib.oracle_page(_ptr(ef), _ptr(es), _ptr(occ), _ptr(prox), _ptr(kf), _ptr(ks), _ptr(ker), _ptr(lat),
+                          ctypes.c_double(max_z), ctypes.c_double(cmin_z), ctypes.c_double(height),
+                          ctypes.c_uint64(orientation), ctypes.byref(cur) if cur is not None else None, page)
+    if n < 0:
+        raise ValueError("empty kernel")
+    return [(tuple(page[i].t), page[i].score, page[i].orientation) for i in range(n)]

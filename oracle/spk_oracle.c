@@ -295,3 +295,140 @@ int oracle_build_proximity(const uint32_t* shape, const uint8_t* occupied, doubl
     free(site_start);
     return 0;
 }
+
+/* ---- spectral page (engine/pack_solver/src/spectral_pipeline.cpp:1618-1857) ----
+ * For every legal translation t = (env_first - kernel_first) + s,
+ * 0 <= s <= E - K: overlap = exact u8 overlap count; ordinary pages keep
+ * overlap == 0; score = .65 * top - .35 * prox / occ with prox the correctly
+ * rounded exact sum of the proximity values under the kernel's ones and
+ * top = (origin_z + pitch * t_z + max_z - c_min_z) / H; order by
+ * (score, orientation, z, y, x); keep 32 entries strictly after the cursor.
+ * A naive FP64 sum (error < 1e-7 here) screens candidates; every candidate
+ * within 1e-6 of the page boundary is rescored with oracle_fsum. */
+typedef struct {
+    int64_t t[3];
+    double score;
+    int32_t direct_zero;
+    int32_t reserved;
+    uint64_t orientation;
+    double binary_overlap;
+} OracleCandidate;
+
+static int oracle_rank_less(const OracleCandidate* l, const OracleCandidate* r)
+{
+    if (l->score != r->score) return l->score < r->score;
+    if (l->orientation != r->orientation) return l->orientation < r->orientation;
+    if (l->t[2] != r->t[2]) return l->t[2] < r->t[2];
+    if (l->t[1] != r->t[1]) return l->t[1] < r->t[1];
+    return l->t[0] < r->t[0];
+}
+
+static int cmp_candidates(const void* a, const void* b)
+{
+    const OracleCandidate* l = (const OracleCandidate*)a;
+    const OracleCandidate* r = (const OracleCandidate*)b;
+    return oracle_rank_less(l, r) ? -1 : oracle_rank_less(r, l) ? 1 : 0;
+}
+
+static double oracle_score(double p, uint64_t occ, int64_t tz, const double* lat, double max_z, double cmin_z,
+                           double height)
+{
+    const double mean = p / (double)occ;
+    const double world_z = lat[2] + lat[3] * (double)tz;
+    const double top = (world_z + max_z - cmin_z) / height;
+    return .65 * top - .35 * mean;
+}
+
+/* lat = {origin x, y, z, pitch}; returns the number of page entries (<= 32),
+ * or -1 for an empty kernel. */
+int oracle_page(const int64_t* env_first, const uint32_t* es, const uint8_t* occ, const double* prox,
+                const int64_t* ker_first, const uint32_t* ks, const uint8_t* ker, const double* lat, double max_z,
+                double cmin_z, double height, uint64_t orientation, const OracleCandidate* cursor,
+                OracleCandidate* page)
+{
+    int64_t nk = 0;
+    const int64_t kn = (int64_t)ks[0] * ks[1] * ks[2];
+    int64_t* ones = (int64_t*)malloc(sizeof(int64_t) * (size_t)(kn ? kn : 1));
+    for (uint32_t z = 0; z < ks[2]; ++z)
+        for (uint32_t y = 0; y < ks[1]; ++y)
+            for (uint32_t x = 0; x < ks[0]; ++x)
+                if (ker[x + (int64_t)ks[0] * (y + (int64_t)ks[1] * z)])
+                    ones[nk++] = x + (int64_t)es[0] * (y + (int64_t)es[1] * z);
+    if (nk == 0) {
+        free(ones);
+        return -1;
+    }
+    for (int a = 0; a < 3; ++a) {
+        if (es[a] < ks[a]) {
+            free(ones);
+            return 0;
+        }
+    }
+    const int64_t legal[3] = { es[0] - ks[0] + 1, es[1] - ks[1] + 1, es[2] - ks[2] + 1 };
+    const int64_t first[3] = { env_first[0] - ker_first[0], env_first[1] - ker_first[1], env_first[2] - ker_first[2] };
+    const double band = 1e-6;
+    /* screening list: every feasible candidate with its naive score */
+    int64_t cap = 1024, n = 0;
+    OracleCandidate* list = (OracleCandidate*)malloc(sizeof(OracleCandidate) * (size_t)cap);
+    double* terms = (double*)malloc(sizeof(double) * (size_t)nk);
+    for (int64_t sz = 0; sz < legal[2]; ++sz)
+        for (int64_t sy = 0; sy < legal[1]; ++sy)
+            for (int64_t sx = 0; sx < legal[0]; ++sx) {
+                const int64_t base = sx + (int64_t)es[0] * (sy + (int64_t)es[1] * sz);
+                int hit = 0;
+                double naive = 0.0;
+                for (int64_t i = 0; i < nk; ++i) {
+                    if (occ[base + ones[i]]) {
+                        hit = 1;
+                        break;
+                    }
+                    naive += prox[base + ones[i]];
+                }
+                if (hit) continue;
+                OracleCandidate c;
+                c.t[0] = first[0] + sx;
+                c.t[1] = first[1] + sy;
+                c.t[2] = first[2] + sz;
+                c.score = oracle_score(naive, (uint64_t)nk, c.t[2], lat, max_z, cmin_z, height);
+                c.direct_zero = 1;
+                c.reserved = 0;
+                c.orientation = orientation;
+                c.binary_overlap = 0.0;
+                /* drop candidates certainly at or before the cursor */
+                if (cursor && c.score < cursor->score - band) continue;
+                if (n == cap) {
+                    cap *= 2;
+                    list = (OracleCandidate*)realloc(list, sizeof(OracleCandidate) * (size_t)cap);
+                }
+                list[n++] = c;
+            }
+    qsort(list, (size_t)n, sizeof(OracleCandidate), cmp_candidates);
+    /* Walk in naive order, rescoring exactly, until 32 entries follow the
+     * cursor and the next naive score is beyond the 32nd exact one + band. */
+    OracleCandidate* kept = (OracleCandidate*)malloc(sizeof(OracleCandidate) * (size_t)(n ? n : 1));
+    int64_t m = 0;
+    double worst = INFINITY;
+    for (int64_t i = 0; i < n; ++i) {
+        if (m >= 32 && list[i].score > worst + 2 * band) break;
+        OracleCandidate c = list[i];
+        const int64_t sx = c.t[0] - first[0], sy = c.t[1] - first[1], sz = c.t[2] - first[2];
+        const int64_t base = sx + (int64_t)es[0] * (sy + (int64_t)es[1] * sz);
+        for (int64_t k = 0; k < nk; ++k) terms[k] = prox[base + ones[k]];
+        c.score = oracle_score(oracle_fsum(terms, nk), (uint64_t)nk, c.t[2], lat, max_z, cmin_z, height);
+        if (cursor && !oracle_rank_less(cursor, &c)) continue;
+        kept[m++] = c;
+        if (m >= 32) {
+            qsort(kept, (size_t)m, sizeof(OracleCandidate), cmp_candidates);
+            worst = kept[31].score;
+        }
+    }
+    qsort(kept, (size_t)m, sizeof(OracleCandidate), cmp_candidates);
+    free(list);
+    list = kept;
+    const int count = (int)(m < 32 ? m : 32);
+    for (int i = 0; i < count; ++i) page[i] = list[i];
+    free(list);
+    free(terms);
+    free(ones);
+    return count;
+}
