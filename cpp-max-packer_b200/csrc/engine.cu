@@ -1,6 +1,876 @@
-// Placement session (filled in by the pipeline engine).
+// Placement session and the stateless field entry points.
+//
+// The session is the device-resident counterpart of the reference's
+// SpectralWorkspace (engine/pack_solver/src/spectral_pipeline.cpp:227-252):
+// container blocker, BlockedField counts, occupancy, proximity, environment
+// spectrum and one kernel per catalog orientation, all kept in HBM.  A layout
+// change re-stamps only the new copy (voxelize_placed + add, :1255-1308),
+// then rebuilds occupancy (:1323-1334), the exact proximity field (:1343) and
+// the environment spectrum once for every orientation's page.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <optional>
+#include <tuple>
+#include <vector>
+
 #include "context.hpp"
+#include "edt.cuh"
+#include "fields.hpp"
+#include "geometry.hpp"
+#include "pipeline.hpp"
 
 namespace spk {
-void session_destroy(spk_context* ctx) { ctx->session = nullptr; }
+
+namespace {
+
+geo::Mesh to_mesh(const spk_mesh& m)
+{
+    geo::Mesh mesh;
+    mesh.vertices.resize(m.vertex_count);
+    mesh.triangles.resize(m.triangle_count);
+    std::memcpy(mesh.vertices.data(), m.vertices, m.vertex_count * 24);
+    std::memcpy(mesh.triangles.data(), m.triangles, m.triangle_count * 12);
+    if (!mesh.vertices.empty()) {
+        mesh.bounds = { mesh.vertices.front(), mesh.vertices.front() };
+        for (const auto& v : mesh.vertices) {
+            for (int a = 0; a < 3; ++a) {
+                mesh.bounds.min[a] = std::min(mesh.bounds.min[a], v[a]);
+                mesh.bounds.max[a] = std::max(mesh.bounds.max[a], v[a]);
+            }
+        }
+    }
+    return mesh;
+}
+
+bool valid_mesh(const spk_mesh* m)
+{
+    if (!m || !m->vertices || !m->triangles || !m->vertex_count || !m->triangle_count) {
+        return false;
+    }
+    for (std::uint64_t i = 0; i < 3 * m->triangle_count; ++i) {
+        if (m->triangles[i] >= m->vertex_count) {
+            return false;
+        }
+    }
+    return true;
+}
+
+bool valid_lattice(const double* origin, double pitch)
+{
+    return std::isfinite(origin[0]) && std::isfinite(origin[1]) && std::isfinite(origin[2]) && std::isfinite(pitch) &&
+           pitch > 0.0;
+}
+
+// expanded() (conservative_fields.cpp:169-187).
+geo::Window expanded(const geo::Window& w, std::uint64_t halo)
+{
+    geo::Window r = w;
+    for (int a = 0; a < 3; ++a) {
+        r.first[a] -= static_cast<std::int64_t>(halo);
+        r.shape[a] = static_cast<std::uint32_t>(w.shape[a] + 2 * halo);
+    }
+    return r;
+}
+
+std::uint64_t cells_of(const geo::Window& w)
+{
+    return static_cast<std::uint64_t>(w.shape[0]) * w.shape[1] * w.shape[2];
+}
+
+// voxelize_object into d_cells (device); window returned in `w`.
+int object_field(spk_context* ctx, const geo::Prepared& prepared, const double* origin, double pitch,
+                 const geo::Quat& q, geo::Window& w, std::vector<std::uint8_t>& host_cells)
+{
+    if (!geo::canonical_unit(q)) {
+        return kFieldInput;
+    }
+    geo::Placed placed;
+    if (!geo::place(prepared, { origin[0], origin[1], origin[2] }, q, placed)) {
+        return kFieldInput;
+    }
+    if (!geo::object_window(placed, origin, pitch, w)) {
+        return kFieldIndexOverflow;
+    }
+    const std::uint64_t n = cells_of(w);
+    int status = kOk;
+    auto* d = static_cast<std::uint8_t*>(device_buffer(ctx, "obj.cells", n, status));
+    if (!d) {
+        return status;
+    }
+    if ((status = raster_fill(ctx, placed, make_window(w, origin, pitch), d, true))) {
+        return status;
+    }
+    host_cells.resize(n);
+    cudaMemcpyAsync(host_cells.data(), d, n, cudaMemcpyDeviceToHost, ctx->stream);
+    return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? kOk : kCuda;
+}
+
+// voxelize_placed into d_out over `requested` (device).
+int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Window& requested, const double* origin,
+                 double pitch, const geo::Vec3& translation, const geo::Quat& q, double clearance,
+                 std::uint8_t* d_out)
+{
+    if (!geo::canonical_unit(q)) {
+        return kFieldInput;
+    }
+    std::uint64_t halo = 0;
+    if (!geo::clearance_halo(clearance, pitch, halo)) {
+        return kFieldInput;
+    }
+    const geo::Window work = expanded(requested, halo);
+    geo::Placed placed;
+    if (!geo::place(prepared, translation, q, placed)) {
+        return kFieldInput;
+    }
+    geo::Window plan;
+    const auto kind = geo::plan_placed_window(placed, work, origin, pitch, plan);
+    const std::uint64_t n = cells_of(requested);
+    if (kind == geo::PlanKind::certified_empty) {
+        cudaMemsetAsync(d_out, 0, n, ctx->stream);
+        return kOk;
+    }
+    int status = kOk;
+    auto* raw = static_cast<std::uint8_t*>(device_buffer(ctx, "placed.raw", cells_of(plan), status));
+    if (!raw) {
+        return status;
+    }
+    if ((status = raster_fill(ctx, placed, make_window(plan, origin, pitch), raw, false))) {
+        return status;
+    }
+    return dilate_crop(ctx, raw, make_window(plan, origin, pitch), halo, clearance, false, d_out,
+                       make_window(requested, origin, pitch));
+}
+
+// voxelize_container into d_out over `requested` (device).
+int container_field(spk_context* ctx, const double* box, const geo::Prepared* prepared, const geo::Window& requested,
+                    const double* origin, double pitch, double clearance, std::uint8_t* d_out)
+{
+    if (!std::isfinite(clearance) || clearance < 0.0) {
+        return kFieldInput;
+    }
+    if (box) {
+        for (int a = 0; a < 3; ++a) {
+            if (!(box[a] > 0) || !std::isfinite(box[a])) {
+                return kFieldInput;
+            }
+        }
+        return box_mask(ctx, box, clearance, make_window(requested, origin, pitch), d_out);
+    }
+    std::uint64_t halo = 0;
+    if (!geo::clearance_halo(clearance, pitch, halo)) {
+        return kFieldInput;
+    }
+    const geo::Window work = expanded(requested, halo);
+    geo::Placed placed;
+    if (!geo::place(*prepared, { 0, 0, 0 }, { 0, 0, 0, 1 }, placed)) {
+        return kFieldInput;
+    }
+    int status = kOk;
+    auto* raw = static_cast<std::uint8_t*>(device_buffer(ctx, "container.raw", cells_of(work), status));
+    if (!raw) {
+        return status;
+    }
+    if ((status = raster_fill(ctx, placed, make_window(work, origin, pitch), raw, false))) {
+        return status;
+    }
+    return dilate_crop(ctx, raw, make_window(work, origin, pitch), halo, clearance, true, d_out,
+                       make_window(requested, origin, pitch));
+}
+
+struct Copy {
+    std::uint64_t orientation;
+    std::int64_t t[3];
+};
+
+struct Session {
+    geo::Mesh object_mesh, container_mesh;
+    geo::Prepared object, container;
+    bool box {};
+    double box_mm[3] {};
+    double pair {}, wall {};
+    double origin[3] {};
+    double pitch {};
+    geo::Window env {};
+    double cmin_z {}, height {};
+    std::vector<geo::Quat> catalog;
+    std::vector<std::uint64_t> slot_of;  // orientation -> pipeline kernel slot
+    std::unique_ptr<Pipeline> pipe;
+    std::uint8_t* mask {};
+    std::uint32_t* counts {};
+    std::uint8_t* occ {};
+    std::vector<Copy> copies;
+    bool dirty { true };
+};
+
+Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
+
+int refresh(spk_context* ctx, Session& s)
+{
+    if (!s.dirty) {
+        return kOk;
+    }
+    const long long n = static_cast<long long>(cells_of(s.env));
+    int status = occupancy(ctx, s.mask, s.counts, s.occ, n);
+    if (status) {
+        return status;
+    }
+    if ((status = s.pipe->set_occupancy(s.occ))) {
+        return status;
+    }
+    s.dirty = false;
+    return kOk;
+}
+
+void to_c(const Candidate& c, spk_candidate& out)
+{
+    std::memset(&out, 0, sizeof(out));
+    std::memcpy(out.translation, c.t, sizeof(out.translation));
+    out.score = c.score;
+    out.direct_zero_overlap = c.direct_zero ? 1 : 0;
+    out.orientation_index = c.orientation;
+    out.binary_overlap = c.binary_overlap;
+}
+
+Candidate from_c(const spk_candidate& c)
+{
+    Candidate out {};
+    std::memcpy(out.t, c.translation, sizeof(out.t));
+    out.score = c.score;
+    out.direct_zero = c.direct_zero_overlap != 0;
+    out.orientation = c.orientation_index;
+    out.binary_overlap = c.binary_overlap;
+    return out;
+}
+
+bool rank_less(const Candidate& l, const Candidate& r)
+{
+    if (l.score != r.score) {
+        return l.score < r.score;
+    }
+    if (l.orientation != r.orientation) {
+        return l.orientation < r.orientation;
+    }
+    return std::tie(l.t[2], l.t[1], l.t[0]) < std::tie(r.t[2], r.t[1], r.t[0]);
+}
+
+int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const std::int64_t* t)
+{
+    if (orientation >= s.catalog.size()) {
+        return kCatalog;
+    }
+    const geo::Vec3 translation { s.origin[0] + s.pitch * static_cast<double>(t[0]),
+                                  s.origin[1] + s.pitch * static_cast<double>(t[1]),
+                                  s.origin[2] + s.pitch * static_cast<double>(t[2]) };
+    int status = kOk;
+    auto* placed = static_cast<std::uint8_t*>(device_buffer(ctx, "session.placed", cells_of(s.env), status));
+    if (!placed) {
+        return status;
+    }
+    if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[orientation], s.pair,
+                               placed))) {
+        return status;
+    }
+    if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), 1))) {
+        return status;
+    }
+    s.copies.push_back({ orientation, { t[0], t[1], t[2] } });
+    s.dirty = true;
+    return kOk;
+}
+
+int session_pages(spk_context* ctx, Session& s, const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out)
+{
+    int status = refresh(ctx, s);
+    if (status) {
+        return status;
+    }
+    return s.pipe->pages(requests, out);
+}
+
+}  // namespace
+
+void session_destroy(spk_context* ctx)
+{
+    delete session_of(ctx);
+    ctx->session = nullptr;
+}
+
 }  // namespace spk
+
+using namespace spk;
+
+extern "C" {
+
+int spk_voxelize_object(spk_context* ctx, const spk_mesh* object, const double origin[3], double pitch,
+                        const double q[4], int64_t first[3], uint32_t shape[3], uint8_t* cells, uint64_t capacity)
+{
+    try {
+        if (!ctx || !valid_mesh(object) || !origin || !q || !first || !shape || !valid_lattice(origin, pitch)) {
+            return kFieldInput;
+        }
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            return kCuda;
+        }
+        const geo::Mesh mesh = to_mesh(*object);
+        const geo::Prepared prepared = geo::prepare(mesh);
+        geo::Window w;
+        std::vector<std::uint8_t> host;
+        int status = object_field(ctx, prepared, origin, pitch, { q[0], q[1], q[2], q[3] }, w, host);
+        if (status) {
+            return status;
+        }
+        for (int a = 0; a < 3; ++a) {
+            first[a] = w.first[a];
+            shape[a] = w.shape[a];
+        }
+        if (!cells || capacity < host.size()) {
+            return kInvalidArgument;
+        }
+        std::memcpy(cells, host.data(), host.size());
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_voxelize_container(spk_context* ctx, const double box[3], const spk_mesh* container, const double origin[3],
+                           double pitch, const int64_t first[3], const uint32_t shape[3], double clearance,
+                           uint8_t* cells)
+{
+    try {
+        if (!ctx || !origin || !first || !shape || !cells || !valid_lattice(origin, pitch) ||
+            (!box && !valid_mesh(container))) {
+            return kFieldInput;
+        }
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            return kCuda;
+        }
+        geo::Window w;
+        for (int a = 0; a < 3; ++a) {
+            w.first[a] = first[a];
+            w.shape[a] = shape[a];
+        }
+        geo::Mesh mesh;
+        geo::Prepared prepared;
+        if (!box) {
+            mesh = to_mesh(*container);
+            prepared = geo::prepare(mesh);
+        }
+        int status = kOk;
+        auto* d = static_cast<std::uint8_t*>(device_buffer(ctx, "api.container", cells_of(w), status));
+        if (!d) {
+            return status;
+        }
+        if ((status = container_field(ctx, box, box ? nullptr : &prepared, w, origin, pitch, clearance, d))) {
+            return status;
+        }
+        cudaMemcpyAsync(cells, d, cells_of(w), cudaMemcpyDeviceToHost, ctx->stream);
+        return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? kOk : kCuda;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_voxelize_placed(spk_context* ctx, const spk_mesh* object, const double origin[3], double pitch,
+                        const int64_t first[3], const uint32_t shape[3], const double translation[3],
+                        const double q[4], double clearance, uint8_t* cells)
+{
+    try {
+        if (!ctx || !valid_mesh(object) || !origin || !first || !shape || !translation || !q || !cells ||
+            !valid_lattice(origin, pitch)) {
+            return kFieldInput;
+        }
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            return kCuda;
+        }
+        geo::Window w;
+        for (int a = 0; a < 3; ++a) {
+            w.first[a] = first[a];
+            w.shape[a] = shape[a];
+        }
+        const geo::Mesh mesh = to_mesh(*object);
+        const geo::Prepared prepared = geo::prepare(mesh);
+        int status = kOk;
+        auto* d = static_cast<std::uint8_t*>(device_buffer(ctx, "api.placed", cells_of(w), status));
+        if (!d) {
+            return status;
+        }
+        if ((status = placed_field(ctx, prepared, w, origin, pitch, { translation[0], translation[1], translation[2] },
+                                   { q[0], q[1], q[2], q[3] }, clearance, d))) {
+            return status;
+        }
+        cudaMemcpyAsync(cells, d, cells_of(w), cudaMemcpyDeviceToHost, ctx->stream);
+        return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? kOk : kCuda;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_oriented_bounds(const spk_mesh* object, const double q[4], double bounds[6])
+{
+    try {
+        if (!valid_mesh(object) || !q || !bounds) {
+            return kFieldInput;
+        }
+        const geo::Mesh mesh = to_mesh(*object);
+        geo::Bounds b;
+        if (!geo::oriented_bounds(mesh, { q[0], q[1], q[2], q[3] }, b)) {
+            return kFieldInput;
+        }
+        for (int a = 0; a < 3; ++a) {
+            bounds[a] = b.min[a];
+            bounds[3 + a] = b.max[a];
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_environment_window(const double bounds[6], const double origin[3], double pitch, int64_t first[3],
+                           uint32_t shape[3])
+{
+    if (!bounds || !origin || !first || !shape || !valid_lattice(origin, pitch)) {
+        return kFieldInput;
+    }
+    geo::Bounds b { { bounds[0], bounds[1], bounds[2] }, { bounds[3], bounds[4], bounds[5] } };
+    geo::Window w;
+    if (!geo::environment_window(b, origin, pitch, w)) {
+        return kFieldIndexOverflow;
+    }
+    for (int a = 0; a < 3; ++a) {
+        first[a] = w.first[a];
+        shape[a] = w.shape[a];
+    }
+    return kOk;
+}
+
+int spk_cube_catalog(double out[96])
+{
+    if (!out) {
+        return kInvalidArgument;
+    }
+    const auto cube = geo::cube_catalog();
+    for (int i = 0; i < 24; ++i) {
+        for (int k = 0; k < 4; ++k) {
+            out[4 * i + k] = cube[i][k];
+        }
+    }
+    return kOk;
+}
+
+int spk_custom_catalog(const double* in, uint64_t count, double* out, uint64_t* out_count)
+{
+    if (!in || !out || !out_count || count == 0) {
+        return kCatalog;
+    }
+    std::vector<geo::Quat> result;
+    for (std::uint64_t i = 0; i < count; ++i) {
+        const geo::Quat q { in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3] };
+        const double n = std::hypot(std::hypot(q[0], q[1]), std::hypot(q[2], q[3]));
+        if (!std::isfinite(n) || !(n > 0)) {
+            return kCatalog;
+        }
+        const auto c = geo::canonical(q);
+        if (std::find(result.begin(), result.end(), c) == result.end()) {
+            result.push_back(c);
+        }
+    }
+    for (std::size_t i = 0; i < result.size(); ++i) {
+        for (int k = 0; k < 4; ++k) {
+            out[4 * i + k] = result[i][k];
+        }
+    }
+    *out_count = result.size();
+    return kOk;
+}
+
+int spk_session_open(spk_context* ctx, const spk_session_desc* d, spk_session_info* info)
+{
+    try {
+        if (!ctx || !d || !valid_mesh(&d->object) || !valid_lattice(d->lattice_origin_mm, d->lattice_pitch_mm) ||
+            !d->orientations_xyzw || !d->orientation_count || (!d->container_is_box && !valid_mesh(&d->container))) {
+            return kFieldInput;
+        }
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            return kCuda;
+        }
+        session_destroy(ctx);
+        auto s = std::make_unique<Session>();
+        s->object_mesh = to_mesh(d->object);
+        s->object = geo::prepare(s->object_mesh);
+        s->box = d->container_is_box != 0;
+        geo::Bounds cb;
+        if (s->box) {
+            for (int a = 0; a < 3; ++a) {
+                s->box_mm[a] = d->box_mm[a];
+            }
+            cb = { { 0, 0, 0 }, { d->box_mm[0], d->box_mm[1], d->box_mm[2] } };
+        }
+        else {
+            s->container_mesh = to_mesh(d->container);
+            s->container = geo::prepare(s->container_mesh);
+            cb = s->container_mesh.bounds;
+        }
+        s->pair = d->pair_clearance_mm;
+        s->wall = d->wall_clearance_mm;
+        for (int a = 0; a < 3; ++a) {
+            s->origin[a] = d->lattice_origin_mm[a];
+        }
+        s->pitch = d->lattice_pitch_mm;
+        if (!geo::environment_window(cb, s->origin, s->pitch, s->env)) {
+            return kFieldIndexOverflow;
+        }
+        s->cmin_z = cb.min[2];
+        s->height = cb.max[2] - cb.min[2];
+        if (!std::isfinite(s->height) || s->height <= 0.) {
+            return kFieldInput;
+        }
+        for (std::uint64_t i = 0; i < d->orientation_count; ++i) {
+            s->catalog.push_back({ d->orientations_xyzw[4 * i], d->orientations_xyzw[4 * i + 1],
+                                   d->orientations_xyzw[4 * i + 2], d->orientations_xyzw[4 * i + 3] });
+        }
+        const std::uint64_t n = cells_of(s->env);
+        int status = kOk;
+        s->mask = static_cast<std::uint8_t*>(device_buffer(ctx, "session.mask", n, status));
+        s->counts = static_cast<std::uint32_t*>(device_buffer(ctx, "session.counts", n * 4, status));
+        s->occ = static_cast<std::uint8_t*>(device_buffer(ctx, "session.occ", n, status));
+        if (!s->mask || !s->counts || !s->occ) {
+            return status;
+        }
+        cudaMemsetAsync(s->counts, 0, n * 4, ctx->stream);
+        if ((status = container_field(ctx, s->box ? s->box_mm : nullptr, s->box ? nullptr : &s->container, s->env,
+                                      s->origin, s->pitch, s->wall, s->mask))) {
+            return status;
+        }
+        s->pipe = std::make_unique<Pipeline>(ctx);
+        if ((status = s->pipe->set_geometry(s->env.first, s->env.shape, s->origin, s->pitch, s->cmin_z, s->height))) {
+            return status;
+        }
+        for (std::uint64_t o = 0; o < s->catalog.size(); ++o) {
+            geo::Window w;
+            std::vector<std::uint8_t> cells;
+            if ((status = object_field(ctx, s->object, s->origin, s->pitch, s->catalog[o], w, cells))) {
+                return status;
+            }
+            geo::Bounds ob;
+            if (!geo::oriented_bounds(s->object_mesh, s->catalog[o], ob)) {
+                return kFieldInput;
+            }
+            std::uint64_t slot = 0;
+            if ((status = s->pipe->add_kernel(o, w.first, w.shape, cells.data(), ob.max[2], slot))) {
+                return status;
+            }
+            s->slot_of.push_back(slot);
+        }
+        ctx->session = s.release();
+        return spk_session_info_get(ctx, info);
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_close(spk_context* ctx)
+{
+    if (!ctx) {
+        return kInvalidArgument;
+    }
+    session_destroy(ctx);
+    return kOk;
+}
+
+int spk_session_info_get(spk_context* ctx, spk_session_info* info)
+{
+    if (!ctx || !session_of(ctx)) {
+        return kNotReady;
+    }
+    if (!info) {
+        return kOk;
+    }
+    const auto& s = *session_of(ctx);
+    for (int a = 0; a < 3; ++a) {
+        info->environment_first[a] = s.env.first[a];
+        info->environment_shape[a] = s.env.shape[a];
+        info->fft_shape[a] = static_cast<std::uint32_t>(s.pipe->fft_shape()[a]);
+    }
+    info->copies = s.copies.size();
+    info->orientations = s.catalog.size();
+    info->container_min_z_mm = s.cmin_z;
+    info->container_height_mm = s.height;
+    return kOk;
+}
+
+int spk_session_place(spk_context* ctx, uint64_t orientation, const int64_t translation[3])
+{
+    try {
+        if (!ctx || !session_of(ctx) || !translation) {
+            return kNotReady;
+        }
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            return kCuda;
+        }
+        return session_place(ctx, *session_of(ctx), orientation, translation);
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_remove_last(spk_context* ctx)
+{
+    try {
+        if (!ctx || !session_of(ctx) || session_of(ctx)->copies.empty()) {
+            return kNotReady;
+        }
+        auto& s = *session_of(ctx);
+        const Copy c = s.copies.back();
+        const geo::Vec3 translation { s.origin[0] + s.pitch * static_cast<double>(c.t[0]),
+                                      s.origin[1] + s.pitch * static_cast<double>(c.t[1]),
+                                      s.origin[2] + s.pitch * static_cast<double>(c.t[2]) };
+        int status = kOk;
+        auto* placed = static_cast<std::uint8_t*>(device_buffer(ctx, "session.placed", cells_of(s.env), status));
+        if (!placed) {
+            return status;
+        }
+        if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[c.orientation],
+                                   s.pair, placed))) {
+            return status;
+        }
+        if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), -1))) {
+            return status;
+        }
+        s.copies.pop_back();
+        s.dirty = true;
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_pages(spk_context* ctx, uint64_t n, const spk_page_query* queries, spk_candidate* pages,
+                      uint32_t* counts, spk_page_report* reports)
+{
+    try {
+        if (!ctx || !session_of(ctx)) {
+            return kNotReady;
+        }
+        if (!queries || !pages || !counts) {
+            return kInvalidArgument;
+        }
+        auto& s = *session_of(ctx);
+        std::vector<PageRequest> requests(n);
+        for (std::uint64_t i = 0; i < n; ++i) {
+            if (queries[i].orientation_index >= s.catalog.size()) {
+                return kCatalog;
+            }
+            if (queries[i].mode != 0) {
+                return kInvalidArgument;
+            }
+            requests[i].slot = s.slot_of[queries[i].orientation_index];
+            requests[i].has_cursor = queries[i].has_cursor != 0;
+            if (requests[i].has_cursor) {
+                requests[i].cursor = from_c(queries[i].exclusive_cursor);
+            }
+        }
+        std::vector<PageOutcome> out;
+        int status = session_pages(ctx, s, requests, out);
+        if (status) {
+            return status;
+        }
+        for (std::uint64_t i = 0; i < n; ++i) {
+            if (out[i].status) {
+                return out[i].status;
+            }
+            counts[i] = static_cast<std::uint32_t>(out[i].page.size());
+            for (std::size_t k = 0; k < out[i].page.size(); ++k) {
+                to_c(out[i].page[k], pages[i * kPageSize + k]);
+            }
+            if (reports) {
+                reports[i].max_integer_residual = out[i].max_integer_residual;
+                reports[i].max_score_error = out[i].max_score_error;
+                reports[i].rescored = out[i].rescored;
+                reports[i].certified = out[i].certified ? 1 : 0;
+                reports[i].threshold_pass = out[i].threshold_pass ? 1 : 0;
+            }
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
+                       int64_t* translations, double* scores)
+{
+    try {
+        if (!ctx || !session_of(ctx) || !placed) {
+            return kNotReady;
+        }
+        auto& s = *session_of(ctx);
+        *placed = 0;
+        const std::size_t O = s.catalog.size();
+        while (*placed < max_steps) {
+            std::vector<std::vector<Candidate>> pages(O);
+            std::vector<std::size_t> index(O, 0);
+            std::vector<std::optional<Candidate>> cursors(O);
+            std::vector<bool> exhausted(O, false);
+            bool admitted = false;
+            for (;;) {
+                std::vector<PageRequest> requests;
+                std::vector<std::size_t> which;
+                for (std::size_t o = 0; o < O; ++o) {
+                    if (exhausted[o] || index[o] != pages[o].size()) {
+                        continue;
+                    }
+                    PageRequest r;
+                    r.slot = s.slot_of[o];
+                    r.has_cursor = cursors[o].has_value();
+                    if (r.has_cursor) {
+                        r.cursor = *cursors[o];
+                    }
+                    requests.push_back(r);
+                    which.push_back(o);
+                }
+                if (!requests.empty()) {
+                    std::vector<PageOutcome> out;
+                    int status = session_pages(ctx, s, requests, out);
+                    if (status) {
+                        return status;
+                    }
+                    for (std::size_t k = 0; k < which.size(); ++k) {
+                        if (out[k].status) {
+                            return out[k].status;
+                        }
+                        pages[which[k]] = std::move(out[k].page);
+                        index[which[k]] = 0;
+                        if (pages[which[k]].empty()) {
+                            exhausted[which[k]] = true;
+                        }
+                    }
+                }
+                std::optional<std::size_t> chosen;
+                for (std::size_t o = 0; o < O; ++o) {
+                    if (index[o] == pages[o].size()) {
+                        continue;
+                    }
+                    if (!chosen || rank_less(pages[o][index[o]], pages[*chosen][index[*chosen]])) {
+                        chosen = o;
+                    }
+                }
+                if (!chosen) {
+                    break;
+                }
+                const Candidate c = pages[*chosen][index[*chosen]++];
+                cursors[*chosen] = c;
+                if (!c.direct_zero) {
+                    continue;
+                }
+                int status = session_place(ctx, s, c.orientation, c.t);
+                if (status) {
+                    return status;
+                }
+                if (orientations) {
+                    orientations[*placed] = c.orientation;
+                }
+                if (translations) {
+                    for (int a = 0; a < 3; ++a) {
+                        translations[3 * *placed + a] = c.t[a];
+                    }
+                }
+                if (scores) {
+                    scores[*placed] = c.score;
+                }
+                ++*placed;
+                admitted = true;
+                break;
+            }
+            if (!admitted) {
+                break;
+            }
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_field(spk_context* ctx, int kind, uint64_t orientation, int64_t first[3], uint32_t shape[3],
+                      void* out, uint64_t capacity)
+{
+    try {
+        if (!ctx || !session_of(ctx) || !first || !shape) {
+            return kNotReady;
+        }
+        auto& s = *session_of(ctx);
+        if (kind == 2) {
+            if (orientation >= s.catalog.size()) {
+                return kCatalog;
+            }
+            const auto& slot = s.pipe->slot(s.slot_of[orientation]);
+            for (int a = 0; a < 3; ++a) {
+                first[a] = slot.first[a];
+                shape[a] = static_cast<std::uint32_t>(slot.K[a]);
+            }
+            if (!out) {
+                return kOk;
+            }
+            if (capacity < slot.host_cells.size()) {
+                return kInvalidArgument;
+            }
+            std::memcpy(out, slot.host_cells.data(), slot.host_cells.size());
+            return kOk;
+        }
+        for (int a = 0; a < 3; ++a) {
+            first[a] = s.env.first[a];
+            shape[a] = s.env.shape[a];
+        }
+        if (!out) {
+            return kOk;
+        }
+        const std::uint64_t n = cells_of(s.env);
+        int status = refresh(ctx, s);
+        if (status) {
+            return status;
+        }
+        if (kind == 0 || kind == 1) {
+            if (capacity < n) {
+                return kInvalidArgument;
+            }
+            cudaMemcpyAsync(out, kind == 0 ? s.mask : s.occ, n, cudaMemcpyDeviceToHost, ctx->stream);
+        }
+        else if (kind == 3) {
+            if (capacity < n * 8) {
+                return kInvalidArgument;
+            }
+            auto* d = static_cast<double*>(device_buffer(ctx, "session.prox", n * 8, status));
+            if (!d) {
+                return status;
+            }
+            if ((status = proximity_from_d2(ctx, s.pipe->d2(), d, s.env.shape, ctx->stream))) {
+                return status;
+            }
+            cudaMemcpyAsync(out, d, n * 8, cudaMemcpyDeviceToHost, ctx->stream);
+        }
+        else {
+            return kInvalidArgument;
+        }
+        return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? kOk : kCuda;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+}  // extern "C"

@@ -1,0 +1,418 @@
+// Conservative fields on the GPU: boundary rasterisation, component labelling,
+// witness fill, clearance dilation, the analytic box container, and the
+// blocked-field stamp/unstamp with occupancy extraction.
+//
+// Reference (engine/pack_geometry/src): rasterize_boundary + run_raster_cursor
+// (validation_kernel.cpp:3248-3340, 3668-3762) tag a cell 2 when the closed
+// cell's interval box and a triangle's vertex intervals are not SAT-disjoint;
+// fill_components (conservative_fields.cpp:257-360) gives every 6-connected
+// component of non-2 cells the decision of its first cell in scan order
+// (0 void, 1 material, 3 uncertain); dilate_and_crop (:436-504) marks every
+// requested cell reached by a seed through the clearance stencil;
+// BlockedField::add/remove/blocked (:1666-1886) keep per-cell copy counts and
+// report mask || count.  The rasterised tags are an OR over faces, so one warp
+// per face with benign same-value writes reproduces them exactly; component
+// roots are the minimum linear index (= first in scan order) by union-find.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "context.hpp"
+#include "fields.hpp"
+#include "interval.cuh"
+
+namespace spk {
+
+namespace {
+
+int blocks_for(long long n, int threads)
+{
+    const long long want = (n + threads - 1) / threads;
+    return static_cast<int>(std::min<long long>(std::max<long long>(want, 1), 148LL * 32));
+}
+
+__global__ void raster_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint,
+                              const geo::FaceRange* __restrict__ ranges, int faces, FieldWindow w,
+                              std::uint8_t* __restrict__ cells, int* __restrict__ error)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= faces) {
+        return;
+    }
+    const geo::FaceRange r = ranges[warp];
+    if (r.outside) {
+        return;
+    }
+    IVec3 tri[3];
+    for (int k = 0; k < 3; ++k) {
+        tri[k] = vint[tris[3 * warp + k]];
+    }
+    const long long nx = r.last[0] - r.first[0] + 1, ny = r.last[1] - r.first[1] + 1,
+                    nz = r.last[2] - r.first[2] + 1;
+    if (nx <= 0 || ny <= 0 || nz <= 0) {
+        return;
+    }
+    const long long n = nx * ny * nz;
+    for (long long c = lane; c < n; c += 32) {
+        std::int64_t index[3];
+        index[0] = r.first[0] + c % nx;
+        index[1] = r.first[1] + (c / nx) % ny;
+        index[2] = r.first[2] + c / (nx * ny);
+        const long long flat = (index[0] - w.first[0]) +
+                               static_cast<long long>(w.shape[0]) *
+                                   ((index[1] - w.first[1]) + static_cast<long long>(w.shape[1]) * (index[2] - w.first[2]));
+        if (cells[flat] == 2) {
+            continue;
+        }
+        IVec3 box;
+        if (!grid_cell_interval(w.origin, w.pitch, index, box)) {
+            atomicOr(error, 1);
+            continue;
+        }
+        if (!triangle_box_disjoint(tri, box)) {
+            cells[flat] = 2;
+        }
+    }
+}
+
+__device__ int find_root(const int* __restrict__ parent, int i)
+{
+    for (int guard = 0; guard < (1 << 26); ++guard) {
+        const int p = parent[i];
+        if (p == i) {
+            return i;
+        }
+        i = p;
+    }
+    return i;
+}
+
+__global__ void ccl_init_kernel(const std::uint8_t* __restrict__ cells, int* __restrict__ parent, long long n)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        parent[i] = cells[i] == 2 ? -1 : static_cast<int>(i);
+    }
+}
+
+__device__ void unite(int* parent, int a, int b, int* error)
+{
+    for (int guard = 0; guard < (1 << 24); ++guard) {
+        a = find_root(parent, a);
+        b = find_root(parent, b);
+        if (a == b) {
+            return;
+        }
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        const int old = atomicMin(&parent[a], b);
+        if (old == a) {
+            return;
+        }
+        a = old;
+    }
+    atomicOr(error, 2);  // bounded retries exhausted: reported, never spun forever
+}
+
+__global__ void ccl_union_kernel(const std::uint8_t* __restrict__ cells, int* __restrict__ parent, int sx, int sy,
+                                 int sz, int* __restrict__ error)
+{
+    const long long n = static_cast<long long>(sx) * sy * sz;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        if (cells[i] == 2) {
+            continue;
+        }
+        const int x = static_cast<int>(i % sx);
+        const long long r = i / sx;
+        const int y = static_cast<int>(r % sy);
+        const int z = static_cast<int>(r / sy);
+        if (x > 0 && cells[i - 1] != 2) {
+            unite(parent, static_cast<int>(i), static_cast<int>(i - 1), error);
+        }
+        if (y > 0 && cells[i - sx] != 2) {
+            unite(parent, static_cast<int>(i), static_cast<int>(i - sx), error);
+        }
+        if (z > 0 && cells[i - static_cast<long long>(sx) * sy] != 2) {
+            unite(parent, static_cast<int>(i), static_cast<int>(i - static_cast<long long>(sx) * sy), error);
+        }
+    }
+}
+
+__global__ void ccl_compress_kernel(int* __restrict__ parent, long long n, int* __restrict__ roots,
+                                    unsigned int* __restrict__ root_count, unsigned int root_capacity)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        if (parent[i] < 0) {
+            continue;
+        }
+        const int root = find_root(parent, static_cast<int>(i));
+        parent[i] = root;
+        if (root == static_cast<int>(i)) {
+            const unsigned int slot = atomicAdd(root_count, 1u);
+            if (slot < root_capacity) {
+                roots[slot] = root;
+            }
+        }
+    }
+}
+
+__global__ void scatter_decisions_kernel(const int* __restrict__ roots, const std::uint8_t* __restrict__ values,
+                                         int count, std::uint8_t* __restrict__ root_value)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        root_value[roots[i]] = values[i];
+    }
+}
+
+__global__ void fill_kernel(std::uint8_t* __restrict__ cells, const int* __restrict__ parent,
+                            const std::uint8_t* __restrict__ root_value, long long n, int normalize)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        std::uint8_t v = cells[i];
+        if (v != 2) {
+            v = root_value[parent[i]];
+        }
+        cells[i] = normalize ? (v != 0 ? 1 : 0) : v;
+    }
+}
+
+// out[t] over `req` = OR over stencil deltas d of seed(raw[t - d]) inside `raw`.
+__global__ void dilate_kernel(const std::uint8_t* __restrict__ raw, FieldWindow rw,
+                              const int* __restrict__ stencil, int stencil_count, int invert,
+                              std::uint8_t* __restrict__ out, FieldWindow req)
+{
+    const long long n = static_cast<long long>(req.shape[0]) * req.shape[1] * req.shape[2];
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long t[3] = { req.first[0] + i % req.shape[0], req.first[1] + (i / req.shape[0]) % req.shape[1],
+                                 req.first[2] + i / (static_cast<long long>(req.shape[0]) * req.shape[1]) };
+        std::uint8_t value = 0;
+        for (int s = 0; s < stencil_count && !value; ++s) {
+            const long long sx = t[0] - stencil[3 * s] - rw.first[0];
+            const long long sy = t[1] - stencil[3 * s + 1] - rw.first[1];
+            const long long sz = t[2] - stencil[3 * s + 2] - rw.first[2];
+            if (sx < 0 || sy < 0 || sz < 0 || sx >= rw.shape[0] || sy >= rw.shape[1] || sz >= rw.shape[2]) {
+                continue;
+            }
+            const std::uint8_t v = raw[sx + rw.shape[0] * (sy + static_cast<long long>(rw.shape[1]) * sz)];
+            value = invert ? (v != 1) : (v != 0);
+        }
+        out[i] = value;
+    }
+}
+
+__global__ void box_mask_kernel(const std::uint8_t* __restrict__ ax, const std::uint8_t* __restrict__ ay,
+                                const std::uint8_t* __restrict__ az, int sx, int sy, int sz,
+                                std::uint8_t* __restrict__ mask)
+{
+    const long long n = static_cast<long long>(sx) * sy * sz;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % sx);
+        const long long r = i / sx;
+        const int y = static_cast<int>(r % sy);
+        const int z = static_cast<int>(r / sy);
+        mask[i] = (ax[x] && ay[y] && az[z]) ? 0 : 1;
+    }
+}
+
+__global__ void stamp_kernel(std::uint32_t* __restrict__ counts, const std::uint8_t* __restrict__ placed, long long n,
+                             int direction)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        if (placed[i]) {
+            counts[i] += direction > 0 ? 1u : static_cast<std::uint32_t>(-1);
+        }
+    }
+}
+
+__global__ void occupancy_kernel(const std::uint8_t* __restrict__ mask, const std::uint32_t* __restrict__ counts,
+                                 std::uint8_t* __restrict__ occ, long long n)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        occ[i] = (mask[i] != 0 || counts[i] != 0) ? 1 : 0;
+    }
+}
+
+}  // namespace
+
+int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells, bool normalize,
+                std::uint64_t* uncertain_components)
+{
+    cudaStream_t st = ctx->stream;
+    const auto& mesh = *placed.prepared->mesh;
+    const long long n = static_cast<long long>(w.shape[0]) * w.shape[1] * w.shape[2];
+    if (n >= (1LL << 31)) {
+        return kCellLimit;
+    }
+    geo::Window gw;
+    for (int a = 0; a < 3; ++a) {
+        gw.first[a] = w.first[a];
+        gw.shape[a] = w.shape[a];
+    }
+    std::vector<geo::FaceRange> ranges;
+    if (!geo::face_ranges(placed, gw, w.origin, w.pitch, ranges)) {
+        return kFieldIndexOverflow;
+    }
+    const std::size_t F = mesh.triangles.size(), V = mesh.vertices.size();
+    int status = kOk;
+    auto* d_tris = static_cast<std::uint32_t*>(device_buffer(ctx, "field.tris", F * 12, status));
+    auto* d_vint = static_cast<IVec3*>(device_buffer(ctx, "field.vint", V * sizeof(IVec3), status));
+    auto* d_ranges = static_cast<geo::FaceRange*>(device_buffer(ctx, "field.ranges", F * sizeof(geo::FaceRange), status));
+    auto* d_parent = static_cast<int*>(device_buffer(ctx, "field.parent", n * sizeof(int), status));
+    auto* d_rootv = static_cast<std::uint8_t*>(device_buffer(ctx, "field.rootv", n, status));
+    auto* d_misc = static_cast<int*>(device_buffer(ctx, "field.misc", 64, status));
+    const unsigned int root_capacity = 1u << 20;
+    auto* d_roots = static_cast<int*>(device_buffer(ctx, "field.roots", root_capacity * 4ULL, status));
+    if (!d_tris || !d_vint || !d_ranges || !d_parent || !d_rootv || !d_misc || !d_roots) {
+        return status;
+    }
+    cudaMemcpyAsync(d_tris, mesh.triangles.data(), F * 12, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_vint, placed.intervals.data(), V * sizeof(IVec3), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_ranges, ranges.data(), F * sizeof(geo::FaceRange), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(d_cells, 0, n, st);
+    cudaMemsetAsync(d_misc, 0, 64, st);
+    const int threads = 256;
+    raster_kernel<<<static_cast<unsigned>((F * 32 + threads - 1) / threads), threads, 0, st>>>(
+        d_tris, d_vint, d_ranges, static_cast<int>(F), w, d_cells, d_misc);
+    ccl_init_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, n);
+    ccl_union_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, w.shape[0], w.shape[1],
+                                                                   w.shape[2], d_misc);
+    auto* d_root_count = reinterpret_cast<unsigned int*>(d_misc + 4);
+    ccl_compress_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_parent, n, d_roots, d_root_count, root_capacity);
+    ctx->launches += 4;
+    int h_misc[8];
+    cudaMemcpyAsync(h_misc, d_misc, 32, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    if (h_misc[0] & 1) {
+        return kFieldIndexOverflow;
+    }
+    if (h_misc[0] & 2) {
+        return kKernelWait;
+    }
+    const unsigned int roots = static_cast<unsigned int>(h_misc[4]);
+    if (roots > root_capacity) {
+        return kCellLimit;
+    }
+    std::vector<int> h_roots(roots);
+    cudaMemcpy(h_roots.data(), d_roots, roots * 4ULL, cudaMemcpyDeviceToHost);
+    std::vector<std::uint8_t> values(roots);
+    std::uint64_t uncertain = 0;
+    for (unsigned int k = 0; k < roots; ++k) {
+        const long long i = h_roots[k];
+        const std::int64_t index[3] = { w.first[0] + i % w.shape[0], w.first[1] + (i / w.shape[0]) % w.shape[1],
+                                         w.first[2] + i / (static_cast<long long>(w.shape[0]) * w.shape[1]) };
+        geo::Bounds witness;
+        if (!geo::outward_grid_cell(w.origin, w.pitch, index, witness)) {
+            return kFieldIndexOverflow;
+        }
+        const auto decision = geo::classify_material_witness(placed, witness);
+        values[k] = decision == geo::Decision::indeterminate ? 3 : decision == geo::Decision::yes ? 1 : 0;
+        uncertain += decision == geo::Decision::indeterminate;
+    }
+    if (uncertain_components) {
+        *uncertain_components = uncertain;
+    }
+    if (roots) {
+        auto* d_values = static_cast<std::uint8_t*>(device_buffer(ctx, "field.values", roots, status));
+        if (!d_values) {
+            return status;
+        }
+        cudaMemcpyAsync(d_values, values.data(), roots, cudaMemcpyHostToDevice, st);
+        scatter_decisions_kernel<<<(roots + 255) / 256, 256, 0, st>>>(d_roots, d_values, static_cast<int>(roots),
+                                                                      d_rootv);
+        ctx->launches++;
+    }
+    fill_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, d_rootv, n, normalize ? 1 : 0);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,
+                double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req)
+{
+    const auto stencil = geo::make_stencil(halo, req.pitch, clearance);
+    std::vector<int> flat(3 * stencil.size());
+    for (std::size_t i = 0; i < stencil.size(); ++i) {
+        for (int a = 0; a < 3; ++a) {
+            flat[3 * i + a] = static_cast<int>(stencil[i][a]);
+        }
+    }
+    int status = kOk;
+    auto* d_stencil = static_cast<int*>(device_buffer(ctx, "field.stencil", std::max<std::size_t>(flat.size(), 3) * 4,
+                                                      status));
+    if (!d_stencil) {
+        return status;
+    }
+    cudaMemcpyAsync(d_stencil, flat.data(), flat.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+    const long long n = static_cast<long long>(req.shape[0]) * req.shape[1] * req.shape[2];
+    dilate_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(d_raw, raw, d_stencil, static_cast<int>(stencil.size()),
+                                                               invert ? 1 : 0, d_out, req);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int box_mask(spk_context* ctx, const double* dims, double clearance, const FieldWindow& w, std::uint8_t* d_mask)
+{
+    std::vector<std::uint8_t> axes[3];
+    for (int a = 0; a < 3; ++a) {
+        axes[a].resize(w.shape[a]);
+        for (std::uint32_t k = 0; k < w.shape[a]; ++k) {
+            std::int64_t index[3] = { w.first[0], w.first[1], w.first[2] };
+            index[a] = w.first[a] + k;
+            IVec3 cell;
+            if (!grid_cell_interval(w.origin, w.pitch, index, cell)) {
+                return kFieldIndexOverflow;
+            }
+            axes[a][k] = geo::analytic_box_axis_inside(w.origin[a], w.pitch, index[a], dims[a], clearance, cell, a) ? 1
+                                                                                                                   : 0;
+        }
+    }
+    int status = kOk;
+    auto* d_axes = static_cast<std::uint8_t*>(
+        device_buffer(ctx, "field.axes", static_cast<std::size_t>(w.shape[0]) + w.shape[1] + w.shape[2], status));
+    if (!d_axes) {
+        return status;
+    }
+    cudaMemcpyAsync(d_axes, axes[0].data(), w.shape[0], cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_axes + w.shape[0], axes[1].data(), w.shape[1], cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(d_axes + w.shape[0] + w.shape[1], axes[2].data(), w.shape[2], cudaMemcpyHostToDevice, ctx->stream);
+    const long long n = static_cast<long long>(w.shape[0]) * w.shape[1] * w.shape[2];
+    box_mask_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(d_axes, d_axes + w.shape[0],
+                                                                 d_axes + w.shape[0] + w.shape[1], w.shape[0],
+                                                                 w.shape[1], w.shape[2], d_mask);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int stamp(spk_context* ctx, std::uint32_t* d_counts, const std::uint8_t* d_placed, long long n, int direction)
+{
+    stamp_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(d_counts, d_placed, n, direction);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int occupancy(spk_context* ctx, const std::uint8_t* d_mask, const std::uint32_t* d_counts, std::uint8_t* d_occ,
+              long long n)
+{
+    occupancy_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(d_mask, d_counts, d_occ, n);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+}  // namespace spk

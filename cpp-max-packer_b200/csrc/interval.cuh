@@ -1,0 +1,270 @@
+// Outward-rounded FP64 interval arithmetic shared by host and device.
+//
+// Restates the raster interval primitives of the reference
+// (engine/pack_geometry/src/validation_kernel.cpp:291-324 widened/add/
+// subtract/multiply/divide, :1942-1966 interval vector ops, :2038-2079
+// triangle_box_disjoint, :2081-2100 grid_cell_interval) so that device and
+// host results are bit-identical to it: every operation is one IEEE binary64
+// round-to-nearest operation (device: __dadd_rn/__dmul_rn/... so nothing is
+// contracted into an FMA), then each bound moves one ulp outward with an
+// integer-bit nextafter; min/max keep std::min/std::max semantics.
+#pragma once
+
+#include <cstdint>
+#include <cstring>
+
+#include "common.cuh"
+
+namespace spk {
+
+SPK_HD double f_add(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dadd_rn(a, b);
+#else
+    return a + b;
+#endif
+}
+SPK_HD double f_sub(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dsub_rn(a, b);
+#else
+    return a - b;
+#endif
+}
+SPK_HD double f_mul(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __dmul_rn(a, b);
+#else
+    return a * b;
+#endif
+}
+SPK_HD double f_div(double a, double b)
+{
+#ifdef __CUDA_ARCH__
+    return __ddiv_rn(a, b);
+#else
+    return a / b;
+#endif
+}
+
+SPK_HD std::uint64_t f_bits(double v)
+{
+#ifdef __CUDA_ARCH__
+    return static_cast<std::uint64_t>(__double_as_longlong(v));
+#else
+    std::uint64_t b;
+    std::memcpy(&b, &v, 8);
+    return b;
+#endif
+}
+SPK_HD double f_from_bits(std::uint64_t b)
+{
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double(static_cast<long long>(b));
+#else
+    double v;
+    std::memcpy(&v, &b, 8);
+    return v;
+#endif
+}
+
+SPK_HD bool f_finite(double v) { return (f_bits(v) & 0x7ff0000000000000ULL) != 0x7ff0000000000000ULL; }
+
+// IEEE nextafter(v, -inf) / nextafter(v, +inf) for finite v, from the bit
+// representation (the next representable binary64 value in that direction).
+SPK_HD double next_down(double v)
+{
+    if (v != v) {
+        return v;
+    }
+    const std::uint64_t b = f_bits(v);
+    if ((b & 0x7fffffffffffffffULL) == 0) {
+        return f_from_bits(0x8000000000000001ULL);  // -denorm_min
+    }
+    if (b >> 63) {
+        return (b & 0x7fffffffffffffffULL) == 0x7ff0000000000000ULL ? v : f_from_bits(b + 1);
+    }
+    return f_from_bits(b - 1);
+}
+SPK_HD double next_up(double v)
+{
+    if (v != v) {
+        return v;
+    }
+    const std::uint64_t b = f_bits(v);
+    if ((b & 0x7fffffffffffffffULL) == 0) {
+        return f_from_bits(0x0000000000000001ULL);  // +denorm_min
+    }
+    if (b >> 63) {
+        return f_from_bits(b - 1);
+    }
+    return b == 0x7ff0000000000000ULL ? v : f_from_bits(b + 1);
+}
+
+// std::min / std::max semantics: min(a, b) = (b < a) ? b : a.
+SPK_HD double f_min(double a, double b) { return (b < a) ? b : a; }
+SPK_HD double f_max(double a, double b) { return (a < b) ? b : a; }
+
+struct Interval {
+    double low;
+    double high;
+    bool valid;
+};
+
+SPK_HD Interval point_interval(double v) { return { v, v, f_finite(v) }; }
+
+SPK_HD Interval widened(double low, double high)
+{
+    if (!f_finite(low) || !f_finite(high)) {
+        return { 0, 0, false };
+    }
+    low = next_down(low);
+    high = next_up(high);
+    return { low, high, f_finite(low) && f_finite(high) };
+}
+
+SPK_HD Interval add_interval(Interval a, Interval b)
+{
+    if (!a.valid || !b.valid) {
+        return { 0, 0, false };
+    }
+    return widened(f_add(a.low, b.low), f_add(a.high, b.high));
+}
+
+SPK_HD Interval subtract_interval(Interval a, Interval b)
+{
+    if (!a.valid || !b.valid) {
+        return { 0, 0, false };
+    }
+    return widened(f_sub(a.low, b.high), f_sub(a.high, b.low));
+}
+
+SPK_HD Interval multiply_interval(Interval a, Interval b)
+{
+    if (!a.valid || !b.valid) {
+        return { 0, 0, false };
+    }
+    const double v0 = f_mul(a.low, b.low), v1 = f_mul(a.low, b.high), v2 = f_mul(a.high, b.low),
+                 v3 = f_mul(a.high, b.high);
+    if (!f_finite(v0) || !f_finite(v1) || !f_finite(v2) || !f_finite(v3)) {
+        return { 0, 0, false };
+    }
+    // std::ranges::min_element / max_element: the first minimum / maximum.
+    double lo = v0, hi = v0;
+    if (v1 < lo) lo = v1;
+    if (v2 < lo) lo = v2;
+    if (v3 < lo) lo = v3;
+    if (hi < v1) hi = v1;
+    if (hi < v2) hi = v2;
+    if (hi < v3) hi = v3;
+    return widened(lo, hi);
+}
+
+SPK_HD Interval divide_interval(Interval n, Interval d)
+{
+    if (!n.valid || !d.valid || d.low <= 0.0) {
+        return { 0, 0, false };
+    }
+    const Interval reciprocal = widened(f_div(1.0, d.high), f_div(1.0, d.low));
+    return multiply_interval(n, reciprocal);
+}
+
+struct IVec3 {
+    Interval v[3];
+};
+
+SPK_HD IVec3 ivec_sub(const IVec3& a, const IVec3& b)
+{
+    return { { subtract_interval(a.v[0], b.v[0]), subtract_interval(a.v[1], b.v[1]),
+               subtract_interval(a.v[2], b.v[2]) } };
+}
+
+SPK_HD IVec3 ivec_cross(const IVec3& a, const IVec3& b)
+{
+    return { { subtract_interval(multiply_interval(a.v[1], b.v[2]), multiply_interval(a.v[2], b.v[1])),
+               subtract_interval(multiply_interval(a.v[2], b.v[0]), multiply_interval(a.v[0], b.v[2])),
+               subtract_interval(multiply_interval(a.v[0], b.v[1]), multiply_interval(a.v[1], b.v[0])) } };
+}
+
+SPK_HD Interval ivec_dot(const IVec3& a, const IVec3& b)
+{
+    Interval r = point_interval(0.0);
+    for (int i = 0; i < 3; ++i) {
+        r = add_interval(r, multiply_interval(a.v[i], b.v[i]));
+    }
+    return r;
+}
+
+SPK_HD bool projection_separates(const IVec3* tri, const IVec3& box, const IVec3& axis)
+{
+    Interval tp = ivec_dot(tri[0], axis);
+    for (int k = 1; k < 3; ++k) {
+        const Interval p = ivec_dot(tri[k], axis);
+        if (!p.valid) {
+            return false;
+        }
+        tp.low = f_min(tp.low, p.low);
+        tp.high = f_max(tp.high, p.high);
+    }
+    const Interval bp = ivec_dot(box, axis);
+    return tp.valid && bp.valid && (tp.high < bp.low || bp.high < tp.low);
+}
+
+// 13-axis separating-axis test of a triangle (vertex intervals) and a box.
+SPK_HD bool triangle_box_disjoint(const IVec3* tri, const IVec3& box)
+{
+    for (int a = 0; a < 3; ++a) {
+        double lo = tri[0].v[a].low, hi = tri[0].v[a].high;
+        for (int k = 1; k < 3; ++k) {
+            lo = f_min(lo, tri[k].v[a].low);
+            hi = f_max(hi, tri[k].v[a].high);
+        }
+        if (hi < box.v[a].low || box.v[a].high < lo) {
+            return true;
+        }
+    }
+    const IVec3 first = ivec_sub(tri[1], tri[0]);
+    const IVec3 second = ivec_sub(tri[2], tri[0]);
+    if (projection_separates(tri, box, ivec_cross(first, second))) {
+        return true;
+    }
+    const IVec3 edges[3] = { first, second, ivec_sub(tri[2], tri[1]) };
+    for (int e = 0; e < 3; ++e) {
+        for (int a = 0; a < 3; ++a) {
+            IVec3 axis = { { point_interval(0.0), point_interval(0.0), point_interval(0.0) } };
+            axis.v[a] = point_interval(1.0);
+            if (projection_separates(tri, box, ivec_cross(edges[e], axis))) {
+                return true;
+            }
+        }
+    }
+    return false;
+}
+
+// Outward enclosure of the closed cell `index` on the lattice; false when an
+// index is not exactly representable (|index| >= 2^53) or arithmetic overflows.
+SPK_HD bool grid_cell_interval(const double* origin, double pitch, const std::int64_t* index, IVec3& out)
+{
+    const std::int64_t limit = std::int64_t { 1 } << 53;
+    for (int a = 0; a < 3; ++a) {
+        if (index[a] < -limit || index[a] >= limit) {
+            return false;
+        }
+        const Interval low = add_interval(point_interval(origin[a]),
+                                          multiply_interval(point_interval(pitch),
+                                                            point_interval(static_cast<double>(index[a]))));
+        const Interval high = add_interval(point_interval(origin[a]),
+                                           multiply_interval(point_interval(pitch),
+                                                             point_interval(static_cast<double>(index[a] + 1))));
+        if (!low.valid || !high.valid) {
+            return false;
+        }
+        out.v[a] = { f_min(low.low, high.low), f_max(low.high, high.high), true };
+    }
+    return true;
+}
+
+}  // namespace spk

@@ -1,0 +1,166 @@
+"""Host mirror of the reference's conservative-field factories on the B200 path.
+
+Reference interface (engine/pack_geometry/include/spectrapack/geometry/
+conservative_fields.hpp:100-164): voxelize_object(geometry, lattice,
+rotation), voxelize_container(container, window, clearance) and
+voxelize_placed(geometry, window, pose, clearance) return CellFields (a
+window plus X-fastest u8 cells) or a RepresentationFailure code.  The
+functions here take the accepted local mesh directly and raise SpkError
+with the reference's code on failure.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import Optional, Sequence, Union
+
+import numpy as np
+
+from . import _lib
+from .assets import AcceptedMesh
+from .compute import Context, default_context
+
+P = ctypes.c_void_p
+
+
+class MeshC(ctypes.Structure):
+    _fields_ = [("vertices", P), ("vertex_count", ctypes.c_uint64), ("triangles", P),
+                ("triangle_count", ctypes.c_uint64)]
+
+
+@dataclasses.dataclass
+class CellField:
+    first: tuple
+    shape: tuple
+    cells: np.ndarray  # X-fastest u8
+
+    def dense(self) -> np.ndarray:
+        return self.cells.reshape(self.shape[2], self.shape[1], self.shape[0])
+
+
+def _mesh_c(mesh: AcceptedMesh):
+    v = np.ascontiguousarray(mesh.vertices, np.float64)
+    t = np.ascontiguousarray(mesh.triangles, np.uint32)
+    return MeshC(v.ctypes.data, len(v), t.ctypes.data, len(t)), (v, t)
+
+
+def _declare(lib):
+    if getattr(lib, "_geometry_declared", False):
+        return
+    M = ctypes.POINTER(MeshC)
+    lib.spk_voxelize_object.argtypes = [P, M, P, ctypes.c_double, P, P, P, P, ctypes.c_uint64]
+    lib.spk_voxelize_container.argtypes = [P, P, M, P, ctypes.c_double, P, P, ctypes.c_double, P]
+    lib.spk_voxelize_placed.argtypes = [P, M, P, ctypes.c_double, P, P, P, P, ctypes.c_double, P]
+    lib.spk_oriented_bounds.argtypes = [M, P, P]
+    lib.spk_environment_window.argtypes = [P, P, ctypes.c_double, P, P]
+    lib.spk_cube_catalog.argtypes = [P]
+    lib.spk_custom_catalog.argtypes = [P, ctypes.c_uint64, P, ctypes.POINTER(ctypes.c_uint64)]
+    lib._geometry_declared = True
+
+
+def _lib_ready():
+    lib = _lib.lib()
+    _declare(lib)
+    return lib
+
+
+def _arr(values, dtype):
+    return np.ascontiguousarray(np.array(values, dtype=dtype))
+
+
+def voxelize_object(mesh: AcceptedMesh, origin_mm: Sequence[float], pitch_mm: float, q_xyzw: Sequence[float],
+                    context: Optional[Context] = None, capacity: int = 1 << 26) -> CellField:
+    lib = _lib_ready()
+    context = context or default_context()
+    mc, keep = _mesh_c(mesh)
+    first = np.zeros(3, np.int64)
+    shape = np.zeros(3, np.uint32)
+    o, q = _arr(origin_mm, np.float64), _arr(q_xyzw, np.float64)
+    cells = np.zeros(capacity, np.uint8)
+    status = lib.spk_voxelize_object(context.handle, ctypes.byref(mc), o.ctypes.data, pitch_mm, q.ctypes.data,
+                                     first.ctypes.data, shape.ctypes.data, cells.ctypes.data, capacity)
+    _lib.check(status, "spk_voxelize_object")
+    n = int(np.prod(shape.astype(np.int64)))
+    return CellField(tuple(int(v) for v in first), tuple(int(v) for v in shape), cells[:n].copy())
+
+
+def voxelize_container(container: Union[Sequence[float], AcceptedMesh], origin_mm, pitch_mm, first, shape,
+                       wall_clearance_mm: float = 0.0, context: Optional[Context] = None) -> CellField:
+    """Box dimensions (width, depth, height) or a container mesh; 1 = blocked."""
+    lib = _lib_ready()
+    context = context or default_context()
+    f, s = _arr(first, np.int64), _arr(shape, np.uint32)
+    cells = np.zeros(int(np.prod(s.astype(np.int64))), np.uint8)
+    o = _arr(origin_mm, np.float64)
+    if isinstance(container, AcceptedMesh):
+        mc, keep = _mesh_c(container)
+        status = lib.spk_voxelize_container(context.handle, None, ctypes.byref(mc), o.ctypes.data, pitch_mm,
+                                            f.ctypes.data, s.ctypes.data, wall_clearance_mm, cells.ctypes.data)
+    else:
+        box = _arr(container, np.float64)
+        status = lib.spk_voxelize_container(context.handle, box.ctypes.data, None, o.ctypes.data, pitch_mm,
+                                            f.ctypes.data, s.ctypes.data, wall_clearance_mm, cells.ctypes.data)
+    _lib.check(status, "spk_voxelize_container")
+    return CellField(tuple(int(v) for v in f), tuple(int(v) for v in s), cells)
+
+
+def voxelize_placed(mesh: AcceptedMesh, origin_mm, pitch_mm, first, shape, translation_mm, q_xyzw,
+                    pair_clearance_mm: float = 0.0, context: Optional[Context] = None) -> CellField:
+    lib = _lib_ready()
+    context = context or default_context()
+    mc, keep = _mesh_c(mesh)
+    f, s = _arr(first, np.int64), _arr(shape, np.uint32)
+    cells = np.zeros(int(np.prod(s.astype(np.int64))), np.uint8)
+    o, t, q = _arr(origin_mm, np.float64), _arr(translation_mm, np.float64), _arr(q_xyzw, np.float64)
+    status = lib.spk_voxelize_placed(context.handle, ctypes.byref(mc), o.ctypes.data, pitch_mm, f.ctypes.data,
+                                     s.ctypes.data, t.ctypes.data, q.ctypes.data, pair_clearance_mm,
+                                     cells.ctypes.data)
+    _lib.check(status, "spk_voxelize_placed")
+    return CellField(tuple(int(v) for v in f), tuple(int(v) for v in s), cells)
+
+
+def oriented_bounds(mesh: AcceptedMesh, q_xyzw) -> np.ndarray:
+    lib = _lib_ready()
+    mc, keep = _mesh_c(mesh)
+    out = np.zeros(6, np.float64)
+    q = _arr(q_xyzw, np.float64)
+    _lib.check(lib.spk_oriented_bounds(ctypes.byref(mc), q.ctypes.data, out.ctypes.data), "spk_oriented_bounds")
+    return out
+
+
+def environment_window(bounds_mm, origin_mm, pitch_mm):
+    lib = _lib_ready()
+    b, o = _arr(bounds_mm, np.float64), _arr(origin_mm, np.float64)
+    first = np.zeros(3, np.int64)
+    shape = np.zeros(3, np.uint32)
+    _lib.check(lib.spk_environment_window(b.ctypes.data, o.ctypes.data, pitch_mm, first.ctypes.data,
+                                          shape.ctypes.data), "spk_environment_window")
+    return tuple(int(v) for v in first), tuple(int(v) for v in shape)
+
+
+def cube_catalog() -> np.ndarray:
+    lib = _lib_ready()
+    out = np.zeros((24, 4), np.float64)
+    _lib.check(lib.spk_cube_catalog(out.ctypes.data), "spk_cube_catalog")
+    return out
+
+
+def custom_catalog(quaternions) -> np.ndarray:
+    lib = _lib_ready()
+    q = np.ascontiguousarray(quaternions, np.float64).reshape(-1, 4)
+    out = np.zeros_like(q)
+    count = ctypes.c_uint64()
+    _lib.check(lib.spk_custom_catalog(q.ctypes.data, len(q), out.ctypes.data, ctypes.byref(count)),
+               "spk_custom_catalog")
+    return out[: count.value].copy()
+
+
+def hopf_catalog(count: int, seed: int) -> np.ndarray:
+    """Seeded uniform SO(3) sample (unit quaternions via Shoemake's subgroup
+    algorithm), made canonical and de-duplicated like a custom catalog."""
+    rng = np.random.default_rng(seed)
+    u1, u2, u3 = rng.random(count), rng.random(count), rng.random(count)
+    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], axis=1)
+    return custom_catalog(q)

@@ -179,6 +179,103 @@ int spk_spectral_page(spk_context* context, const spk_page_scene* scene, const u
                       const spk_page_query* query, spk_candidate* page, uint32_t* count,
                       spk_page_report* report);
 
+/* ---- geometry and conservative fields ---------------------------------- */
+
+/* An accepted solid's local mesh (reference AcceptedSolid::mesh(),
+ * engine/pack_geometry/include/spectrapack/geometry/import.hpp:184-219). */
+typedef struct spk_mesh {
+    const double* vertices;     /* vertex_count x 3 */
+    uint64_t vertex_count;
+    const uint32_t* triangles;  /* triangle_count x 3, outward winding */
+    uint64_t triangle_count;
+} spk_mesh;
+
+/* Replaces geometry::voxelize_object (conservative_fields.hpp:106-112,
+ * conservative_fields.cpp:919-1003): the object at lattice.origin with
+ * rotation q (canonical XYZW), trimmed window, cells in {0,1}.  `first` and
+ * `shape` receive the window; `cells` needs shape[0]*shape[1]*shape[2]. */
+int spk_voxelize_object(spk_context* context, const spk_mesh* object, const double origin_mm[3], double pitch_mm,
+                        const double q_xyzw[4], int64_t first[3], uint32_t shape[3], uint8_t* cells,
+                        uint64_t capacity);
+
+/* Replaces geometry::voxelize_container (conservative_fields.hpp:119-125,
+ * conservative_fields.cpp:1124-1282) over a caller window: an analytic box
+ * (box_mm non-NULL, per-cell inset test) or a closed container mesh (interior
+ * is free, the rest blocked, dilated by the wall clearance).  1 = blocked. */
+int spk_voxelize_container(spk_context* context, const double box_mm[3], const spk_mesh* container,
+                           const double origin_mm[3], double pitch_mm, const int64_t first[3],
+                           const uint32_t shape[3], double wall_clearance_mm, uint8_t* cells);
+
+/* Replaces geometry::voxelize_placed (conservative_fields.hpp:113-118,
+ * conservative_fields.cpp:1005-1122): one placed copy's pair-clearance
+ * blocker over a caller window (support-cropped raster, then dilation). */
+int spk_voxelize_placed(spk_context* context, const spk_mesh* object, const double origin_mm[3], double pitch_mm,
+                        const int64_t first[3], const uint32_t shape[3], const double translation_mm[3],
+                        const double q_xyzw[4], double pair_clearance_mm, uint8_t* cells);
+
+/* Replaces geometry::oriented_bounds (physical_bounds.cpp:347): min xyz then
+ * max xyz of the rotated mesh.  Host only. */
+int spk_oriented_bounds(const spk_mesh* object, const double q_xyzw[4], double bounds_mm[6]);
+
+/* Environment window of a container's bounds (spectral_pipeline.cpp:107-140). */
+int spk_environment_window(const double bounds_mm[6], const double origin_mm[3], double pitch_mm,
+                           int64_t first[3], uint32_t shape[3]);
+
+/* Orientation catalogs (orientation_cube.hpp:10-80, orientations.cpp:104-172):
+ * the 24 cube rotations in the reference order, or a custom list made
+ * canonical (unit, w > 0 sign rule) and de-duplicated. */
+int spk_cube_catalog(double out_xyzw[96]);
+int spk_custom_catalog(const double* in_xyzw, uint64_t count, double* out_xyzw, uint64_t* out_count);
+
+/* ---- placement session ---------------------------------------------------
+ * A device-resident SpectralWorkspace (spectral_pipeline.hpp:67-92): the
+ * container blocker, per-copy counts (BlockedField), occupancy, exact
+ * proximity, the environment spectrum and every catalog orientation's kernel
+ * stay in HBM across placement steps.  One session per context. */
+typedef struct spk_session_desc {
+    spk_mesh object;
+    int32_t container_is_box;
+    int32_t reserved;
+    double box_mm[3];
+    spk_mesh container;
+    double pair_clearance_mm;
+    double wall_clearance_mm;
+    double lattice_origin_mm[3];
+    double lattice_pitch_mm;
+    const double* orientations_xyzw;
+    uint64_t orientation_count;
+} spk_session_desc;
+
+typedef struct spk_session_info {
+    int64_t environment_first[3];
+    uint32_t environment_shape[3];
+    uint32_t fft_shape[3];
+    uint64_t copies;
+    uint64_t orientations;
+    double container_min_z_mm;
+    double container_height_mm;
+} spk_session_info;
+
+int spk_session_open(spk_context* context, const spk_session_desc* desc, spk_session_info* info);
+int spk_session_close(spk_context* context);
+int spk_session_info_get(spk_context* context, spk_session_info* info);
+/* Stamps a copy at lattice translation t with catalog orientation o
+ * (BlockedField::add of voxelize_placed at pose origin + pitch * t). */
+int spk_session_place(spk_context* context, uint64_t orientation, const int64_t translation[3]);
+/* Unstamps the most recent copy (BlockedField::remove). */
+int spk_session_remove_last(spk_context* context);
+/* Pages for n queries over the current layout; pages holds n x 32 entries. */
+int spk_session_pages(spk_context* context, uint64_t n, const spk_page_query* queries, spk_candidate* pages,
+                      uint32_t* counts, spk_page_report* reports);
+/* Greedy fill (spectral.cpp:1460-1591 page merge, direct-zero recount gate;
+ * native validation is the caller's): up to max_steps copies are placed. */
+int spk_session_greedy(spk_context* context, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
+                       int64_t* translations, double* scores);
+/* Field readback: kind 0 container blocker, 1 occupancy, 2 kernel of
+ * `orientation` (window in first/shape), 3 proximity (f64). */
+int spk_session_field(spk_context* context, int kind, uint64_t orientation, int64_t first[3], uint32_t shape[3],
+                      void* out, uint64_t capacity_bytes);
+
 #ifdef __cplusplus
 }
 #endif
