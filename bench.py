@@ -1,0 +1,323 @@
+#!/usr/bin/env python
+"""Spectral placement throughput: placements per second on the B200 path.
+
+One step is one greedy placement: every catalog orientation's page over the
+current layout (legal-translation FFT correlation of occupancy + proximity,
+fused threshold / score / top-k, exact recount and rescoring), the page merge,
+and the stamp of the chosen copy (rasterise, dilate, update counts, occupancy,
+exact EDT and the environment spectrum for the next step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+
+Under torchrun (N > 1) each rank packs an independent seeded job (replicas:
+the path has no data exchange between jobs); value = all ranks' placements /
+max over ranks of the device time.  --impl reference times the reference's
+own CPU implementation of the same per-orientation page (compiled from its
+sources, single-threaded on Linux) on the host cores.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+METRIC = "placements/s at 256^3 grid x512 orients: learned-proposal vs exhaustive GPU"
+UNIT = "placements/s"
+
+
+def pkg(name):
+    return importlib.import_module("cpp-max-packer_b200." + name)
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_bytes(session):
+    """Algorithmic HBM bytes of pass A (the per-orientation spectral pass) per launch:
+    environment spectrum read + kernel partial spectrum read + legal-z intermediate write."""
+    L0, L1, L2 = session.fft_shape
+    E = session.environment_shape
+    per = []
+    for o in range(len(session.catalog)):
+        _ = session.field("kernel", o)
+        K = session.last_window[1]
+        legal_z = E[2] - K[2] + 1
+        per.append(8 * L0 * L1 * L2 + 8 * L0 * L1 * K[2] + 8 * L0 * L1 * legal_z)
+    return float(np.mean(per))
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    compute, session_mod, workloads, lib_mod = pkg("compute"), pkg("session"), pkg("workloads"), pkg("_lib")
+    torch.cuda.set_device(local_rank)
+    ctx = compute.Context(local_rank)
+    lib = lib_mod.lib()
+    wl = workloads.WORKLOADS[args.workload](seed=2 + rank) if args.workload != "box64_cuboid_cube24" else \
+        workloads.WORKLOADS[args.workload]()
+    t0 = time.time()
+    session = session_mod.Session(wl.obj, wl.container, wl.origin, wl.pitch, wl.catalog, wl.pair_clearance,
+                                  wl.wall_clearance, context=ctx)
+    open_s = time.time() - t0
+    stream = torch.cuda.ExternalStream(lib.spk_context_stream(ctx.handle))
+    session.greedy(args.warmup)
+    dist = world > 1
+    if dist:
+        import torch.distributed as tdist
+        tdist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.launches
+    with ClockSampler(local_rank) as clocks:
+        start.record(stream)
+        placed = session.greedy(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize()
+    launches = ctx.launches - launches0
+    ms = start.elapsed_time(end)
+    n_placed = len(placed)
+    if dist:
+        t = torch.tensor([ms, float(n_placed)], device="cuda")
+        import torch.distributed as tdist
+        gathered = [torch.zeros_like(t) for _ in range(world)]
+        tdist.all_gather(gathered, t)
+        ms = max(float(g[0]) for g in gathered)
+        n_total = sum(float(g[1]) for g in gathered)
+    else:
+        n_total = float(n_placed)
+    value = n_total / (ms / 1000.0) if ms > 0 else 0.0
+
+    # Roofline of pass A (the dominant spectral pass), timed with events on the
+    # context stream around each launch during two further greedy steps.
+    lib.spk_context_set_profiling(ctx.handle, 1)
+    session.greedy(2)
+    launches_arr = np.zeros(4, np.uint64)
+    total_ms = np.zeros(4, np.float64)
+    lib.spk_context_pass_times(ctx.handle, launches_arr.ctypes.data, total_ms.ctypes.data, 4)
+    lib.spk_context_set_profiling(ctx.handle, 0)
+    hbm, peak_kind = peaks()
+    bytes_a = algorithmic_bytes(session)
+    avg_a_ms = total_ms[0] / max(int(launches_arr[0]), 1)
+    achieved = bytes_a / (avg_a_ms / 1000.0) / 1e9 if avg_a_ms > 0 else 0.0
+    pass_share = {name: round(float(total_ms[i] / max(total_ms.sum(), 1e-9)), 3)
+                  for i, name in enumerate(["spectral_z", "inverse_y", "inverse_x_epilogue", "merge_exact"])}
+
+    # End to end through the public API with host buffers: queries in, pages out.
+    e2e_steps = max(1, min(args.steps, 8))
+    O = len(session.catalog)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    e2e_placed = 0
+    for _ in range(e2e_steps):
+        pages = session.pages(range(O))
+        heads = [(p[0].score, p[0].orientation_index, p[0].translation[2], p[0].translation[1],
+                  p[0].translation[0], p[0]) for p in pages if p]
+        if not heads:
+            break
+        best = min(heads, key=lambda h: h[:5])[5]
+        session.place(best.orientation_index, best.translation)
+        e2e_placed += 1
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t1
+    query_bytes = ctypes.sizeof(pkg("pipeline").PageQueryC) * O + 8 + 24
+    page_bytes = (ctypes.sizeof(pkg("pipeline").CandidateC) * 32 + 4 + ctypes.sizeof(pkg("pipeline").PageReportC)) * O
+    e2e = {"value": round(e2e_placed / e2e_s, 4) if e2e_s > 0 else 0.0, "unit": UNIT,
+           "h2d_bytes_per_step": int(query_bytes), "d2h_bytes_per_step": int(page_bytes), "steps": e2e_placed}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl, O)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms / max(n_placed, 1), 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 spectra, fp64 exact scores, u8 fields",
+            "data": "synthetic (seeded rounded-box STL container, spherical-harmonic blob item, seeded SO(3) catalog)",
+            "config": {"workload": wl.name, "grid": list(session.environment_shape), "fft": list(session.fft_shape),
+                       "orientations": O, "object_triangles": int(len(wl.obj.triangles)),
+                       "container_triangles": int(len(wl.container.triangles)) if hasattr(wl.container, "triangles")
+                       else 0, "mode": "exhaustive", "placements_timed": n_placed,
+                       "l2": "working set above L2 (all orientations' kernel spectra stay in HBM)",
+                       "session_open_s": round(open_s, 2), "parallelism": f"replicas x{world}"},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": "pass_a_kernel (spectral z pass)",
+                         "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": round(achieved / hbm, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": int(bytes_a), "avg_launch_ms": round(avg_a_ms, 5),
+                         "pass_share": pass_share},
+            "e2e": e2e,
+            "clocks": clocks.summary(),
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    session.close()
+    ctx.close()
+
+
+def cpu_baseline(wl, orientations):
+    """The reference's own page (compiled from its sources) for one orientation
+    on one host core, extrapolated to a placement step of every orientation."""
+    try:
+        from oracle.bindings import REF_SO, Ref
+
+        if not os.path.exists(REF_SO) or not wl.object_stl:
+            return None
+        ref = Ref()
+        obj = ref.asset(wl.object_stl)
+        container = ref.asset(wl.container_stl, container=True) if wl.container_stl else tuple(wl.container)
+        session = ref.session(obj, container, wl.pair_clearance, wl.wall_clearance, wl.origin, wl.pitch,
+                              wl.catalog[:2])
+        session.page(0)  # container mask, blocked field, occupancy and proximity of the empty layout
+        t = time.perf_counter()
+        session.page(1)  # one orientation: kernel raster, two FFT correlations, scan, recount
+        per_orientation = time.perf_counter() - t
+        step = per_orientation * orientations
+        return {"value": round(1.0 / step, 6), "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"one orientation page of the same workload ({per_orientation:.1f} s, reference C++ "
+                          f"with an FP64 Bluestein FFT stand-in for pocketfft), extrapolated x{orientations} "
+                          f"orientations per placement"}
+    except Exception as exc:  # the baseline is reported, never required
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {exc}"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    workloads = pkg("workloads")
+    wl = workloads.WORKLOADS[args.workload]()
+    O = len(wl.catalog)
+    try:
+        from oracle.bindings import REF_SO, Ref
+
+        if not os.path.exists(REF_SO):
+            print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libspk_ref.so missing"}))
+            return
+        ref = Ref()
+        obj = ref.asset(wl.object_stl)
+        container = ref.asset(wl.container_stl, container=True) if wl.container_stl else tuple(wl.container)
+        session = ref.session(obj, container, wl.pair_clearance, wl.wall_clearance, wl.origin, wl.pitch,
+                              wl.catalog[: args.warmup + args.steps + 1])
+        session.page(0)
+        for o in range(1, args.warmup + 1):
+            session.page(o)
+        times = []
+        for o in range(args.warmup + 1, args.warmup + args.steps + 1):
+            t = time.perf_counter()
+            session.page(o)
+            times.append(time.perf_counter() - t)
+        per_orientation = float(np.mean(times))
+        step_s = per_orientation * O
+        value = 1.0 / step_s
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_s * 1000, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": wl.name, "orientations": O, "mode": "exhaustive"},
+            "cpu_baseline": {"value": round(value, 6), "unit": UNIT, "cores": 1, "kind": "reference",
+                             "sample": f"{args.steps} orientation pages timed (mean {per_orientation:.2f} s), "
+                                       f"x{O} orientations per placement; single-threaded as on Linux"},
+            "e2e": {"value": round(value, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+    except Exception as exc:
+        print(json.dumps({"impl": "reference", "unavailable": f"{type(exc).__name__}: {exc}"}), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="rounded256_blob_hopf512")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local_rank)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as tdist
+
+            tdist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -62,6 +62,35 @@ void spk_context_destroy(spk_context* ctx)
 
 uint64_t spk_context_launches(const spk_context* ctx) { return ctx ? ctx->launches.load() : 0; }
 
+void* spk_context_stream(const spk_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int spk_context_set_profiling(spk_context* ctx, int enabled)
+{
+    if (!ctx) {
+        return spk::kInvalidArgument;
+    }
+    spk::pass_collect(ctx);
+    ctx->profiling = enabled != 0;
+    for (int i = 0; i < 4; ++i) {
+        ctx->pass_launches[i] = 0;
+        ctx->pass_ms[i] = 0;
+    }
+    return spk::kOk;
+}
+
+int spk_context_pass_times(const spk_context* ctx, uint64_t* launches, double* total_ms, uint32_t capacity)
+{
+    if (!ctx || !launches || !total_ms) {
+        return spk::kInvalidArgument;
+    }
+    spk::pass_collect(const_cast<spk_context*>(ctx));
+    for (uint32_t i = 0; i < capacity && i < 4; ++i) {
+        launches[i] = ctx->pass_launches[i];
+        total_ms[i] = ctx->pass_ms[i];
+    }
+    return spk::kOk;
+}
+
 const char* spk_status_code(int status)
 {
     switch (status) {

@@ -31,6 +31,10 @@ struct spk_context {
     std::map<std::string, Buffer> host_buffers;  // pinned staging
     std::map<std::pair<int, int>, void*> twiddles;  // (sizeof scalar, L) -> table
     void* session {};                              // placement session (engine.cpp)
+    bool profiling {};
+    std::uint64_t pass_launches[4] {};
+    double pass_ms[4] {};
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;  // (pass, events)
 };
 
 namespace spk {
@@ -138,6 +142,39 @@ inline int poll(const spk_control* control)
         return kDeadline;
     }
     return kOk;
+}
+
+// Brackets one pass launch with events when profiling is on.
+inline std::pair<cudaEvent_t, cudaEvent_t> pass_begin(spk_context* ctx)
+{
+    std::pair<cudaEvent_t, cudaEvent_t> ev {};
+    if (ctx->profiling) {
+        cudaEventCreate(&ev.first);
+        cudaEventCreate(&ev.second);
+        cudaEventRecord(ev.first, ctx->stream);
+    }
+    return ev;
+}
+inline void pass_end(spk_context* ctx, int pass, std::pair<cudaEvent_t, cudaEvent_t> ev)
+{
+    if (ctx->profiling && ev.first) {
+        cudaEventRecord(ev.second, ctx->stream);
+        ctx->pending.push_back({ pass, ev });
+    }
+}
+inline void pass_collect(spk_context* ctx)
+{
+    for (auto& [pass, ev] : ctx->pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(ev.second) == cudaSuccess && cudaEventElapsedTime(&ms, ev.first, ev.second) ==
+                                                                 cudaSuccess) {
+            ctx->pass_ms[pass] += ms;
+            ctx->pass_launches[pass] += 1;
+        }
+        cudaEventDestroy(ev.first);
+        cudaEventDestroy(ev.second);
+    }
+    ctx->pending.clear();
 }
 
 inline std::uint32_t next_pow2(std::uint64_t v)

@@ -674,18 +674,24 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
         return status;
     }
     const std::size_t smem_a = sizeof(float2) * (L_[2] + 2 * kColumnGroup * (L_[2] + 1) + kColumnGroup * L_[2]);
+    auto ev = pass_begin(ctx_);
     pass_a_kernel<<<(L_[0] / kColumnGroup) * L_[1], 256, smem_a, st>>>(spectrum_, s.partial, inter_, L_[0], L_[1],
                                                                         L_[2], s.K[2], s.legal[2], tw2);
+    pass_end(ctx_, 0, ev);
     ctx_->launches++;
+    ev = pass_begin(ctx_);
     if (fft_axis<float>(inter_, L_[0], L_[1], s.legal[2], 1, true, 1.f, tw1, st, s.legal[1]) != cudaSuccess) {
         return kCuda;
     }
+    pass_end(ctx_, 1, ev);
     ctx_->launches++;
     const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
     const std::size_t smem_b = sizeof(float2) * (L_[0] + 2 * kB2Rows * (L_[0] + 1));
+    ev = pass_begin(ctx_);
     pass_b2_kernel<<<static_cast<unsigned>((rows + kB2Rows - 1) / kB2Rows), 32 * kB2Rows, smem_b, st>>>(
         inter_, L_[0], L_[1], s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied),
         mode, threshold, cursor_floor, keys, count, cap, tau, resid);
+    pass_end(ctx_, 2, ev);
     ctx_->launches++;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
@@ -740,9 +746,11 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         }
     }
     cudaMemcpyAsync(jobs, host_jobs.data(), R * sizeof(ExactJob), cudaMemcpyHostToDevice, st);
+    auto ev = pass_begin(ctx_);
     merge_kernel<<<R, 1024, 0, st>>>(keys, count, selected);
     exact_kernel<<<R * per, 256, 0, st>>>(selected, jobs, per, occ_, d2_, table_, E_[0], E_[1], counts_out, p_out,
                                           range_error);
+    pass_end(ctx_, 3, ev);
     ctx_->launches += 2;
     std::vector<unsigned long long> h_meta(3 * R), h_sel(static_cast<std::size_t>(R) * per);
     std::vector<long long> h_count(static_cast<std::size_t>(R) * per);

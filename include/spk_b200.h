@@ -83,6 +83,14 @@ void spk_context_destroy(spk_context* context);
 const char* spk_status_code(int status);
 /* Number of kernels this library launched on the context (all entry points). */
 uint64_t spk_context_launches(const spk_context* context);
+/* The CUDA stream (cudaStream_t) every launch of this context is queued on,
+ * so a caller can record timing events on it. */
+void* spk_context_stream(const spk_context* context);
+/* Per-pass device timing of the page pipeline (CUDA events around each pass
+ * launch when enabled): fills up to `capacity` entries of {launches, total_ms}
+ * for passes 0 spectrum-A, 1 inverse-y, 2 inverse-x+epilogue, 3 merge+exact. */
+int spk_context_set_profiling(spk_context* context, int enabled);
+int spk_context_pass_times(const spk_context* context, uint64_t* launches, double* total_ms, uint32_t capacity);
 
 /* ---- full-range correlation drop-in ----------------------------------- */
 
