@@ -282,13 +282,19 @@ int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const
     return kOk;
 }
 
-int session_pages(spk_context* ctx, Session& s, const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out)
+int session_pages_mode(spk_context* ctx, Session& s, const std::vector<PageRequest>& requests,
+                       std::vector<PageOutcome>& out, bool full)
 {
     int status = refresh(ctx, s);
     if (status) {
         return status;
     }
-    return s.pipe->pages(requests, out);
+    return s.pipe->pages(requests, out, full);
+}
+
+int session_pages(spk_context* ctx, Session& s, const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out)
+{
+    return session_pages_mode(ctx, s, requests, out, true);
 }
 
 }  // namespace
@@ -713,6 +719,10 @@ int spk_session_pages(spk_context* ctx, uint64_t n, const spk_page_query* querie
 int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
                        int64_t* translations, double* scores)
 {
+    // Page merge of spectral.cpp:1460-1591.  Pages come from the first pass;
+    // an entry is exact once its score is <= that page's exact floor.  An
+    // orientation whose next entry is not yet exact is resolved (certified
+    // page) only when its lower bound could reach the current best head.
     try {
         if (!ctx || !session_of(ctx) || !placed) {
             return kNotReady;
@@ -723,14 +733,20 @@ int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, u
         while (*placed < max_steps) {
             std::vector<std::vector<Candidate>> pages(O);
             std::vector<std::size_t> index(O, 0);
+            std::vector<double> floor(O, -INFINITY);
             std::vector<std::optional<Candidate>> cursors(O);
-            std::vector<bool> exhausted(O, false);
+            std::vector<bool> exhausted(O, false), loaded(O, false);
             bool admitted = false;
             for (;;) {
+                // (Re)load pages that are consumed: lazily, all at once.
                 std::vector<PageRequest> requests;
                 std::vector<std::size_t> which;
                 for (std::size_t o = 0; o < O; ++o) {
-                    if (exhausted[o] || index[o] != pages[o].size()) {
+                    if (exhausted[o] || (loaded[o] && index[o] != pages[o].size())) {
+                        continue;
+                    }
+                    if (loaded[o] && floor[o] == INFINITY) {
+                        exhausted[o] = true;  // a complete page was fully consumed
                         continue;
                     }
                     PageRequest r;
@@ -744,7 +760,7 @@ int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, u
                 }
                 if (!requests.empty()) {
                     std::vector<PageOutcome> out;
-                    int status = session_pages(ctx, s, requests, out);
+                    int status = session_pages_mode(ctx, s, requests, out, false);
                     if (status) {
                         return status;
                     }
@@ -752,27 +768,84 @@ int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, u
                         if (out[k].status) {
                             return out[k].status;
                         }
-                        pages[which[k]] = std::move(out[k].page);
-                        index[which[k]] = 0;
-                        if (pages[which[k]].empty()) {
-                            exhausted[which[k]] = true;
+                        const auto o = which[k];
+                        pages[o] = std::move(out[k].page);
+                        index[o] = 0;
+                        floor[o] = out[k].exact_floor;
+                        loaded[o] = true;
+                        if (pages[o].empty() && floor[o] == INFINITY) {
+                            exhausted[o] = true;
                         }
                     }
                 }
-                std::optional<std::size_t> chosen;
+                // Best exact head.
+                std::optional<std::size_t> best;
                 for (std::size_t o = 0; o < O; ++o) {
-                    if (index[o] == pages[o].size()) {
+                    if (exhausted[o] || index[o] >= pages[o].size() || pages[o][index[o]].score > floor[o]) {
                         continue;
                     }
-                    if (!chosen || rank_less(pages[o][index[o]], pages[*chosen][index[*chosen]])) {
-                        chosen = o;
+                    if (!best || rank_less(pages[o][index[o]], pages[*best][index[*best]])) {
+                        best = o;
                     }
                 }
-                if (!chosen) {
+                // Orientations whose next exact candidate could precede it.
+                std::vector<PageRequest> resolve;
+                std::vector<std::size_t> resolve_which;
+                for (std::size_t o = 0; o < O; ++o) {
+                    if (exhausted[o]) {
+                        continue;
+                    }
+                    const bool exact_next = index[o] < pages[o].size() && pages[o][index[o]].score <= floor[o];
+                    if (exact_next) {
+                        continue;
+                    }
+                    double lower = floor[o];
+                    if (index[o] < pages[o].size()) {
+                        lower = std::min(lower, pages[o][index[o]].score);
+                    }
+                    if (best && lower > pages[*best][index[*best]].score) {
+                        continue;
+                    }
+                    PageRequest r;
+                    r.slot = s.slot_of[o];
+                    r.has_cursor = cursors[o].has_value();
+                    if (r.has_cursor) {
+                        r.cursor = *cursors[o];
+                    }
+                    resolve.push_back(r);
+                    resolve_which.push_back(o);
+                }
+                if (!resolve.empty()) {
+                    std::vector<PageOutcome> out;
+                    int status = session_pages_mode(ctx, s, resolve, out, true);
+                    if (status) {
+                        return status;
+                    }
+                    for (std::size_t k = 0; k < resolve_which.size(); ++k) {
+                        if (out[k].status) {
+                            return out[k].status;
+                        }
+                        const auto o = resolve_which[k];
+                        pages[o] = std::move(out[k].page);
+                        index[o] = 0;
+                        floor[o] = out[k].page.size() == static_cast<std::size_t>(kPageSize) || !out[k].certified
+                                       ? out[k].exact_floor
+                                       : INFINITY;
+                        if (out[k].certified && floor[o] < INFINITY && !pages[o].empty()) {
+                            floor[o] = std::max(floor[o], pages[o].back().score);
+                        }
+                        loaded[o] = true;
+                        if (pages[o].empty()) {
+                            exhausted[o] = true;
+                        }
+                    }
+                    continue;
+                }
+                if (!best) {
                     break;
                 }
-                const Candidate c = pages[*chosen][index[*chosen]++];
-                cursors[*chosen] = c;
+                const Candidate c = pages[*best][index[*best]++];
+                cursors[*best] = c;
                 if (!c.direct_zero) {
                     continue;
                 }

@@ -35,6 +35,7 @@
 #include "context.hpp"
 #include "edt.cuh"
 #include "fft.cuh"
+#include "fft_reg.cuh"
 #include "pipeline.hpp"
 #include "superacc.cuh"
 
@@ -306,6 +307,173 @@ __global__ void pass_b2_kernel(const float2* __restrict__ inter, int L0, int L1,
                 const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
                 if (take && base + rank < cap) {
                     keys[base + rank] = v;
+                }
+            }
+        }
+        const unsigned long long worst = __shfl_sync(kFull, list_hi, 31);
+        if (lane == 0 && worst != kEmptyKey) {
+            atomicMin(tau, worst);
+        }
+    }
+}
+
+// ---- 256^3 grids: register four-step FFT kernels ---------------------------
+// Block = 16 lines x 16 threads per line (see fft_reg.cuh).
+
+__global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict__ spectrum,
+                                                       const float2* __restrict__ partial,
+                                                       float2* __restrict__ inter, int K2, int legal_z,
+                                                       const float2* __restrict__ twiddles)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int j = threadIdx.x & 15;  // column within the group (coalesced direction)
+    const int t = threadIdx.x >> 4;  // lane within the line
+    const int ky = blockIdx.x >> 4;
+    const long long col = ((blockIdx.x & 15) << 4) + j + 256LL * ky;
+    const long long plane = 65536;
+    float2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        const int z = 16 * n1 + t;
+        v[n1] = z < K2 ? partial[col + plane * z] : make_float2(0.f, 0.f);
+    }
+    float2* line = lines + j * kRegLine;
+    fft256<false>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+        const float2 sv = spectrum[col + plane * (t + 16 * k2)];
+        v[k2] = make_float2(sv.x * v[k2].x + sv.y * v[k2].y, sv.y * v[k2].x - sv.x * v[k2].y);
+    }
+    fft256<true>(v, line, t, tw);  // v[m2] = w(z = t + 16 m2)
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int z = t + 16 * m2;
+        if (z < legal_z) {
+            inter[col + plane * z] = v[m2];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ inter, int legal_y,
+                                                         const float2* __restrict__ twiddles)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int j = threadIdx.x & 15;
+    const int t = threadIdx.x >> 4;
+    const long long zz = blockIdx.x >> 4;
+    const long long col = ((blockIdx.x & 15) << 4) + j + 65536LL * zz;
+    float2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        v[n1] = inter[col + 256LL * (16 * n1 + t)];
+    }
+    fft256<true>(v, lines + j * kRegLine, t, tw);
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int y = t + 16 * m2;
+        if (y < legal_y) {
+            inter[col + 256LL * y] = v[m2];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
+                                                         int legal_y, int legal_z,
+                                                         const float2* __restrict__ twiddles,
+                                                         const double* __restrict__ t65, double inv_occ, int mode,
+                                                         double threshold, double cursor_floor,
+                                                         unsigned long long* __restrict__ keys,
+                                                         unsigned int* __restrict__ count, unsigned int cap,
+                                                         unsigned long long* __restrict__ tau,
+                                                         unsigned long long* __restrict__ resid)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int t = threadIdx.x & 15;  // lane within the row (coalesced direction)
+    const int j = threadIdx.x >> 4;  // row within the block
+    const int lane = threadIdx.x & 31;
+    const long long rows = static_cast<long long>(legal_y) * legal_z;
+    const long long row = static_cast<long long>(blockIdx.x) * 16 + j;
+    const bool valid = row < rows;
+    const int y = valid ? static_cast<int>(row % legal_y) : 0;
+    const int zz = valid ? static_cast<int>(row / legal_y) : 0;
+    const long long base = 256LL * (y + 256LL * zz);
+    float2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
+    }
+    fft256<true>(v, lines + j * kRegLine, t, tw);  // v[m2] = value at x = t + 16 m2
+    const double t65z = valid ? t65[zz] : 0.0;
+    const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
+    unsigned long long list_lo = kEmptyKey, list_hi = kEmptyKey;
+    float residual = 0.f;
+#pragma unroll 1
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int x = t + 16 * m2;
+        unsigned long long key = kEmptyKey;
+        bool take = false;
+        if (valid && x < legal_x) {
+            const float2 w = v[m2];
+            residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
+            if (fabsf(w.x) < 0.5f) {
+                const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
+                if (score >= cursor_floor) {
+                    key = make_key(score, row_index + x);
+                    take = mode == 1 && score <= threshold;
+                    if (mode == 1) {
+                        atomicAdd(tau, 1ULL);
+                    }
+                }
+            }
+        }
+        if (mode == 0) {
+            warp_insert(list_lo, list_hi, key, lane);
+        }
+        else {
+            const unsigned mask = __ballot_sync(kFull, take);
+            if (mask) {
+                unsigned int slot = 0;
+                if (lane == 0) {
+                    slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+                }
+                slot = __shfl_sync(kFull, slot, 0);
+                const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+                if (take && slot + rank < cap) {
+                    keys[slot + rank] = key;
+                }
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        residual = fmaxf(residual, __shfl_xor_sync(kFull, residual, o));
+    }
+    if (lane == 0 && residual > 0.f) {
+        atomicMax(resid, static_cast<unsigned long long>(__float_as_uint(residual)));
+    }
+    if (mode == 0) {
+        const unsigned long long bound = *reinterpret_cast<volatile unsigned long long*>(tau);
+        for (int half = 0; half < 2; ++half) {
+            const unsigned long long kv = half ? list_hi : list_lo;
+            const bool take = kv != kEmptyKey && kv <= bound;
+            const unsigned mask = __ballot_sync(kFull, take);
+            if (mask) {
+                unsigned int slot = 0;
+                if (lane == 0) {
+                    slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+                }
+                slot = __shfl_sync(kFull, slot, 0);
+                const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+                if (take && slot + rank < cap) {
+                    keys[slot + rank] = kv;
                 }
             }
         }
@@ -673,6 +841,22 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
     if (!tw0 || !tw1 || !tw2) {
         return status;
     }
+    if (L_[0] == 256 && L_[1] == 256 && L_[2] == 256) {
+        auto ev = pass_begin(ctx_);
+        pass_a256_kernel<<<16 * 256, 256, 0, st>>>(spectrum_, s.partial, inter_, s.K[2], s.legal[2], tw2);
+        pass_end(ctx_, 0, ev);
+        ev = pass_begin(ctx_);
+        pass_b1_256_kernel<<<16 * s.legal[2], 256, 0, st>>>(inter_, s.legal[1], tw1);
+        pass_end(ctx_, 1, ev);
+        const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
+        ev = pass_begin(ctx_);
+        pass_b2_256_kernel<<<static_cast<unsigned>((rows + 15) / 16), 256, 0, st>>>(
+            inter_, s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied), mode,
+            threshold, cursor_floor, keys, count, cap, tau, resid);
+        pass_end(ctx_, 2, ev);
+        ctx_->launches += 3;
+        return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+    }
     const std::size_t smem_a = sizeof(float2) * (L_[2] + 2 * kColumnGroup * (L_[2] + 1) + kColumnGroup * L_[2]);
     auto ev = pass_begin(ctx_);
     pass_a_kernel<<<(L_[0] / kColumnGroup) * L_[1], 256, smem_a, st>>>(spectrum_, s.partial, inter_, L_[0], L_[1],
@@ -696,7 +880,7 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
-int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out)
+int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out, bool full)
 {
     const int R = static_cast<int>(requests.size());
     out.assign(R, {});
@@ -851,6 +1035,9 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         }
         o.page = std::move(all);
         o.certified = certified;
+        o.exact_floor = excluded == kEmptyKey ? INFINITY
+                        : excluded == 0      ? -INFINITY
+                                             : decode_key_score(excluded) - eps_s[r];
         // Starting bound for a threshold pass over a page that is not full:
         // the lowest excluded approximate score, or the last rescored one.
         double start = m > 0 ? decode_key_score(h_sel[static_cast<std::size_t>(r) * per + m - 1]) : -INFINITY;
@@ -866,7 +1053,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
     // Threshold passes for every uncertified page (each recomputes that
     // orientation): collect every candidate whose approximate score is <= T,
     // rescore all of them exactly, and widen T until the page is certified.
-    for (int r = 0; r < R; ++r) {
+    for (int r = 0; r < R && full; ++r) {
         auto& o = out[r];
         if (o.status || o.certified) {
             continue;
@@ -954,18 +1141,19 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
                 all.resize(kPageSize);
             }
             const bool complete = n == total;
-            const bool full = all.size() == static_cast<std::size_t>(kPageSize);
+            const bool full_page = all.size() == static_cast<std::size_t>(kPageSize);
             o.page = std::move(all);
             o.threshold_pass = true;
-            if (complete || (full && o.page.back().score < threshold - eps_s[r])) {
+            if (complete || (full_page && o.page.back().score < threshold - eps_s[r])) {
                 o.certified = true;
+                o.exact_floor = complete ? INFINITY : threshold - eps_s[r];
                 break;
             }
             if (std::getenv("SPK_DEBUG_PAGES")) {
                 std::fprintf(stderr, "threshold r=%d T=%.17g n=%u total=%llu page=%zu\n", r, threshold, n, total,
                              o.page.size());
             }
-            threshold = full ? std::max(o.page.back().score + 2 * eps_s[r], threshold + widen) : threshold + widen;
+            threshold = full_page ? std::max(o.page.back().score + 2 * eps_s[r], threshold + widen) : threshold + widen;
             widen *= 4;
         }
         if (!o.certified && !o.status) {

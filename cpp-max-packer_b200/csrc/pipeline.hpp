@@ -13,6 +13,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <vector>
 
@@ -64,6 +65,9 @@ struct PageOutcome {
     double max_integer_residual {};
     double max_score_error {};
     double excluded_score {};  // lowest approximate score of an unrescored candidate
+    // Every candidate left out of the rescored set has an exact score above
+    // this bound; page entries scoring <= it are exact and correctly placed.
+    double exact_floor { INFINITY };
     std::uint64_t rescored {};
 };
 
@@ -80,7 +84,9 @@ public:
     // Adds an oriented kernel field (host cells, X-fastest); returns the slot.
     int add_kernel(std::uint64_t orientation, const std::int64_t* first, const std::uint32_t* shape,
                    const std::uint8_t* cells, double max_z, std::uint64_t& slot);
-    int pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out);
+    // full = true certifies whole pages (threshold passes where needed);
+    // full = false returns first-pass pages with their exact_floor only.
+    int pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out, bool full = true);
 
     const std::uint8_t* occupancy() const { return occ_; }
     const std::int32_t* d2() const { return d2_; }

@@ -73,3 +73,13 @@ def test_full_layout_has_no_candidates(gpu_ctx):
     sc = scene(2)
     sc["occ"] = np.ones_like(sc["occ"])
     assert _gpu_page(sc, ctx=gpu_ctx) == []
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_pages_on_a_256_grid_match_oracle(gpu_ctx, oracle_c, seed):
+    # E in (128, 256] on every axis selects the 256^3 register-FFT kernels.
+    sc = scene(seed, shape=(200, 180, 160), kernel_shape=(9, 7, 8), blobs=40)
+    rep = {}
+    gpu = _gpu_page(sc, orientation=1, ctx=gpu_ctx, report=rep)
+    _same(gpu, _oracle_page(oracle_c, sc, orientation=1))
+    assert rep["max_integer_residual"] < 0.25
