@@ -10,7 +10,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libspk_b200.so")
+LIB_PATH = os.environ.get("SPK_LIBRARY") or os.path.join(HERE, "libspk_b200.so")
 
 
 class SpkUnavailable(RuntimeError):

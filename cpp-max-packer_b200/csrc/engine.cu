@@ -879,6 +879,22 @@ int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, u
     }
 }
 
+int spk_session_stats(spk_context* ctx, uint64_t out[4], int reset)
+{
+    if (!ctx || !session_of(ctx) || !out) {
+        return kNotReady;
+    }
+    auto& p = *session_of(ctx)->pipe;
+    out[0] = p.stat_pages;
+    out[1] = p.stat_threshold_passes;
+    out[2] = p.stat_rescored;
+    out[3] = p.stat_first_certified;
+    if (reset) {
+        p.stat_pages = p.stat_threshold_passes = p.stat_rescored = p.stat_first_certified = 0;
+    }
+    return kOk;
+}
+
 int spk_session_field(spk_context* ctx, int kind, uint64_t orientation, int64_t first[3], uint32_t shape[3],
                       void* out, uint64_t capacity)
 {

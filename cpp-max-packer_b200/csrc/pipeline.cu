@@ -334,7 +334,13 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
     const int ky = blockIdx.x >> 4;
     const long long col = ((blockIdx.x & 15) << 4) + j + 256LL * ky;
     const long long plane = 65536;
-    float2 v[16];
+    float2 v[16], sp[16];
+    // The environment spectrum column is fetched first so its latency
+    // overlaps the forward transform of the kernel column.
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+        sp[k2] = __ldcs(spectrum + col + plane * (t + 16 * k2));
+    }
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) {
         const int z = 16 * n1 + t;
@@ -344,7 +350,7 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
     fft256<false>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) {
-        const float2 sv = spectrum[col + plane * (t + 16 * k2)];
+        const float2 sv = sp[k2];
         v[k2] = make_float2(sv.x * v[k2].x + sv.y * v[k2].y, sv.y * v[k2].x - sv.x * v[k2].y);
     }
     fft256<true>(v, line, t, tw);  // v[m2] = w(z = t + 16 m2)
@@ -411,23 +417,37 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     for (int n1 = 0; n1 < 16; ++n1) {
         v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
     }
-    fft256<true>(v, lines + j * kRegLine, t, tw);  // v[m2] = value at x = t + 16 m2
+    float2* line = lines + j * kRegLine;
+    fft256<true>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
+    // Stage the row in shared memory (each thread reads back only its own
+    // outputs) so the epilogue loop indexes it without a local-memory array.
+    __syncthreads();
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        line[t + 16 * m2] = v[m2];
+    }
     const double t65z = valid ? t65[zz] : 0.0;
     const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
     unsigned long long list_lo = kEmptyKey, list_hi = kEmptyKey;
     float residual = 0.f;
+    // Keys above the request's pruning bound cannot enter the merged top-64:
+    // drop them before the warp sort (the bound only ever decreases).
+    unsigned long long bound = mode == 0 ? *reinterpret_cast<volatile unsigned long long*>(tau) : ~0ULL;
 #pragma unroll 1
     for (int m2 = 0; m2 < 16; ++m2) {
         const int x = t + 16 * m2;
         unsigned long long key = kEmptyKey;
         bool take = false;
         if (valid && x < legal_x) {
-            const float2 w = v[m2];
+            const float2 w = line[x];
             residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
             if (fabsf(w.x) < 0.5f) {
                 const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
                 if (score >= cursor_floor) {
                     key = make_key(score, row_index + x);
+                    if (mode == 0 && key > bound) {
+                        key = kEmptyKey;
+                    }
                     take = mode == 1 && score <= threshold;
                     if (mode == 1) {
                         atomicAdd(tau, 1ULL);
@@ -1035,6 +1055,9 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         }
         o.page = std::move(all);
         o.certified = certified;
+        ++stat_pages;
+        stat_first_certified += certified ? 1 : 0;
+        stat_rescored += o.rescored;
         o.exact_floor = excluded == kEmptyKey ? INFINITY
                         : excluded == 0      ? -INFINITY
                                              : decode_key_score(excluded) - eps_s[r];
@@ -1081,6 +1104,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
                                           cap, meta, meta + 1))) {
                 return status;
             }
+            ++stat_threshold_passes;
             unsigned long long h[3];
             cudaMemcpyAsync(h, meta, 24, cudaMemcpyDeviceToHost, st);
             if (cudaStreamSynchronize(st) != cudaSuccess) {

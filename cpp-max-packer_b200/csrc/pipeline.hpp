@@ -119,6 +119,11 @@ private:
     const double* table_ {};
     double z_norm_ {};  // sqrt(sum over cells of b^2 + p^2)
     std::vector<KernelSlot> slots_;
+
+public:
+    // Work counters since the last reset: first-pass pages, threshold passes,
+    // candidates rescored exactly, pages certified by the first pass.
+    std::uint64_t stat_pages {}, stat_threshold_passes {}, stat_rescored {}, stat_first_certified {};
 };
 
 }  // namespace spk

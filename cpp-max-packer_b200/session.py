@@ -50,6 +50,7 @@ def _declare(lib):
                                       P, ctypes.POINTER(PageReportC)]
     lib.spk_session_greedy.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), P, P, P]
     lib.spk_session_field.argtypes = [P, ctypes.c_int, ctypes.c_uint64, P, P, P, ctypes.c_uint64]
+    lib.spk_session_stats.argtypes = [P, P, ctypes.c_int]
     lib._session_declared = True
 
 
@@ -150,6 +151,12 @@ class Session:
         out = [Placement(int(ori[i]), tuple(int(v) for v in t[i]), float(scores[i])) for i in range(placed.value)]
         self.placements += out
         return out
+
+    def stats(self, reset: bool = False) -> dict:
+        out = np.zeros(4, np.uint64)
+        _lib.check(self.lib.spk_session_stats(self.context.handle, out.ctypes.data, int(reset)), "spk_session_stats")
+        return {"pages": int(out[0]), "threshold_passes": int(out[1]), "rescored": int(out[2]),
+                "first_pass_certified": int(out[3])}
 
     def field(self, kind: str, orientation: int = 0) -> np.ndarray:
         code = {"container": 0, "occupancy": 1, "kernel": 2, "proximity": 3}[kind]

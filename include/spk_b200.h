@@ -279,6 +279,10 @@ int spk_session_pages(spk_context* context, uint64_t n, const spk_page_query* qu
  * native validation is the caller's): up to max_steps copies are placed. */
 int spk_session_greedy(spk_context* context, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
                        int64_t* translations, double* scores);
+/* Work counters of the session's page pipeline since open or the last reset:
+ * out[0] first-pass pages, [1] threshold passes, [2] exactly rescored
+ * candidates, [3] pages certified by the first pass. */
+int spk_session_stats(spk_context* context, uint64_t out[4], int reset);
 /* Field readback: kind 0 container blocker, 1 occupancy, 2 kernel of
  * `orientation` (window in first/shape), 3 proximity (f64). */
 int spk_session_field(spk_context* context, int kind, uint64_t orientation, int64_t first[3], uint32_t shape[3],
