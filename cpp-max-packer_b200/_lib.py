@@ -90,6 +90,7 @@ def _declare(h):
                                      ctypes.POINTER(Control), ctypes.c_uint32, P, ctypes.c_uint64,
                                      ctypes.POINTER(CorrelationResultC)]
     h.spk_build_proximity.argtypes = [P, P, P, P]
+    h.spk_build_proximity_static.argtypes = [P, P, P, P]
 
 
 def status_code(status: int) -> str:

@@ -233,3 +233,22 @@ def build_proximity(shape: Sequence[int], occupied, context: Optional[Context] =
         return None
     check(status, "spk_build_proximity")
     return out
+
+
+STATIC_PROXIMITY_MAX_AXIS = 64
+
+
+def build_proximity_static(shape: Sequence[int], occupied_device_ptr: int, values_device_ptr: int,
+                           stream: int = 0) -> None:
+    """Allocation-free build_proximity for callers that cannot allocate device
+    memory (no context, no cudaMalloc/cudaFree): `occupied_device_ptr` (u8)
+    and `values_device_ptr` (f64) are caller-owned device addresses, `stream`
+    a cudaStream_t handle (0 = default stream).  The scratch is one static
+    device array shared by every call: fields larger than 64 cells on any axis
+    raise SPK_SCRATCH_LIMIT, the first call on a device sets the array up and
+    must come before any stream capture, and overlapping calls race."""
+    s = np.array(shape, np.uint32)
+    status = lib().spk_build_proximity_static(ctypes.c_void_p(stream or None), s.ctypes.data_as(ctypes.c_void_p),
+                                              ctypes.c_void_p(occupied_device_ptr),
+                                              ctypes.c_void_p(values_device_ptr))
+    check(status, "spk_build_proximity_static")

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "context.hpp"
@@ -209,7 +210,123 @@ int proximity_from_d2(spk_context* ctx, const std::int32_t* d_d2, double* d_out,
 
 }  // namespace spk
 
+// ---- allocation-free variant ---------------------------------------------
+//
+// Scratch for fields of up to kStaticCells cells lives in one file-scope
+// device array: squared distances, the three line scratch arrays and the
+// exp(-sqrt(v)/2) table.  Host code never uses the array's name as a device
+// address; the address comes from cudaGetSymbolAddress, looked up once per
+// device with that device current.
+namespace spk {
+namespace {
+
+constexpr std::uint32_t kStaticCells = SPK_STATIC_PROXIMITY_MAX_CELLS;
+constexpr std::int32_t kStaticMaxD2 = 3 * 63 * 63;  // largest d2 of a field whose cells fit (64^3)
+constexpr std::size_t kStaticD2 = 0;
+constexpr std::size_t kStaticLineF = kStaticD2 + 4ULL * kStaticCells;
+constexpr std::size_t kStaticSiteQ = kStaticLineF + 4ULL * kStaticCells;
+constexpr std::size_t kStaticSiteS = kStaticSiteQ + 4ULL * kStaticCells;
+constexpr std::size_t kStaticTable = kStaticSiteS + 8ULL * kStaticCells;
+constexpr std::size_t kStaticBytes = kStaticTable + 8ULL * (kStaticMaxD2 + 1);
+
+__device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_scratch_address[kMaxDevices] {};
+std::mutex g_scratch_mutex;
+double g_table_host[kStaticMaxD2 + 1];
+bool g_table_ready = false;
+
+// Largest d2 any shape with at most kStaticCells cells can produce.
+std::int32_t static_max_d2(const std::uint32_t* shape) { return max_squared_distance(shape); }
+
+int static_setup(int device, cudaStream_t stream, unsigned char*& base)
+{
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (device < 0 || device >= kMaxDevices) {
+        return kInvalidArgument;
+    }
+    if (g_scratch_address[device]) {
+        base = g_scratch_address[device];
+        return kOk;
+    }
+    void* address = nullptr;
+    if (cudaGetSymbolAddress(&address, g_static_scratch) != cudaSuccess || !address) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    if (!g_table_ready) {
+        for (std::int32_t v = 0; v <= kStaticMaxD2; ++v) {
+            g_table_host[v] = std::exp(-std::sqrt(static_cast<double>(v)) / 2.);
+        }
+        g_table_ready = true;
+    }
+    auto* bytes = static_cast<unsigned char*>(address);
+    if (cudaMemcpyAsync(bytes + kStaticTable, g_table_host, sizeof(g_table_host), cudaMemcpyHostToDevice, stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    g_scratch_address[device] = bytes;
+    base = bytes;
+    return kOk;
+}
+
+}  // namespace
+
+}  // namespace spk
+
 using namespace spk;
+
+extern "C" int spk_build_proximity_static(void* stream_handle, const uint32_t shape[3], const uint8_t* occupied,
+                                          double* values)
+{
+    try {
+        if (!shape || !occupied || !values) {
+            return kInvalidArgument;
+        }
+        if (!proximity_shape_supported(shape)) {
+            return kProximityShape;
+        }
+        if (shape[0] > 64 || shape[1] > 64 || shape[2] > 64) {
+            return kScratchLimit;  // beyond the static scratch: 64 cells per axis
+        }
+        const unsigned long long n = static_cast<unsigned long long>(shape[0]) * shape[1] * shape[2];
+        if (n > kStaticCells || static_max_d2(shape) > kStaticMaxD2) {
+            return kScratchLimit;
+        }
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess) {
+            cudaGetLastError();
+            return kCuda;
+        }
+        auto stream = static_cast<cudaStream_t>(stream_handle);
+        unsigned char* base = nullptr;
+        int status = static_setup(device, stream, base);
+        if (status) {
+            return status;
+        }
+        auto* d2 = reinterpret_cast<std::int32_t*>(base + kStaticD2);
+        auto* line_f = reinterpret_cast<std::int32_t*>(base + kStaticLineF);
+        auto* site_q = reinterpret_cast<std::int32_t*>(base + kStaticSiteQ);
+        auto* site_s = reinterpret_cast<long long*>(base + kStaticSiteS);
+        const auto* table = reinterpret_cast<const double*>(base + kStaticTable);
+        const long long cells = static_cast<long long>(n);
+        // Every scratch cell that is read is written first in this call.
+        edt_init_kernel<<<blocks_for(cells, 256), 256, 0, stream>>>(occupied, d2, cells);
+        for (int axis = 0; axis != 3; ++axis) {
+            const long long lines = cells / shape[axis];
+            edt_pass_kernel<<<static_cast<unsigned>((lines + 127) / 128), 128, 0, stream>>>(
+                d2, line_f, site_q, site_s, shape[0], shape[1], shape[2], axis);
+        }
+        proximity_gather_kernel<<<blocks_for(cells, 256), 256, 0, stream>>>(d2, table, values, cells);
+        return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+    }
+    catch (...) {
+        return kCuda;
+    }
+}
 
 extern "C" int spk_build_proximity(spk_context* ctx, const uint32_t shape[3], const uint8_t* occupied, double* values)
 {

@@ -127,6 +127,27 @@ int spk_correlate_proximity(spk_context* context, const spk_correlation_spec* sp
 int spk_build_proximity(spk_context* context, const uint32_t shape[3], const uint8_t* occupied,
                         double* values);
 
+/* Largest field spk_build_proximity_static accepts: 64 cells per axis. */
+#define SPK_STATIC_PROXIMITY_MAX_AXIS 64u
+#define SPK_STATIC_PROXIMITY_MAX_CELLS (64u * 64u * 64u)
+
+/* No counterpart in the reference: an allocation-free spk_build_proximity
+ * for callers that cannot allocate device memory - for example a host engine
+ * whose device memory is owned by its own pool allocator, or a steady-state
+ * loop that must not allocate (an allocation can block on the device and can
+ * fail).  It takes no context and calls no cudaMalloc, cudaFree or other
+ * allocating routine: the scratch (squared distances, line scratch and the
+ * exp(-sqrt(d2)/2) table, about 5.3 MB) is one static device array that
+ * every GPU which loads this library holds until the process exits.
+ * `occupied` (u8) and `values` (f64) are device pointers the caller owns;
+ * `stream` is a cudaStream_t (NULL = default stream) on the current device.
+ * Fields with more than SPK_STATIC_PROXIMITY_MAX_AXIS (64) cells on any axis
+ * are rejected with SPK_SCRATCH_LIMIT (status 25).  The first call on a device looks up the array's address
+ * and uploads the table (synchronising `stream`); make that first call before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU (concurrent streams) race, so serialise them. */
+int spk_build_proximity_static(void* stream, const uint32_t shape[3], const uint8_t* occupied, double* values);
+
 /* ---- spectral pages ---------------------------------------------------- */
 
 /* Reference: SpectralPipelineResult::RankedCandidate,
