@@ -22,6 +22,7 @@
 #include "fields.hpp"
 #include "geometry.hpp"
 #include "pipeline.hpp"
+#include "proposal.hpp"
 
 namespace spk {
 
@@ -204,6 +205,8 @@ struct Session {
     std::uint8_t* occ {};
     std::vector<Copy> copies;
     bool dirty { true };
+    __nv_bfloat16* items {};  // every orientation's kernel pooled to 32^3 (proposal input)
+    bool items_ready {};
 };
 
 Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
@@ -295,6 +298,268 @@ int session_pages_mode(spk_context* ctx, Session& s, const std::vector<PageReque
 int session_pages(spk_context* ctx, Session& s, const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out)
 {
     return session_pages_mode(ctx, s, requests, out, true);
+}
+
+// One greedy placement over the orientations in `subset`: the page merge of
+// spectral.cpp:1460-1591.  Pages come from the first pass; an entry is exact
+// once its score is <= that page's exact floor.  An orientation whose next
+// entry is not yet exact is resolved (certified page) only when its lower
+// bound could reach the current best head.  Places the chosen candidate and
+// returns it in `chosen` (empty when no orientation of the subset admits one).
+int greedy_step(spk_context* ctx, Session& s, const std::vector<std::size_t>& subset, std::optional<Candidate>& chosen)
+{
+    chosen.reset();
+    const std::size_t O = s.catalog.size();
+    std::vector<bool> active(O, false);
+    for (std::size_t o : subset) {
+        if (o < O) {
+            active[o] = true;
+        }
+    }
+    std::vector<std::vector<Candidate>> pages(O);
+    std::vector<std::size_t> index(O, 0);
+    std::vector<double> floor(O, -INFINITY);
+    std::vector<std::optional<Candidate>> cursors(O);
+    std::vector<bool> exhausted(O, false), loaded(O, false);
+    for (std::size_t o = 0; o < O; ++o) {
+        exhausted[o] = !active[o];
+    }
+    for (;;) {
+        // (Re)load pages that are consumed: lazily, all at once.
+        std::vector<PageRequest> requests;
+        std::vector<std::size_t> which;
+        for (std::size_t o = 0; o < O; ++o) {
+            if (exhausted[o] || (loaded[o] && index[o] != pages[o].size())) {
+                continue;
+            }
+            if (loaded[o] && floor[o] == INFINITY) {
+                exhausted[o] = true;  // a complete page was fully consumed
+                continue;
+            }
+            PageRequest r;
+            r.slot = s.slot_of[o];
+            r.has_cursor = cursors[o].has_value();
+            if (r.has_cursor) {
+                r.cursor = *cursors[o];
+            }
+            requests.push_back(r);
+            which.push_back(o);
+        }
+        if (!requests.empty()) {
+            std::vector<PageOutcome> out;
+            int status = session_pages_mode(ctx, s, requests, out, false);
+            if (status) {
+                return status;
+            }
+            for (std::size_t k = 0; k < which.size(); ++k) {
+                if (out[k].status) {
+                    return out[k].status;
+                }
+                const auto o = which[k];
+                pages[o] = std::move(out[k].page);
+                index[o] = 0;
+                floor[o] = out[k].exact_floor;
+                loaded[o] = true;
+                if (pages[o].empty() && floor[o] == INFINITY) {
+                    exhausted[o] = true;
+                }
+            }
+        }
+        // Best exact head.
+        std::optional<std::size_t> best;
+        for (std::size_t o = 0; o < O; ++o) {
+            if (exhausted[o] || index[o] >= pages[o].size() || pages[o][index[o]].score > floor[o]) {
+                continue;
+            }
+            if (!best || rank_less(pages[o][index[o]], pages[*best][index[*best]])) {
+                best = o;
+            }
+        }
+        // Orientations whose next exact candidate could precede it.
+        std::vector<PageRequest> resolve;
+        std::vector<std::size_t> resolve_which;
+        for (std::size_t o = 0; o < O; ++o) {
+            if (exhausted[o]) {
+                continue;
+            }
+            const bool exact_next = index[o] < pages[o].size() && pages[o][index[o]].score <= floor[o];
+            if (exact_next) {
+                continue;
+            }
+            double lower = floor[o];
+            if (index[o] < pages[o].size()) {
+                lower = std::min(lower, pages[o][index[o]].score);
+            }
+            if (best && lower > pages[*best][index[*best]].score) {
+                continue;
+            }
+            PageRequest r;
+            r.slot = s.slot_of[o];
+            r.has_cursor = cursors[o].has_value();
+            if (r.has_cursor) {
+                r.cursor = *cursors[o];
+            }
+            resolve.push_back(r);
+            resolve_which.push_back(o);
+        }
+        if (!resolve.empty()) {
+            std::vector<PageOutcome> out;
+            int status = session_pages_mode(ctx, s, resolve, out, true);
+            if (status) {
+                return status;
+            }
+            for (std::size_t k = 0; k < resolve_which.size(); ++k) {
+                if (out[k].status) {
+                    return out[k].status;
+                }
+                const auto o = resolve_which[k];
+                pages[o] = std::move(out[k].page);
+                index[o] = 0;
+                floor[o] = out[k].page.size() == static_cast<std::size_t>(kPageSize) || !out[k].certified
+                               ? out[k].exact_floor
+                               : INFINITY;
+                if (out[k].certified && floor[o] < INFINITY && !pages[o].empty()) {
+                    floor[o] = std::max(floor[o], pages[o].back().score);
+                }
+                loaded[o] = true;
+                if (pages[o].empty()) {
+                    exhausted[o] = true;
+                }
+            }
+            continue;
+        }
+        if (!best) {
+            break;
+        }
+        const Candidate c = pages[*best][index[*best]++];
+        cursors[*best] = c;
+        if (!c.direct_zero) {
+            continue;
+        }
+        int status = session_place(ctx, s, c.orientation, c.t);
+        if (status) {
+            return status;
+        }
+        chosen = c;
+        break;
+    }
+    return kOk;
+}
+
+void record(const Candidate& c, std::uint64_t i, std::uint64_t* orientations, std::int64_t* translations,
+            double* scores)
+{
+    if (orientations) {
+        orientations[i] = c.orientation;
+    }
+    if (translations) {
+        for (int a = 0; a < 3; ++a) {
+            translations[3 * i + a] = c.t[a];
+        }
+    }
+    if (scores) {
+        scores[i] = c.score;
+    }
+}
+
+// Pools every orientation's kernel field to the proposal grid (once per session).
+int session_items(spk_context* ctx, Session& s)
+{
+    if (s.items_ready) {
+        return kOk;
+    }
+    const std::size_t O = s.catalog.size();
+    int status = kOk;
+    s.items = static_cast<__nv_bfloat16*>(
+        device_buffer(ctx, "session.items", O * kProposalVoxels * sizeof(__nv_bfloat16), status));
+    if (!s.items) {
+        return status;
+    }
+    std::size_t most = 1;
+    for (std::size_t o = 0; o < O; ++o) {
+        most = std::max(most, s.pipe->slot(s.slot_of[o]).host_cells.size());
+    }
+    auto* cells = static_cast<std::uint8_t*>(device_buffer(ctx, "session.item_cells", most * O, status));
+    if (!cells) {
+        return status;
+    }
+    for (std::size_t o = 0; o < O; ++o) {
+        const KernelSlot& k = s.pipe->slot(s.slot_of[o]);
+        cudaMemcpyAsync(cells + o * most, k.host_cells.data(), k.host_cells.size(), cudaMemcpyHostToDevice,
+                        ctx->stream);
+        if ((status = pool_item(ctx, cells + o * most, k.K, s.items + o * kProposalVoxels))) {
+            return status;
+        }
+    }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    s.items_ready = true;
+    return kOk;
+}
+
+// Pools the current occupancy to the proposal grid.
+int session_crop(spk_context* ctx, Session& s, __nv_bfloat16*& crop)
+{
+    int status = refresh(ctx, s);
+    if (status) {
+        return status;
+    }
+    crop = static_cast<__nv_bfloat16*>(
+        device_buffer(ctx, "session.crop", kProposalVoxels * sizeof(__nv_bfloat16), status));
+    if (!crop) {
+        return status;
+    }
+    const int shape[3] = { static_cast<int>(s.env.shape[0]), static_cast<int>(s.env.shape[1]),
+                           static_cast<int>(s.env.shape[2]) };
+    return pool_occupancy(ctx, s.occ, shape, crop);
+}
+
+// Network score of every orientation for the current layout (host copy).
+int session_predict(spk_context* ctx, Session& s, ProposalNet* net, std::vector<float>& pred)
+{
+    int status = session_items(ctx, s);
+    __nv_bfloat16* crop {};
+    if (!status) {
+        status = session_crop(ctx, s, crop);
+    }
+    if (status) {
+        return status;
+    }
+    const std::size_t O = s.catalog.size();
+    auto* d = static_cast<float*>(device_buffer(ctx, "session.pred", O * sizeof(float), status));
+    if (!d) {
+        return status;
+    }
+    if ((status = proposal_predict(ctx, net, static_cast<std::uint32_t>(O), crop, nullptr, s.items, nullptr, d))) {
+        return status;
+    }
+    pred.resize(O);
+    cudaMemcpyAsync(pred.data(), d, O * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    return kOk;
+}
+
+// The k orientations with the lowest predicted score (ties: lower index).
+std::vector<std::size_t> top_k(const std::vector<float>& pred, std::size_t k)
+{
+    std::vector<std::size_t> order(pred.size());
+    for (std::size_t o = 0; o < order.size(); ++o) {
+        order[o] = o;
+    }
+    k = std::min(k, order.size());
+    std::partial_sort(order.begin(), order.begin() + static_cast<std::ptrdiff_t>(k), order.end(),
+                      [&](std::size_t a, std::size_t b) {
+                          const float pa = std::isnan(pred[a]) ? INFINITY : pred[a];
+                          const float pb = std::isnan(pred[b]) ? INFINITY : pred[b];
+                          return pa != pb ? pa < pb : a < b;
+                      });
+    order.resize(k);
+    return order;
 }
 
 }  // namespace
@@ -719,158 +984,157 @@ int spk_session_pages(spk_context* ctx, uint64_t n, const spk_page_query* querie
 int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
                        int64_t* translations, double* scores)
 {
-    // Page merge of spectral.cpp:1460-1591.  Pages come from the first pass;
-    // an entry is exact once its score is <= that page's exact floor.  An
-    // orientation whose next entry is not yet exact is resolved (certified
-    // page) only when its lower bound could reach the current best head.
     try {
         if (!ctx || !session_of(ctx) || !placed) {
             return kNotReady;
         }
         auto& s = *session_of(ctx);
         *placed = 0;
-        const std::size_t O = s.catalog.size();
+        std::vector<std::size_t> all(s.catalog.size());
+        for (std::size_t o = 0; o < all.size(); ++o) {
+            all[o] = o;
+        }
         while (*placed < max_steps) {
-            std::vector<std::vector<Candidate>> pages(O);
-            std::vector<std::size_t> index(O, 0);
-            std::vector<double> floor(O, -INFINITY);
-            std::vector<std::optional<Candidate>> cursors(O);
-            std::vector<bool> exhausted(O, false), loaded(O, false);
-            bool admitted = false;
-            for (;;) {
-                // (Re)load pages that are consumed: lazily, all at once.
-                std::vector<PageRequest> requests;
-                std::vector<std::size_t> which;
-                for (std::size_t o = 0; o < O; ++o) {
-                    if (exhausted[o] || (loaded[o] && index[o] != pages[o].size())) {
-                        continue;
-                    }
-                    if (loaded[o] && floor[o] == INFINITY) {
-                        exhausted[o] = true;  // a complete page was fully consumed
-                        continue;
-                    }
-                    PageRequest r;
-                    r.slot = s.slot_of[o];
-                    r.has_cursor = cursors[o].has_value();
-                    if (r.has_cursor) {
-                        r.cursor = *cursors[o];
-                    }
-                    requests.push_back(r);
-                    which.push_back(o);
-                }
-                if (!requests.empty()) {
-                    std::vector<PageOutcome> out;
-                    int status = session_pages_mode(ctx, s, requests, out, false);
-                    if (status) {
-                        return status;
-                    }
-                    for (std::size_t k = 0; k < which.size(); ++k) {
-                        if (out[k].status) {
-                            return out[k].status;
-                        }
-                        const auto o = which[k];
-                        pages[o] = std::move(out[k].page);
-                        index[o] = 0;
-                        floor[o] = out[k].exact_floor;
-                        loaded[o] = true;
-                        if (pages[o].empty() && floor[o] == INFINITY) {
-                            exhausted[o] = true;
-                        }
-                    }
-                }
-                // Best exact head.
-                std::optional<std::size_t> best;
-                for (std::size_t o = 0; o < O; ++o) {
-                    if (exhausted[o] || index[o] >= pages[o].size() || pages[o][index[o]].score > floor[o]) {
-                        continue;
-                    }
-                    if (!best || rank_less(pages[o][index[o]], pages[*best][index[*best]])) {
-                        best = o;
-                    }
-                }
-                // Orientations whose next exact candidate could precede it.
-                std::vector<PageRequest> resolve;
-                std::vector<std::size_t> resolve_which;
-                for (std::size_t o = 0; o < O; ++o) {
-                    if (exhausted[o]) {
-                        continue;
-                    }
-                    const bool exact_next = index[o] < pages[o].size() && pages[o][index[o]].score <= floor[o];
-                    if (exact_next) {
-                        continue;
-                    }
-                    double lower = floor[o];
-                    if (index[o] < pages[o].size()) {
-                        lower = std::min(lower, pages[o][index[o]].score);
-                    }
-                    if (best && lower > pages[*best][index[*best]].score) {
-                        continue;
-                    }
-                    PageRequest r;
-                    r.slot = s.slot_of[o];
-                    r.has_cursor = cursors[o].has_value();
-                    if (r.has_cursor) {
-                        r.cursor = *cursors[o];
-                    }
-                    resolve.push_back(r);
-                    resolve_which.push_back(o);
-                }
-                if (!resolve.empty()) {
-                    std::vector<PageOutcome> out;
-                    int status = session_pages_mode(ctx, s, resolve, out, true);
-                    if (status) {
-                        return status;
-                    }
-                    for (std::size_t k = 0; k < resolve_which.size(); ++k) {
-                        if (out[k].status) {
-                            return out[k].status;
-                        }
-                        const auto o = resolve_which[k];
-                        pages[o] = std::move(out[k].page);
-                        index[o] = 0;
-                        floor[o] = out[k].page.size() == static_cast<std::size_t>(kPageSize) || !out[k].certified
-                                       ? out[k].exact_floor
-                                       : INFINITY;
-                        if (out[k].certified && floor[o] < INFINITY && !pages[o].empty()) {
-                            floor[o] = std::max(floor[o], pages[o].back().score);
-                        }
-                        loaded[o] = true;
-                        if (pages[o].empty()) {
-                            exhausted[o] = true;
-                        }
-                    }
-                    continue;
-                }
-                if (!best) {
-                    break;
-                }
-                const Candidate c = pages[*best][index[*best]++];
-                cursors[*best] = c;
-                if (!c.direct_zero) {
-                    continue;
-                }
-                int status = session_place(ctx, s, c.orientation, c.t);
-                if (status) {
+            std::optional<Candidate> chosen;
+            int status = greedy_step(ctx, s, all, chosen);
+            if (status) {
+                return status;
+            }
+            if (!chosen) {
+                break;
+            }
+            record(*chosen, *placed, orientations, translations, scores);
+            ++*placed;
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_features(spk_context* ctx, float* crop, float* items)
+{
+    try {
+        if (!ctx || !session_of(ctx)) {
+            return kNotReady;
+        }
+        auto& s = *session_of(ctx);
+        const std::size_t O = s.catalog.size();
+        int status = kOk;
+        std::vector<std::uint16_t> host;
+        if (crop) {
+            __nv_bfloat16* d {};
+            if ((status = session_crop(ctx, s, d))) {
+                return status;
+            }
+            host.resize(kProposalVoxels);
+            cudaMemcpyAsync(host.data(), d, kProposalVoxels * 2, cudaMemcpyDeviceToHost, ctx->stream);
+            if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+                return kCuda;
+            }
+            for (int v = 0; v < kProposalVoxels; ++v) {
+                const std::uint32_t bits = static_cast<std::uint32_t>(host[v]) << 16;
+                std::memcpy(crop + v, &bits, 4);
+            }
+        }
+        if (items) {
+            if ((status = session_items(ctx, s))) {
+                return status;
+            }
+            host.resize(O * kProposalVoxels);
+            cudaMemcpyAsync(host.data(), s.items, host.size() * 2, cudaMemcpyDeviceToHost, ctx->stream);
+            if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+                return kCuda;
+            }
+            for (std::size_t v = 0; v < host.size(); ++v) {
+                const std::uint32_t bits = static_cast<std::uint32_t>(host[v]) << 16;
+                std::memcpy(items + v, &bits, 4);
+            }
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_propose(spk_context* ctx, spk_proposal* proposal, uint32_t k, uint64_t* orientations,
+                        float* predictions)
+{
+    try {
+        if (!ctx || !session_of(ctx)) {
+            return kNotReady;
+        }
+        ProposalNet* net = proposal_net(proposal);
+        if (!net || (k && !orientations)) {
+            return kInvalidArgument;
+        }
+        auto& s = *session_of(ctx);
+        std::vector<float> pred;
+        int status = session_predict(ctx, s, net, pred);
+        if (status) {
+            return status;
+        }
+        if (predictions) {
+            std::memcpy(predictions, pred.data(), pred.size() * sizeof(float));
+        }
+        const auto best = top_k(pred, k);
+        for (std::size_t i = 0; i < best.size(); ++i) {
+            orientations[i] = best[i];
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_greedy_proposed(spk_context* ctx, spk_proposal* proposal, uint32_t k, uint64_t max_steps,
+                                uint64_t* placed, uint64_t* orientations, int64_t* translations, double* scores,
+                                uint64_t* fallbacks)
+{
+    try {
+        if (!ctx || !session_of(ctx) || !placed) {
+            return kNotReady;
+        }
+        ProposalNet* net = proposal_net(proposal);
+        if (!net || k == 0) {
+            return kInvalidArgument;
+        }
+        auto& s = *session_of(ctx);
+        *placed = 0;
+        if (fallbacks) {
+            *fallbacks = 0;
+        }
+        std::vector<std::size_t> all(s.catalog.size());
+        for (std::size_t o = 0; o < all.size(); ++o) {
+            all[o] = o;
+        }
+        std::vector<float> pred;
+        while (*placed < max_steps) {
+            int status = session_predict(ctx, s, net, pred);
+            if (status) {
+                return status;
+            }
+            std::optional<Candidate> chosen;
+            if ((status = greedy_step(ctx, s, top_k(pred, k), chosen))) {
+                return status;
+            }
+            if (!chosen) {
+                // No proposed orientation admits a copy: the exhaustive step decides.
+                if ((status = greedy_step(ctx, s, all, chosen))) {
                     return status;
                 }
-                if (orientations) {
-                    orientations[*placed] = c.orientation;
+                if (!chosen) {
+                    break;
                 }
-                if (translations) {
-                    for (int a = 0; a < 3; ++a) {
-                        translations[3 * *placed + a] = c.t[a];
-                    }
+                if (fallbacks) {
+                    ++*fallbacks;
                 }
-                if (scores) {
-                    scores[*placed] = c.score;
-                }
-                ++*placed;
-                admitted = true;
-                break;
             }
-            if (!admitted) {
-                break;
-            }
+            record(*chosen, *placed, orientations, translations, scores);
+            ++*placed;
         }
         return kOk;
     }

@@ -1,0 +1,1132 @@
+// Learned orientation proposal network on the fifth-generation tensor cores.
+//
+// Every convolution (forward, data gradient, weight gradient) is one
+// implicit GEMM D[M x N] = sum_k A[m, k] B[n, k] on tcgen05:
+//   forward : m = output voxel, n = cout, k = (tap, cin)   A K-major, B K-major
+//   data    : m = input voxel,  n = cin,  k = (tap, cout)  A K-major, B MN-major
+//   weight  : m = (tap, cin),   n = cout, k = output voxel A MN-major, B MN-major
+// The CTA's 128 threads gather the im2col operand tiles straight from the
+// channels-last activations into shared memory (one 16-byte unit = 8 channels
+// of one voxel), a single thread issues the MMAs into a TMEM accumulator of
+// 128 lanes x N FP32 columns, and tcgen05.commit on a per-stage mbarrier
+// releases each of the four shared-memory stages for the next gather.  The
+// epilogue reads TMEM with tcgen05.ld: bias + ReLU + BF16 store (forward),
+// ReLU mask + BF16 store (data gradient), FP32 partial sums per K split
+// (weight gradient; the row after the last (tap, cin) row is all ones, so its
+// sums are the bias gradient).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/spk_b200.h"
+#include "context.hpp"
+#include "proposal.hpp"
+#include "umma.cuh"
+
+struct spk_proposal;
+
+namespace spk {
+
+using bf16 = __nv_bfloat16;
+
+namespace {
+
+constexpr int kRows = 128;   // MMA M = TMEM lanes
+constexpr int kKC = 32;      // K elements per stage (two MMA K-steps of 16)
+constexpr int kStages = 4;
+constexpr int kThreads = 128;
+constexpr int kStepBytesA = kRows * 16 * 2;  // one K-step block of A: 128 rows x 16 bf16
+enum Mode { kFwd = 0, kData = 1, kWeight = 2 };
+
+int cin_pad(int cin) { return cin < 8 ? 8 : cin; }
+
+struct ConvArgs {
+    const bf16* x;       // layer input, [batch][s_in^3][cin]
+    const bf16* dy;      // gradient of this layer's pre-activation, [batch][s_out^3][cout]
+    const bf16* w;       // [cout][kw], kw = 27 * cin_pad, zero padded channels
+    const float* bias;   // [cout]
+    bf16* out;           // forward: [batch][s_out^3][cout]; data: [batch][s_in^3][cin]
+    float* partial;      // weight: [split][cout][kw + 1]
+    unsigned* error;
+    int batch, s_in, s_out, stride, cin, cinp, cout, kw;
+    long long m_total;   // GEMM rows
+    long long k_total;   // GEMM K
+    int chunks_per_split;
+    int relu_mask;       // data gradient: multiply by (x > 0)
+};
+
+struct Vox {
+    int n, z, y, x;
+};
+
+__device__ __forceinline__ Vox decode(long long m, int s)
+{
+    Vox v;
+    v.x = static_cast<int>(m % s);
+    long long t = m / s;
+    v.y = static_cast<int>(t % s);
+    t /= s;
+    v.z = static_cast<int>(t % s);
+    v.n = static_cast<int>(t / s);
+    return v;
+}
+
+__device__ __forceinline__ uint4 load_channels(const bf16* voxel, int cin, int ci0)
+{
+    if (cin >= 8) {
+        return __ldg(reinterpret_cast<const uint4*>(voxel + ci0));
+    }
+    const unsigned short* h = reinterpret_cast<const unsigned short*>(voxel);
+    unsigned w[4] = { 0u, 0u, 0u, 0u };
+    for (int i = 0; i < cin; ++i) {
+        w[i >> 1] |= static_cast<unsigned>(__ldg(h + i)) << (16 * (i & 1));
+    }
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+__device__ __forceinline__ void put(unsigned char* base, std::uint32_t offset, uint4 v)
+{
+    *reinterpret_cast<uint4*>(base + offset) = v;
+}
+
+// Input voxel of output voxel `o` through tap (kz, ky, kx); false outside.
+__device__ __forceinline__ bool tap_input(const Vox& o, int tap, int stride, int s_in, int& iz, int& iy, int& ix)
+{
+    const int kz = tap / 9, ky = (tap / 3) % 3, kx = tap % 3;
+    iz = o.z * stride + kz - 1;
+    iy = o.y * stride + ky - 1;
+    ix = o.x * stride + kx - 1;
+    return iz >= 0 && iz < s_in && iy >= 0 && iy < s_in && ix >= 0 && ix < s_in;
+}
+
+// Output voxel that reads input voxel `p` through tap; false when none.
+__device__ __forceinline__ bool tap_output(const Vox& p, int tap, int stride, int s_out, int& qz, int& qy, int& qx)
+{
+    const int kz = tap / 9, ky = (tap / 3) % 3, kx = tap % 3;
+    const int az = p.z + 1 - kz, ay = p.y + 1 - ky, ax = p.x + 1 - kx;
+    if (az < 0 || ay < 0 || ax < 0 || az % stride || ay % stride || ax % stride) {
+        return false;
+    }
+    qz = az / stride;
+    qy = ay / stride;
+    qx = ax / stride;
+    return qz < s_out && qy < s_out && qx < s_out;
+}
+
+template <int MODE>
+__device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, long long m0, int chunk, int tid,
+                                         const Vox& row_vox, bool row_ok)
+{
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    if (MODE == kFwd || MODE == kData) {
+        // K-major: thread tid owns row tid; unit j covers K half (j & 1) of K-step (j >> 1).
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int ks = j >> 1, c = j & 1;
+            const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + c * 8;
+            uint4 v = zero;
+            if (row_ok && k < a.k_total) {
+                if (MODE == kFwd) {
+                    const int tap = static_cast<int>(k / a.cinp), ci0 = static_cast<int>(k % a.cinp);
+                    int iz, iy, ix;
+                    if (tap < 27 && (a.cin >= 8 || ci0 == 0) && tap_input(row_vox, tap, a.stride, a.s_in, iz, iy, ix)) {
+                        const long long vi =
+                            ((static_cast<long long>(row_vox.n) * a.s_in + iz) * a.s_in + iy) * a.s_in + ix;
+                        v = load_channels(a.x + vi * a.cin, a.cin, ci0);
+                    }
+                }
+                else {
+                    const int tap = static_cast<int>(k / a.cout), co0 = static_cast<int>(k % a.cout);
+                    int qz, qy, qx;
+                    if (tap < 27 && tap_output(row_vox, tap, a.stride, a.s_out, qz, qy, qx)) {
+                        const long long qi =
+                            ((static_cast<long long>(row_vox.n) * a.s_out + qz) * a.s_out + qy) * a.s_out + qx;
+                        v = __ldg(reinterpret_cast<const uint4*>(a.dy + qi * a.cout + co0));
+                    }
+                }
+            }
+            put(A, ks * kStepBytesA + umma::unit_offset(tid >> 3, c, tid & 7), v);
+        }
+    }
+    else {
+        // MN-major over rows (tap, cin): unit = 8 channels of one output voxel q.
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int e = tid + kThreads * j;
+            const int ks = e >> 8, kk = e & 15, g = (e & 255) >> 4;
+            const long long r0 = m0 + 8 * g;
+            const long long q = static_cast<long long>(chunk) * kKC + ks * 16 + kk;
+            uint4 v = zero;
+            if (q < a.k_total) {
+                if (r0 < a.kw) {
+                    const int tap = static_cast<int>(r0 / a.cinp), ci0 = static_cast<int>(r0 % a.cinp);
+                    const Vox o = decode(q, a.s_out);
+                    int iz, iy, ix;
+                    if ((a.cin >= 8 || ci0 == 0) && tap_input(o, tap, a.stride, a.s_in, iz, iy, ix)) {
+                        const long long vi = ((static_cast<long long>(o.n) * a.s_in + iz) * a.s_in + iy) * a.s_in + ix;
+                        v = load_channels(a.x + vi * a.cin, a.cin, ci0);
+                    }
+                }
+                else if (r0 == a.kw) {
+                    v.x = 0x3F80u;  // bf16 1.0 in row kw: the bias-gradient row
+                }
+            }
+            put(A, ks * kStepBytesA + umma::unit_offset(g, kk >> 3, kk & 7), v);
+        }
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ void gather_b(const ConvArgs& a, unsigned char* B, int N, int chunk, int tid)
+{
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    const int units = 4 * N;  // (N / 8) groups x 2 halves x 8 x 2 K-steps
+    for (int e = tid; e < units; e += kThreads) {
+        const int ks = e / (2 * N), rem = e % (2 * N);
+        uint4 v = zero;
+        std::uint32_t off;
+        if (MODE == kFwd) {
+            // K-major rows cout.
+            const int c = rem / N, co = rem % N;
+            const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + c * 8;
+            if (k < a.kw) {
+                v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<long long>(co) * a.kw + k));
+            }
+            off = umma::unit_offset(co >> 3, c, co & 7);
+        }
+        else {
+            // MN-major: unit = 8 consecutive rows at one K index.
+            const int kk = rem & 15, g = rem >> 4;
+            const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + kk;
+            if (MODE == kData) {
+                const int tap = static_cast<int>(k / a.cout), co = static_cast<int>(k % a.cout);
+                if (k < a.k_total && tap < 27) {
+                    v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<long long>(co) * a.kw +
+                                                             tap * a.cinp + 8 * g));
+                }
+            }
+            else if (k < a.k_total) {
+                v = __ldg(reinterpret_cast<const uint4*>(a.dy + k * a.cout + 8 * g));
+            }
+            off = umma::unit_offset(g, kk >> 3, kk & 7);
+        }
+        put(B, ks * (N * 32) + off, v);
+    }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ __align__(8) unsigned long long bars[kStages];
+    __shared__ std::uint32_t tmem_base;
+
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int N = MODE == kData ? a.cin : a.cout;
+    const std::uint32_t columns = N <= 32 ? 32u : 64u;
+    const int stage_bytes = kRows * kKC * 2 + N * kKC * 2;
+
+    if (warp == 0) {
+        umma::tmem_alloc(&tmem_base, columns);
+        umma::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            umma::bar_init(&bars[s], 1);
+        }
+        umma::bar_init_fence();
+    }
+    umma::fence_before();
+    __syncthreads();
+    umma::fence_after();
+    const std::uint32_t tmem = tmem_base;
+
+    const long long m0 = static_cast<long long>(blockIdx.x) * kRows;
+    const int chunks = static_cast<int>((a.k_total + kKC - 1) / kKC);
+    int c_begin = 0, c_end = chunks;
+    if (MODE == kWeight) {
+        c_begin = blockIdx.y * a.chunks_per_split;
+        c_end = min(chunks, c_begin + a.chunks_per_split);
+    }
+    Vox row_vox {};
+    bool row_ok = false;
+    if (MODE != kWeight) {
+        const long long m = m0 + tid;
+        row_ok = m < a.m_total;
+        row_vox = decode(row_ok ? m : 0, MODE == kFwd ? a.s_out : a.s_in);
+    }
+    constexpr bool a_mn = MODE == kWeight;
+    constexpr bool b_mn = MODE != kFwd;
+    const std::uint32_t idesc = umma::idesc_bf16(kRows, N, a_mn, b_mn);
+
+    bool ok = true;
+    for (int c = c_begin; c < c_end; ++c) {
+        const int it = c - c_begin, st = it % kStages;
+        if (it >= kStages && !umma::bar_wait(&bars[st], static_cast<std::uint32_t>((it / kStages - 1) & 1))) {
+            ok = false;
+        }
+        unsigned char* A = smem + st * stage_bytes;
+        unsigned char* B = A + kRows * kKC * 2;
+        gather_a<MODE>(a, A, m0, c, tid, row_vox, row_ok);
+        gather_b<MODE>(a, B, N, c, tid);
+        umma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after();
+#pragma unroll
+            for (int ks = 0; ks < 2; ++ks) {
+                const std::uint64_t da = umma::desc(umma::smem_addr(A + ks * kStepBytesA));
+                const std::uint64_t db = umma::desc(umma::smem_addr(B + ks * N * 32));
+                umma::mma_bf16(tmem, da, db, idesc, (it > 0 || ks > 0) ? 1u : 0u);
+            }
+            umma::commit(&bars[st]);
+        }
+    }
+    const int n_it = c_end - c_begin;
+    if (n_it > 0) {
+        const int last = n_it - 1;
+        if (!umma::bar_wait(&bars[last % kStages], static_cast<std::uint32_t>((last / kStages) & 1))) {
+            ok = false;
+        }
+    }
+    umma::fence_after();
+    if (!ok && (tid & 31) == 0) {
+        atomicOr(a.error, 1u);
+    }
+
+    // Epilogue: thread tid holds TMEM lane tid = tile row tid.
+    const std::uint32_t lane_addr = tmem + (static_cast<std::uint32_t>(warp * 32) << 16);
+    const long long row = m0 + tid;
+    for (int c0 = 0; c0 < N; c0 += 16) {
+        float v[16];
+        umma::tmem_load16(lane_addr + static_cast<std::uint32_t>(c0), v);
+        if (n_it == 0) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                v[i] = 0.f;
+            }
+        }
+        if (MODE == kFwd) {
+            if (row < a.m_total) {
+                __align__(16) bf16 h[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    h[i] = __float2bfloat16_rn(fmaxf(v[i] + a.bias[c0 + i], 0.f));
+                }
+                uint4* dst = reinterpret_cast<uint4*>(a.out + row * a.cout + c0);
+                dst[0] = reinterpret_cast<const uint4*>(h)[0];
+                dst[1] = reinterpret_cast<const uint4*>(h)[1];
+            }
+        }
+        else if (MODE == kData) {
+            if (row < a.m_total) {
+                __align__(16) bf16 h[16];
+                const bf16* xr = a.x + row * a.cin + c0;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    float g = v[i];
+                    if (a.relu_mask && !(__bfloat162float(xr[i]) > 0.f)) {
+                        g = 0.f;
+                    }
+                    h[i] = __float2bfloat16_rn(g);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(a.out + row * a.cin + c0);
+                dst[0] = reinterpret_cast<const uint4*>(h)[0];
+                dst[1] = reinterpret_cast<const uint4*>(h)[1];
+            }
+        }
+        else {
+            if (row <= a.kw) {
+                float* p = a.partial + static_cast<long long>(blockIdx.y) * a.cout * (a.kw + 1);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    p[static_cast<long long>(c0 + i) * (a.kw + 1) + row] = v[i];
+                }
+            }
+        }
+    }
+
+    umma::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after();
+        umma::tmem_dealloc(tmem, columns);
+    }
+}
+
+// Sums the weight-gradient partials of `splits` K ranges into the flat FP32
+// gradient (weights [cout][27][cin], then bias [cout]).
+__global__ void reduce_weight_grad_kernel(const float* partial, int splits, int cout, int cin, int cinp, float* grad_w,
+                                          float* grad_b)
+{
+    const int kw = 27 * cinp;
+    const int total = cout * 27 * cin + cout;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        int co, col;
+        float* dst;
+        if (i < cout * 27 * cin) {
+            co = i / (27 * cin);
+            const int rest = i % (27 * cin);
+            col = (rest / cin) * cinp + rest % cin;
+            dst = grad_w + i;
+        }
+        else {
+            co = i - cout * 27 * cin;
+            col = kw;
+            dst = grad_b + co;
+        }
+        float s = 0.f;
+        for (int sp = 0; sp < splits; ++sp) {
+            s += partial[(static_cast<long long>(sp) * cout + co) * (kw + 1) + col];
+        }
+        *dst = s;
+    }
+}
+
+// Head: mean over the 64 voxels of the last layer, linear 64 -> 1.  With
+// labels it also forms the squared-error loss, its gradient through the head
+// and the last layer's ReLU mask, and keeps the pooled features and dpred
+// for the head's parameter gradients.  One block of 64 threads per sample.
+__global__ void head_kernel(const bf16* act, const float* w, const float* b, int batch, const float* labels,
+                            float* pred, float* pooled_out, float* dpred_out, float* loss_terms, bf16* dpre)
+{
+    const int n = blockIdx.x, c = threadIdx.x;
+    if (n >= batch) {
+        return;
+    }
+    __shared__ float part[64];
+    __shared__ float shared_dpred;
+    const bf16* a = act + static_cast<long long>(n) * 64 * 64;
+    float s = 0.f;
+    for (int v = 0; v < 64; ++v) {
+        s += __bfloat162float(a[v * 64 + c]);
+    }
+    const float pooled = s * (1.0f / 64.0f);
+    part[c] = w[c] * pooled;
+    __syncthreads();
+    if (c == 0) {
+        float t = 0.f;
+        for (int i = 0; i < 64; ++i) {
+            t += part[i];
+        }
+        const float p = t + b[0];
+        pred[n] = p;
+        if (labels) {
+            const float d = p - labels[n];
+            loss_terms[n] = d * d;
+            shared_dpred = 2.0f * d / static_cast<float>(batch);
+            dpred_out[n] = shared_dpred;
+        }
+    }
+    if (!labels) {
+        return;
+    }
+    __syncthreads();
+    pooled_out[n * 64 + c] = pooled;
+    const float g = shared_dpred * w[c] * (1.0f / 64.0f);
+    bf16* d = dpre + static_cast<long long>(n) * 64 * 64;
+    for (int v = 0; v < 64; ++v) {
+        d[v * 64 + c] = __float2bfloat16_rn(__bfloat162float(a[v * 64 + c]) > 0.f ? g : 0.f);
+    }
+}
+
+// Head parameter gradients and the mean loss (one block of 64 threads).
+__global__ void head_grad_kernel(const float* pooled, const float* dpred, const float* loss_terms, int batch,
+                                 float* grad_w, float* grad_b, float* loss)
+{
+    const int c = threadIdx.x;
+    float gw = 0.f;
+    for (int n = 0; n < batch; ++n) {
+        gw += dpred[n] * pooled[n * 64 + c];
+    }
+    grad_w[c] = gw;
+    if (c == 0) {
+        float gb = 0.f, l = 0.f;
+        for (int n = 0; n < batch; ++n) {
+            gb += dpred[n];
+            l += loss_terms[n];
+        }
+        grad_b[0] = gb;
+        loss[0] = l / static_cast<float>(batch);
+    }
+}
+
+__global__ void adam_kernel(float* p, const float* g, float* m, float* v, long long count, float lr, float b1,
+                            float b2, float eps, float c1, float c2)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+// FP32 master weights [cout][27][cin] -> BF16 [cout][27 * cinp], zero padded.
+__global__ void pack_weights_kernel(const float* w, int cout, int cin, int cinp, bf16* out)
+{
+    const int kw = 27 * cinp;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cout * kw; i += gridDim.x * blockDim.x) {
+        const int co = i / kw, col = i % kw, tap = col / cinp, ci = col % cinp;
+        out[i] = __float2bfloat16_rn(ci < cin ? w[(co * 27 + tap) * cin + ci] : 0.f);
+    }
+}
+
+// Network input: sample b = (crop[crop_index[b]], item[item_index[b]]), 2 channels.
+__global__ void assemble_kernel(const bf16* crops, const std::uint32_t* crop_index, const bf16* items,
+                                const std::uint32_t* item_index, int batch, bf16* x0)
+{
+    const long long total = static_cast<long long>(batch) * kProposalVoxels;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int b = static_cast<int>(i / kProposalVoxels), v = static_cast<int>(i % kProposalVoxels);
+        const long long crop = crop_index ? crop_index[b] : 0;
+        const long long item = item_index ? item_index[b] : b;
+        __nv_bfloat162 pair;
+        pair.x = crops[crop * kProposalVoxels + v];
+        pair.y = items[item * kProposalVoxels + v];
+        reinterpret_cast<__nv_bfloat162*>(x0)[i] = pair;
+    }
+}
+
+__global__ void to_bf16_kernel(const float* in, long long count, bf16* out)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        out[i] = __float2bfloat16_rn(in[i]);
+    }
+}
+
+// Pools a u8 field (X-fastest, shape[0..2]) into 32^3 fractions with block
+// edge f per axis; cells outside the field count as `outside`.
+__global__ void pool_kernel(const std::uint8_t* field, int s0, int s1, int s2, int f0, int f1, int f2,
+                            float outside, bf16* out)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= kProposalVoxels) {
+        return;
+    }
+    const int x = v % kProposalGrid, y = (v / kProposalGrid) % kProposalGrid, z = v / (kProposalGrid * kProposalGrid);
+    float sum = 0.f;
+    for (int dz = 0; dz < f2; ++dz) {
+        const int cz = z * f2 + dz;
+        for (int dy = 0; dy < f1; ++dy) {
+            const int cy = y * f1 + dy;
+            for (int dx = 0; dx < f0; ++dx) {
+                const int cx = x * f0 + dx;
+                if (cx < s0 && cy < s1 && cz < s2) {
+                    sum += field[(static_cast<long long>(cz) * s1 + cy) * s0 + cx] ? 1.f : 0.f;
+                }
+                else {
+                    sum += outside;
+                }
+            }
+        }
+    }
+    out[v] = __float2bfloat16_rn(sum / static_cast<float>(f0 * f1 * f2));
+}
+
+template <int MODE>
+void set_smem_attribute()
+{
+    static std::once_flag flag[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::call_once(flag[dev & 63], [] {
+        cudaFuncSetAttribute(conv_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kStages * (kRows * kKC * 2 + 64 * kKC * 2));
+    });
+}
+
+std::uint64_t splitmix(std::uint64_t& s)
+{
+    std::uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+double uniform01(std::uint64_t& s) { return (static_cast<double>(splitmix(s) >> 11) + 0.5) * (1.0 / 9007199254740992.0); }
+
+}  // namespace
+
+struct ProposalNet {
+    int device {};
+    std::uint64_t count {};
+    std::uint64_t w_off[kProposalLayers] {}, b_off[kProposalLayers] {}, head_w {}, head_b {};
+    float* params {};
+    float* grads {};
+    float* adam_m {};
+    float* adam_v {};
+    std::uint64_t adam_t {};
+    bf16* w[kProposalLayers] {};
+    // batch buffers
+    std::uint32_t capacity {};
+    bf16* x0 {};
+    bf16* act[kProposalLayers] {};
+    bf16* dpre[kProposalLayers] {};
+    float* pred {};
+    float* labels {};
+    float* pooled {};
+    float* dpred {};
+    float* loss_terms {};
+    float* loss {};
+    float* partial {};
+    std::size_t partial_bytes {};
+    unsigned* error {};
+    std::vector<void*> owned;
+};
+
+namespace {
+
+int out_side(const ProposalLayer& l) { return l.s_in / l.stride; }
+
+template <typename T>
+int alloc(ProposalNet* net, T*& p, std::size_t count)
+{
+    void* raw {};
+    if (cudaMalloc(&raw, sizeof(T) * (count ? count : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return kAllocation;
+    }
+    net->owned.push_back(raw);
+    p = static_cast<T*>(raw);
+    return kOk;
+}
+
+void release(ProposalNet* net, void* p)
+{
+    if (!p) {
+        return;
+    }
+    cudaFree(p);
+    net->owned.erase(std::remove(net->owned.begin(), net->owned.end(), p), net->owned.end());
+}
+
+int ensure_batch(ProposalNet* net, std::uint32_t batch)
+{
+    if (batch <= net->capacity) {
+        return kOk;
+    }
+    release(net, net->x0);
+    for (int l = 0; l < kProposalLayers; ++l) {
+        release(net, net->act[l]);
+        release(net, net->dpre[l]);
+    }
+    for (float* p : { net->pred, net->labels, net->pooled, net->dpred, net->loss_terms }) {
+        release(net, p);
+    }
+    net->capacity = 0;
+    int s = alloc(net, net->x0, static_cast<std::size_t>(batch) * kProposalVoxels * 2);
+    for (int l = 0; l < kProposalLayers && !s; ++l) {
+        const int so = out_side(kProposalSpec[l]);
+        const std::size_t n = static_cast<std::size_t>(batch) * so * so * so * kProposalSpec[l].cout;
+        s = alloc(net, net->act[l], n);
+        if (!s) {
+            s = alloc(net, net->dpre[l], n);
+        }
+    }
+    if (!s) s = alloc(net, net->pred, batch);
+    if (!s) s = alloc(net, net->labels, batch);
+    if (!s) s = alloc(net, net->pooled, static_cast<std::size_t>(batch) * 64);
+    if (!s) s = alloc(net, net->dpred, batch);
+    if (!s) s = alloc(net, net->loss_terms, batch);
+    if (s) {
+        return s;
+    }
+    net->capacity = batch;
+    return kOk;
+}
+
+int grid_for(long long n, int threads = 256)
+{
+    const long long g = (n + threads - 1) / threads;
+    return static_cast<int>(std::min<long long>(std::max<long long>(g, 1), 148LL * 32));
+}
+
+ConvArgs layer_args(ProposalNet* net, int l, std::uint32_t batch)
+{
+    const ProposalLayer& L = kProposalSpec[l];
+    ConvArgs a {};
+    a.x = l == 0 ? net->x0 : net->act[l - 1];
+    a.dy = net->dpre[l];
+    a.w = net->w[l];
+    a.bias = net->params + net->b_off[l];
+    a.error = net->error;
+    a.batch = static_cast<int>(batch);
+    a.s_in = L.s_in;
+    a.s_out = out_side(L);
+    a.stride = L.stride;
+    a.cin = L.cin;
+    a.cinp = cin_pad(L.cin);
+    a.cout = L.cout;
+    a.kw = 27 * a.cinp;
+    return a;
+}
+
+int launch_forward(spk_context* ctx, ProposalNet* net, std::uint32_t batch)
+{
+    set_smem_attribute<kFwd>();
+    for (int l = 0; l < kProposalLayers; ++l) {
+        ConvArgs a = layer_args(net, l, batch);
+        a.out = net->act[l];
+        a.m_total = static_cast<long long>(batch) * a.s_out * a.s_out * a.s_out;
+        a.k_total = a.kw;
+        const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
+        const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
+        conv_kernel<kFwd><<<blocks, kThreads, smem, ctx->stream>>>(a);
+        ctx->launches++;
+    }
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+// Forward + backward for `batch` samples already in x0 with labels in
+// net->labels; leaves the flat gradient in net->grads and the loss in net->loss.
+int launch_gradients(spk_context* ctx, ProposalNet* net, std::uint32_t batch)
+{
+    int status = launch_forward(ctx, net, batch);
+    if (status) {
+        return status;
+    }
+    head_kernel<<<batch, 64, 0, ctx->stream>>>(net->act[3], net->params + net->head_w, net->params + net->head_b,
+                                                static_cast<int>(batch), net->labels, net->pred, net->pooled,
+                                                net->dpred, net->loss_terms, net->dpre[3]);
+    head_grad_kernel<<<1, 64, 0, ctx->stream>>>(net->pooled, net->dpred, net->loss_terms, static_cast<int>(batch),
+                                                net->grads + net->head_w, net->grads + net->head_b, net->loss);
+    ctx->launches += 2;
+    set_smem_attribute<kData>();
+    set_smem_attribute<kWeight>();
+    for (int l = kProposalLayers - 1; l >= 0; --l) {
+        ConvArgs a = layer_args(net, l, batch);
+        // weight gradient
+        {
+            ConvArgs g = a;
+            g.k_total = static_cast<long long>(batch) * a.s_out * a.s_out * a.s_out;
+            g.m_total = a.kw + 1;
+            const int m_tiles = static_cast<int>((a.kw + 1 + kRows - 1) / kRows);
+            const int chunks = static_cast<int>((g.k_total + kKC - 1) / kKC);
+            int splits = std::max(1, std::min((2 * 148 * 2 + m_tiles - 1) / m_tiles, chunks / 4));
+            g.chunks_per_split = (chunks + splits - 1) / splits;
+            splits = (chunks + g.chunks_per_split - 1) / g.chunks_per_split;
+            const std::size_t need = static_cast<std::size_t>(splits) * a.cout * (a.kw + 1) * sizeof(float);
+            if (need > net->partial_bytes) {
+                release(net, net->partial);
+                net->partial = nullptr;
+                net->partial_bytes = 0;
+                if ((status = alloc(net, net->partial, need / sizeof(float)))) {
+                    return status;
+                }
+                net->partial_bytes = need;
+            }
+            g.partial = net->partial;
+            const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
+            conv_kernel<kWeight><<<dim3(m_tiles, splits), kThreads, smem, ctx->stream>>>(g);
+            reduce_weight_grad_kernel<<<grid_for(a.cout * 27 * a.cin + a.cout), 256, 0, ctx->stream>>>(
+                net->partial, splits, a.cout, a.cin, a.cinp, net->grads + net->w_off[l], net->grads + net->b_off[l]);
+            ctx->launches += 2;
+        }
+        // data gradient into the previous layer's pre-activation gradient
+        if (l > 0) {
+            ConvArgs d = a;
+            d.out = net->dpre[l - 1];
+            d.m_total = static_cast<long long>(batch) * a.s_in * a.s_in * a.s_in;
+            d.k_total = 27LL * a.cout;
+            d.relu_mask = 1;
+            const int blocks = static_cast<int>((d.m_total + kRows - 1) / kRows);
+            const int smem = kStages * (kRows * kKC * 2 + a.cin * kKC * 2);
+            conv_kernel<kData><<<blocks, kThreads, smem, ctx->stream>>>(d);
+            ctx->launches++;
+        }
+    }
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int pack_all(spk_context* ctx, ProposalNet* net)
+{
+    for (int l = 0; l < kProposalLayers; ++l) {
+        const ProposalLayer& L = kProposalSpec[l];
+        pack_weights_kernel<<<grid_for(L.cout * 27 * cin_pad(L.cin)), 256, 0, ctx->stream>>>(
+            net->params + net->w_off[l], L.cout, L.cin, cin_pad(L.cin), net->w[l]);
+        ctx->launches++;
+    }
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int check_error(spk_context* ctx, ProposalNet* net)
+{
+    unsigned err = 0;
+    if (cudaMemcpyAsync(&err, net->error, sizeof(err), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    if (err) {
+        cudaMemsetAsync(net->error, 0, sizeof(unsigned), ctx->stream);
+        return kKernelWait;
+    }
+    return kOk;
+}
+
+int upload_inputs(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const float* inputs)
+{
+    const long long n = static_cast<long long>(batch) * kProposalVoxels * 2;
+    int status = kOk;
+    float* staging = static_cast<float*>(device_buffer(ctx, "proposal_inputs", sizeof(float) * n, status));
+    if (!staging) {
+        return status;
+    }
+    if (cudaMemcpyAsync(staging, inputs, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    to_bf16_kernel<<<grid_for(n), 256, 0, ctx->stream>>>(staging, n, net->x0);
+    ctx->launches++;
+    return kOk;
+}
+
+}  // namespace
+
+std::uint64_t proposal_parameter_count()
+{
+    std::uint64_t n = 0;
+    for (const ProposalLayer& l : kProposalSpec) {
+        n += static_cast<std::uint64_t>(l.cout) * 27 * l.cin + l.cout;
+    }
+    return n + 64 + 1;
+}
+
+int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const bf16* crops,
+                     const std::uint32_t* crop_index, const bf16* items, const std::uint32_t* item_index, float* pred)
+{
+    int status = ensure_batch(net, batch);
+    if (status) {
+        return status;
+    }
+    assemble_kernel<<<grid_for(static_cast<long long>(batch) * kProposalVoxels), 256, 0, ctx->stream>>>(
+        crops, crop_index, items, item_index, static_cast<int>(batch), net->x0);
+    ctx->launches++;
+    if ((status = launch_forward(ctx, net, batch))) {
+        return status;
+    }
+    head_kernel<<<batch, 64, 0, ctx->stream>>>(net->act[3], net->params + net->head_w, net->params + net->head_b,
+                                                static_cast<int>(batch), nullptr, pred, nullptr, nullptr, nullptr,
+                                                nullptr);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int pool_occupancy(spk_context* ctx, const std::uint8_t* occupancy, const int* shape, bf16* out)
+{
+    int f[3];
+    for (int a = 0; a < 3; ++a) {
+        f[a] = std::max(1, (shape[a] + kProposalGrid - 1) / kProposalGrid);
+    }
+    pool_kernel<<<kProposalVoxels / 256, 256, 0, ctx->stream>>>(occupancy, shape[0], shape[1], shape[2], f[0], f[1],
+                                                                 f[2], 1.0f, out);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int pool_item(spk_context* ctx, const std::uint8_t* cells, const int* shape, bf16* out)
+{
+    const int m = std::max(shape[0], std::max(shape[1], shape[2]));
+    const int f = std::max(1, (m + kProposalGrid - 1) / kProposalGrid);
+    pool_kernel<<<kProposalVoxels / 256, 256, 0, ctx->stream>>>(cells, shape[0], shape[1], shape[2], f, f, f, 0.0f,
+                                                                 out);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+}  // namespace spk
+
+using spk::ProposalNet;
+
+struct spk_proposal {
+    ProposalNet net;
+};
+
+namespace {
+
+ProposalNet* net_of(spk_proposal* p) { return p ? &p->net : nullptr; }
+
+}  // namespace
+
+extern "C" {
+
+uint64_t spk_proposal_parameter_count(void) { return spk::proposal_parameter_count(); }
+
+int spk_proposal_create(spk_context* ctx, uint64_t seed, spk_proposal** out)
+{
+    try {
+        if (!ctx || !out) {
+            return spk::kInvalidArgument;
+        }
+        *out = nullptr;
+        if (cudaSetDevice(ctx->device) != cudaSuccess) {
+            return spk::kCuda;
+        }
+        auto* p = new spk_proposal();
+        ProposalNet* net = &p->net;
+        net->device = ctx->device;
+        net->count = spk::proposal_parameter_count();
+        std::vector<float> host(net->count, 0.f);
+        std::uint64_t off = 0, state = seed ^ 0x5EED5EED5EEDull;
+        for (int l = 0; l < spk::kProposalLayers; ++l) {
+            const spk::ProposalLayer& L = spk::kProposalSpec[l];
+            net->w_off[l] = off;
+            const std::uint64_t nw = static_cast<std::uint64_t>(L.cout) * 27 * L.cin;
+            const double sd = std::sqrt(2.0 / (27.0 * L.cin));  // He initialisation for ReLU
+            for (std::uint64_t i = 0; i < nw; ++i) {
+                const double u1 = spk::uniform01(state), u2 = spk::uniform01(state);
+                host[off + i] = static_cast<float>(sd * std::sqrt(-2.0 * std::log(u1)) *
+                                                   std::cos(6.283185307179586 * u2));
+            }
+            off += nw;
+            net->b_off[l] = off;
+            off += L.cout;
+        }
+        net->head_w = off;
+        for (int c = 0; c < 64; ++c) {
+            const double u1 = spk::uniform01(state), u2 = spk::uniform01(state);
+            host[off + c] = static_cast<float>(0.125 * std::sqrt(-2.0 * std::log(u1)) *
+                                               std::cos(6.283185307179586 * u2));
+        }
+        off += 64;
+        net->head_b = off;
+        int s = spk::alloc(net, net->params, net->count);
+        if (!s) s = spk::alloc(net, net->grads, net->count);
+        if (!s) s = spk::alloc(net, net->adam_m, net->count);
+        if (!s) s = spk::alloc(net, net->adam_v, net->count);
+        if (!s) s = spk::alloc(net, net->loss, 1);
+        if (!s) s = spk::alloc(net, net->error, 1);
+        for (int l = 0; l < spk::kProposalLayers && !s; ++l) {
+            const spk::ProposalLayer& L = spk::kProposalSpec[l];
+            s = spk::alloc(net, net->w[l], static_cast<std::size_t>(L.cout) * 27 * spk::cin_pad(L.cin));
+        }
+        if (s) {
+            for (void* q : net->owned) {
+                cudaFree(q);
+            }
+            delete p;
+            return s;
+        }
+        cudaMemcpyAsync(net->params, host.data(), sizeof(float) * net->count, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemsetAsync(net->adam_m, 0, sizeof(float) * net->count, ctx->stream);
+        cudaMemsetAsync(net->adam_v, 0, sizeof(float) * net->count, ctx->stream);
+        cudaMemsetAsync(net->grads, 0, sizeof(float) * net->count, ctx->stream);
+        cudaMemsetAsync(net->error, 0, sizeof(unsigned), ctx->stream);
+        if ((s = spk::pack_all(ctx, net)) || cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            cudaGetLastError();
+            for (void* q : net->owned) {
+                cudaFree(q);
+            }
+            delete p;
+            return s ? s : spk::kCuda;
+        }
+        *out = p;
+        return spk::kOk;
+    }
+    catch (...) {
+        return spk::kAllocation;
+    }
+}
+
+void spk_proposal_destroy(spk_proposal* p)
+{
+    if (!p) {
+        return;
+    }
+    cudaSetDevice(p->net.device);
+    for (void* q : p->net.owned) {
+        cudaFree(q);
+    }
+    delete p;
+}
+
+int spk_proposal_get_parameters(spk_context* ctx, spk_proposal* p, float* out)
+{
+    ProposalNet* net = net_of(p);
+    if (!ctx || !net || !out) {
+        return spk::kInvalidArgument;
+    }
+    if (cudaMemcpyAsync(out, net->params, sizeof(float) * net->count, cudaMemcpyDeviceToHost, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return spk::kCuda;
+    }
+    return spk::kOk;
+}
+
+int spk_proposal_set_parameters(spk_context* ctx, spk_proposal* p, const float* in)
+{
+    ProposalNet* net = net_of(p);
+    if (!ctx || !net || !in) {
+        return spk::kInvalidArgument;
+    }
+    if (cudaMemcpyAsync(net->params, in, sizeof(float) * net->count, cudaMemcpyHostToDevice, ctx->stream) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return spk::kCuda;
+    }
+    cudaMemsetAsync(net->adam_m, 0, sizeof(float) * net->count, ctx->stream);
+    cudaMemsetAsync(net->adam_v, 0, sizeof(float) * net->count, ctx->stream);
+    net->adam_t = 0;
+    int s = spk::pack_all(ctx, net);
+    if (!s && cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        s = spk::kCuda;
+    }
+    return s;
+}
+
+int spk_proposal_forward(spk_context* ctx, spk_proposal* p, uint64_t batch, const float* inputs, float* predictions)
+{
+    try {
+        ProposalNet* net = net_of(p);
+        if (!ctx || !net || !inputs || !predictions || batch == 0 || batch > (1u << 16)) {
+            return spk::kInvalidArgument;
+        }
+        const auto b = static_cast<std::uint32_t>(batch);
+        int s = spk::ensure_batch(net, b);
+        if (!s) s = spk::upload_inputs(ctx, net, b, inputs);
+        if (!s) s = spk::launch_forward(ctx, net, b);
+        if (s) {
+            return s;
+        }
+        spk::head_kernel<<<b, 64, 0, ctx->stream>>>(net->act[3], net->params + net->head_w,
+                                                     net->params + net->head_b, static_cast<int>(b), nullptr,
+                                                     net->pred, nullptr, nullptr, nullptr, nullptr);
+        ctx->launches++;
+        if (cudaMemcpyAsync(predictions, net->pred, sizeof(float) * b, cudaMemcpyDeviceToHost, ctx->stream) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            return spk::kCuda;
+        }
+        return spk::check_error(ctx, net);
+    }
+    catch (...) {
+        return spk::kAllocation;
+    }
+}
+
+int spk_proposal_gradients(spk_context* ctx, spk_proposal* p, uint64_t batch, const float* inputs,
+                           const float* labels, float* loss, float* gradients)
+{
+    try {
+        ProposalNet* net = net_of(p);
+        if (!ctx || !net || !inputs || !labels || !loss || !gradients || batch == 0 || batch > (1u << 16)) {
+            return spk::kInvalidArgument;
+        }
+        const auto b = static_cast<std::uint32_t>(batch);
+        int s = spk::ensure_batch(net, b);
+        if (!s) s = spk::upload_inputs(ctx, net, b, inputs);
+        if (s) {
+            return s;
+        }
+        cudaMemcpyAsync(net->labels, labels, sizeof(float) * b, cudaMemcpyHostToDevice, ctx->stream);
+        if ((s = spk::launch_gradients(ctx, net, b))) {
+            return s;
+        }
+        cudaMemcpyAsync(loss, net->loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+        cudaMemcpyAsync(gradients, net->grads, sizeof(float) * net->count, cudaMemcpyDeviceToHost, ctx->stream);
+        return spk::check_error(ctx, net);
+    }
+    catch (...) {
+        return spk::kAllocation;
+    }
+}
+
+int spk_proposal_train(spk_context* ctx, spk_proposal* p, const spk_proposal_dataset* data, uint32_t batch,
+                       uint32_t steps, float learning_rate, uint64_t seed, float* losses)
+{
+    try {
+        ProposalNet* net = net_of(p);
+        if (!ctx || !net || !data || !data->crops || !data->items || !data->sample_crop || !data->sample_item ||
+            !data->sample_label || data->sample_count == 0 || batch == 0 || batch > (1u << 14)) {
+            return spk::kInvalidArgument;
+        }
+        for (std::uint64_t i = 0; i < data->sample_count; ++i) {
+            if (data->sample_crop[i] >= data->crop_count || data->sample_item[i] >= data->item_count) {
+                return spk::kInvalidArgument;
+            }
+        }
+        int s = spk::ensure_batch(net, batch);
+        if (s) {
+            return s;
+        }
+        const std::uint64_t nc = data->crop_count * spk::kProposalVoxels;
+        const std::uint64_t ni = data->item_count * spk::kProposalVoxels;
+        float* staging =
+            static_cast<float*>(spk::device_buffer(ctx, "proposal_inputs", sizeof(float) * std::max(nc, ni), s));
+        spk::bf16* crops = static_cast<spk::bf16*>(spk::device_buffer(ctx, "proposal_crops", sizeof(spk::bf16) * nc, s));
+        spk::bf16* items = static_cast<spk::bf16*>(spk::device_buffer(ctx, "proposal_items", sizeof(spk::bf16) * ni, s));
+        auto* index = static_cast<std::uint32_t*>(
+            spk::device_buffer(ctx, "proposal_index", sizeof(std::uint32_t) * 2 * batch, s));
+        auto* host_index = static_cast<std::uint32_t*>(
+            spk::host_buffer(ctx, "proposal_index_host", sizeof(std::uint32_t) * 2 * batch * steps, s));
+        auto* host_labels =
+            static_cast<float*>(spk::host_buffer(ctx, "proposal_labels_host", sizeof(float) * batch * steps, s));
+        if (!staging || !crops || !items || !index || !host_index || !host_labels) {
+            return s ? s : spk::kAllocation;
+        }
+        cudaMemcpyAsync(staging, data->crops, sizeof(float) * nc, cudaMemcpyHostToDevice, ctx->stream);
+        spk::to_bf16_kernel<<<spk::grid_for(nc), 256, 0, ctx->stream>>>(staging, nc, crops);
+        cudaMemcpyAsync(staging, data->items, sizeof(float) * ni, cudaMemcpyHostToDevice, ctx->stream);
+        spk::to_bf16_kernel<<<spk::grid_for(ni), 256, 0, ctx->stream>>>(staging, ni, items);
+        ctx->launches += 2;
+        std::uint64_t state = seed;
+        for (std::uint32_t t = 0; t < steps; ++t) {
+            for (std::uint32_t b = 0; b < batch; ++b) {
+                const std::uint64_t pick = spk::splitmix(state) % data->sample_count;
+                host_index[2 * batch * t + b] = data->sample_crop[pick];
+                host_index[2 * batch * t + batch + b] = data->sample_item[pick];
+                host_labels[batch * t + b] = data->sample_label[pick];
+            }
+        }
+        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+        for (std::uint32_t t = 0; t < steps; ++t) {
+            cudaMemcpyAsync(index, host_index + 2 * batch * t, sizeof(std::uint32_t) * 2 * batch,
+                            cudaMemcpyHostToDevice, ctx->stream);
+            cudaMemcpyAsync(net->labels, host_labels + batch * t, sizeof(float) * batch, cudaMemcpyHostToDevice,
+                            ctx->stream);
+            spk::assemble_kernel<<<spk::grid_for(static_cast<long long>(batch) * spk::kProposalVoxels), 256, 0,
+                                   ctx->stream>>>(crops, index, items, index + batch, static_cast<int>(batch),
+                                                  net->x0);
+            ctx->launches++;
+            if ((s = spk::launch_gradients(ctx, net, batch))) {
+                return s;
+            }
+            net->adam_t += 1;
+            const float c1 = 1.f - std::pow(b1, static_cast<float>(net->adam_t));
+            const float c2 = 1.f - std::pow(b2, static_cast<float>(net->adam_t));
+            spk::adam_kernel<<<spk::grid_for(static_cast<long long>(net->count)), 256, 0, ctx->stream>>>(
+                net->params, net->grads, net->adam_m, net->adam_v, static_cast<long long>(net->count), learning_rate,
+                b1, b2, eps, c1, c2);
+            ctx->launches++;
+            if ((s = spk::pack_all(ctx, net))) {
+                return s;
+            }
+            if (losses) {
+                cudaMemcpyAsync(losses + t, net->loss, sizeof(float), cudaMemcpyDeviceToHost, ctx->stream);
+            }
+        }
+        return spk::check_error(ctx, net);
+    }
+    catch (...) {
+        return spk::kAllocation;
+    }
+}
+
+}  // extern "C"
+
+namespace spk {
+ProposalNet* proposal_net(spk_proposal* p) { return p ? &p->net : nullptr; }
+}  // namespace spk

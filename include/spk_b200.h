@@ -309,6 +309,65 @@ int spk_session_stats(spk_context* context, uint64_t out[4], int reset);
 int spk_session_field(spk_context* context, int kind, uint64_t orientation, int64_t first[3], uint32_t shape[3],
                       void* out, uint64_t capacity_bytes);
 
+/* ---- learned orientation proposal ------------------------------------------
+ * No counterpart in the reference: a small 3D CNN that ranks the catalog's
+ * orientations for the current layout so a placement step pages only the k
+ * best (the exhaustive step remains the fallback).  Input per sample: 2 x 32^3
+ * channels-last floats ([z][y][x][c]): c = 0 the layout's occupancy fraction
+ * pooled over the environment window (cells outside count as occupied),
+ * c = 1 the oriented item's cells pooled to 32^3 (corner aligned).  Network:
+ * conv3d 3^3 pad 1 + ReLU: 2->16 s1, 16->32 s2, 32->64 s2, 64->64 s2; mean
+ * over the 4^3 voxels; linear 64->1.  BF16 tensor-core arithmetic with FP32
+ * accumulation; FP32 master parameters in the flat order: per conv layer
+ * weights [cout][27][cin] (tap = (kz*3+ky)*3+kx, input = out*stride+k-1) and
+ * bias [cout], then head weights [64] and bias [1].  Loss: mean squared error
+ * of the prediction against the label. */
+typedef struct spk_proposal spk_proposal;
+
+typedef struct spk_proposal_dataset {
+    const float* crops;           /* crop_count x 32^3 occupancy channels */
+    uint64_t crop_count;
+    const float* items;           /* item_count x 32^3 item channels */
+    uint64_t item_count;
+    const uint32_t* sample_crop;  /* per sample: crop index */
+    const uint32_t* sample_item;  /* per sample: item index */
+    const float* sample_label;    /* per sample: target */
+    uint64_t sample_count;
+} spk_proposal_dataset;
+
+uint64_t spk_proposal_parameter_count(void);
+/* He-initialised parameters from `seed`. */
+int spk_proposal_create(spk_context* context, uint64_t seed, spk_proposal** out);
+void spk_proposal_destroy(spk_proposal* proposal);
+int spk_proposal_get_parameters(spk_context* context, spk_proposal* proposal, float* out);
+/* Replaces the parameters and resets the optimiser state. */
+int spk_proposal_set_parameters(spk_context* context, spk_proposal* proposal, const float* in);
+/* Predictions for `batch` host samples (batch x 32^3 x 2 floats). */
+int spk_proposal_forward(spk_context* context, spk_proposal* proposal, uint64_t batch, const float* inputs,
+                         float* predictions);
+/* Loss and the gradient of every parameter (flat order) for one batch. */
+int spk_proposal_gradients(spk_context* context, spk_proposal* proposal, uint64_t batch, const float* inputs,
+                           const float* labels, float* loss, float* gradients);
+/* `steps` Adam steps (beta 0.9/0.999, eps 1e-8) on batches drawn from the
+ * dataset with a splitmix64 stream seeded by `seed`; losses[steps] optional. */
+int spk_proposal_train(spk_context* context, spk_proposal* proposal, const spk_proposal_dataset* data, uint32_t batch,
+                       uint32_t steps, float learning_rate, uint64_t seed, float* losses);
+
+/* Proposal inputs of the open session: the current layout's occupancy
+ * channel (32^3 floats) and every orientation's item channel
+ * (orientations x 32^3 floats); either pointer may be NULL. */
+int spk_session_features(spk_context* context, float* crop, float* items);
+/* The k orientations the network ranks best for the current layout, and
+ * optionally every orientation's prediction. */
+int spk_session_propose(spk_context* context, spk_proposal* proposal, uint32_t k, uint64_t* orientations,
+                        float* predictions);
+/* Greedy fill that pages only the k proposed orientations per step; a step
+ * where none of them admits a copy runs the exhaustive step (counted in
+ * *fallbacks). */
+int spk_session_greedy_proposed(spk_context* context, spk_proposal* proposal, uint32_t k, uint64_t max_steps,
+                                uint64_t* placed, uint64_t* orientations, int64_t* translations, double* scores,
+                                uint64_t* fallbacks);
+
 #ifdef __cplusplus
 }
 #endif
