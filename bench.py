@@ -37,6 +37,8 @@ UNIT = "placements/s"
 # dram__bytes_read.sum + dram__bytes_write.sum of one pass_a256_kernel launch
 # (profiles/pass_a256_pass_b2_256_blob256_o16.md): 143,679,744 + 67,410,688.
 PASS_A256_DRAM_BYTES = 211090432
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp-max-packer_b200", "weights",
+                               "proposal_rounded256.npz")
 
 
 def pkg(name):
@@ -112,10 +114,51 @@ def algorithmic_bytes(session):
     return float(np.mean(per))
 
 
+def timed_steps(stream, fn, dist):
+    """Runs fn() between a barrier + synchronize on both sides with CUDA
+    events on the library's stream; returns (ms, result)."""
+    import torch
+
+    if dist:
+        import torch.distributed as tdist
+
+        tdist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    out = fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        import torch.distributed as tdist
+
+        tdist.barrier()
+    return start.elapsed_time(end), out
+
+
+def max_over_ranks(ms, placed, world):
+    """(max ms over ranks, placements summed over ranks)."""
+    if world == 1:
+        return ms, float(placed)
+    import torch
+    import torch.distributed as tdist
+
+    t = torch.tensor([ms, float(placed)], device="cuda")
+    gathered = [torch.zeros_like(t) for _ in range(world)]
+    tdist.all_gather(gathered, t)
+    return max(float(g[0]) for g in gathered), sum(float(g[1]) for g in gathered)
+
+
+def reset_layout(session):
+    while session.placements:
+        session.remove_last()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
     compute, session_mod, workloads, lib_mod = pkg("compute"), pkg("session"), pkg("workloads"), pkg("_lib")
+    proposal = pkg("proposal")
     torch.cuda.set_device(local_rank)
     ctx = compute.Context(local_rank)
     lib = lib_mod.lib()
@@ -123,50 +166,56 @@ def run_ours(args, rank, world, local_rank):
         workloads.WORKLOADS[args.workload]()
     if args.orientations:
         wl.catalog = wl.catalog[: args.orientations]
+    O = len(wl.catalog)
     t0 = time.time()
     session = session_mod.Session(wl.obj, wl.container, wl.origin, wl.pitch, wl.catalog, wl.pair_clearance,
                                   wl.wall_clearance, context=ctx)
     open_s = time.time() - t0
     stream = torch.cuda.ExternalStream(lib.spk_context_stream(ctx.handle))
-    session.greedy(args.warmup)
     dist = world > 1
-    if dist:
-        import torch.distributed as tdist
-        tdist.barrier()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = ctx.launches
-    session.stats(reset=True)
+    weights = args.weights if args.weights else DEFAULT_WEIGHTS
+    learned = args.mode == "learned" and os.path.exists(weights)
+    k = min(args.k, O)
+
     with ClockSampler(local_rank) as clocks:
-        start.record(stream)
-        placed = session.greedy(args.steps)
-        end.record(stream)
-        torch.cuda.synchronize()
-    launches = ctx.launches - launches0
-    page_stats = session.stats(reset=True)
-    ms = start.elapsed_time(end)
-    n_placed = len(placed)
-    if dist:
-        t = torch.tensor([ms, float(n_placed)], device="cuda")
-        import torch.distributed as tdist
-        gathered = [torch.zeros_like(t) for _ in range(world)]
-        tdist.all_gather(gathered, t)
-        ms = max(float(g[0]) for g in gathered)
-        n_total = sum(float(g[1]) for g in gathered)
-    else:
-        n_total = float(n_placed)
-    value = n_total / (ms / 1000.0) if ms > 0 else 0.0
+        # Exhaustive arm: every orientation paged at every step.
+        session.greedy(args.warmup)
+        session.stats(reset=True)
+        launches0 = ctx.launches
+        ex_ms, ex_placed = timed_steps(stream, lambda: session.greedy(args.steps), dist)
+        ex_launches = ctx.launches - launches0
+        page_stats = session.stats(reset=True)
+        ex_ms, ex_total = max_over_ranks(ex_ms, len(ex_placed), world)
+        ex_value = ex_total / (ex_ms / 1000.0) if ex_ms > 0 else 0.0
+        ex_sequence = [(p.orientation_index, p.translation) for p in session.placements]
+
+        ln_value, ln_ms, ln_placed, fallbacks, ln_launches, ln_sequence = None, None, [], 0, 0, []
+        if learned:
+            net = proposal.Proposal(seed=0, context=ctx)
+            net.load(weights)
+            reset_layout(session)
+            proposal.greedy_proposed(session, net, k, args.warmup)
+            launches0 = ctx.launches
+            ln_ms, (ln_placed, fallbacks) = timed_steps(
+                stream, lambda: proposal.greedy_proposed(session, net, k, args.steps), dist)
+            ln_launches = ctx.launches - launches0
+            ln_ms, ln_total = max_over_ranks(ln_ms, len(ln_placed), world)
+            ln_value = ln_total / (ln_ms / 1000.0) if ln_ms > 0 else 0.0
+            ln_sequence = [(p.orientation_index, p.translation) for p in session.placements]
 
     if args.no_extras:
         if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": round(value, 4), "unit": UNIT, "profiling_run": True,
-                              "ms_per_step": round(ms / max(n_placed, 1), 4), "gpu_launches": int(launches),
+            print(json.dumps({"metric": METRIC, "value": round(ln_value if learned else ex_value, 4), "unit": UNIT,
+                              "profiling_run": True, "exhaustive_value": round(ex_value, 4),
+                              "ms_per_step": round((ln_ms if learned else ex_ms) / max(args.steps, 1), 4),
+                              "gpu_launches": int(ln_launches if learned else ex_launches),
                               "page_stats": page_stats}))
         session.close()
         ctx.close()
         return
+
     # Roofline of pass A (the dominant spectral pass), timed with events on the
-    # context stream around each launch during two further greedy steps.
+    # context stream around each launch during two further exhaustive steps.
     lib.spk_context_set_profiling(ctx.handle, 1)
     session.greedy(2)
     launches_arr = np.zeros(4, np.uint64)
@@ -180,46 +229,71 @@ def run_ours(args, rank, world, local_rank):
     pass_share = {name: round(float(total_ms[i] / max(total_ms.sum(), 1e-9)), 3)
                   for i, name in enumerate(["spectral_z", "inverse_y", "inverse_x_epilogue", "merge_exact"])}
 
-    # End to end through the public API with host buffers: queries in, pages out.
+    # End to end through the public API with host buffers: the proposal
+    # (predictions out), page queries in, pages out, the chosen copy placed.
     e2e_steps = max(1, min(args.steps, 8))
-    O = len(session.catalog)
+    pipeline = pkg("pipeline")
     torch.cuda.synchronize()
     t1 = time.perf_counter()
-    e2e_placed = 0
+    e2e_placed, h2d, d2h = 0, 0, 0
     for _ in range(e2e_steps):
-        pages = session.pages(range(O))
-        heads = [(p[0].score, p[0].orientation_index, p[0].translation[2], p[0].translation[1],
-                  p[0].translation[0], p[0]) for p in pages if p]
+        if learned:
+            orients, _ = proposal.propose(session, net, k)
+            orients = [int(o) for o in orients]
+            d2h += 4 * O + 8 * k
+        else:
+            orients = list(range(O))
+        pages = session.pages(orients)
+        h2d += ctypes.sizeof(pipeline.PageQueryC) * len(orients)
+        d2h += (ctypes.sizeof(pipeline.CandidateC) * 32 + 4 + ctypes.sizeof(pipeline.PageReportC)) * len(orients)
+        heads = [next(c for c in p if c.direct_zero_overlap) for p in pages if any(c.direct_zero_overlap for c in p)]
+        if not heads and learned:
+            pages = session.pages(range(O))
+            h2d += ctypes.sizeof(pipeline.PageQueryC) * O
+            d2h += (ctypes.sizeof(pipeline.CandidateC) * 32 + 4 + ctypes.sizeof(pipeline.PageReportC)) * O
+            heads = [next(c for c in p if c.direct_zero_overlap) for p in pages if any(c.direct_zero_overlap for c in p)]
         if not heads:
             break
-        best = min(heads, key=lambda h: h[:5])[5]
+        best = min(heads, key=lambda c: (c.score, c.orientation_index, c.translation[2], c.translation[1],
+                                         c.translation[0]))
         session.place(best.orientation_index, best.translation)
+        h2d += 8 + 24
         e2e_placed += 1
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t1
-    query_bytes = ctypes.sizeof(pkg("pipeline").PageQueryC) * O + 8 + 24
-    page_bytes = (ctypes.sizeof(pkg("pipeline").CandidateC) * 32 + 4 + ctypes.sizeof(pkg("pipeline").PageReportC)) * O
     e2e = {"value": round(e2e_placed / e2e_s, 4) if e2e_s > 0 else 0.0, "unit": UNIT,
-           "h2d_bytes_per_step": int(query_bytes), "d2h_bytes_per_step": int(page_bytes), "steps": e2e_placed}
+           "h2d_bytes_per_step": int(h2d / max(e2e_placed, 1)), "d2h_bytes_per_step": int(d2h / max(e2e_placed, 1)),
+           "steps": e2e_placed, "path": "propose + pages + place" if learned else "pages + place"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl, O)
 
     if rank == 0:
+        value = ln_value if learned else ex_value
+        ms = ln_ms if learned else ex_ms
+        same = 0
+        for a, b in zip(ex_sequence, ln_sequence):
+            if a != b:
+                break
+            same += 1
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms / max(n_placed, 1), 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32 spectra, fp64 exact scores, u8 fields",
+            "warmup": args.warmup, "ms_per_step": round(ms / max(args.steps, 1), 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 spectra, fp64 exact scores, u8 fields, bf16 proposal network",
             "data": "synthetic (seeded rounded-box STL container, spherical-harmonic blob item, seeded SO(3) catalog)",
             "config": {"workload": wl.name, "grid": list(session.environment_shape), "fft": list(session.fft_shape),
                        "orientations": O, "object_triangles": int(len(wl.obj.triangles)),
                        "container_triangles": int(len(wl.container.triangles)) if hasattr(wl.container, "triangles")
-                       else 0, "mode": "exhaustive", "placements_timed": n_placed,
+                       else 0,
+                       "mode": f"learned proposal (top {k} of {O}, exhaustive fallback)" if learned else "exhaustive",
                        "l2": "working set above L2 (all orientations' kernel spectra stay in HBM)",
                        "session_open_s": round(open_s, 2), "parallelism": f"replicas x{world}",
-                       "page_stats": page_stats},
-            "gpu_launches": int(launches),
+                       "page_stats_exhaustive": page_stats},
+            "exhaustive": {"value": round(ex_value, 4), "ms_per_step": round(ex_ms / max(args.steps, 1), 4),
+                           "gpu_launches": int(ex_launches)},
+            "gpu_launches": int(ln_launches if learned else ex_launches),
             "roofline": {"bound": "hbm", "kernel": "pass_a256_kernel (spectral z pass)",
                          "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4),
@@ -231,9 +305,16 @@ def run_ours(args, rank, world, local_rank):
             "e2e": e2e,
             "clocks": clocks.summary(),
         }
+        if learned:
+            line["proposal"] = {"k": k, "weights": os.path.relpath(weights, os.path.dirname(os.path.abspath(__file__))),
+                                "learned_over_exhaustive": round(value / ex_value, 3) if ex_value else None,
+                                "fallback_steps": int(fallbacks),
+                                "same_placements_as_exhaustive": f"{same} of first {len(ex_sequence)}"}
         if cpu is not None:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
+    if learned:
+        net.close()
     session.close()
     ctx.close()
 
@@ -404,6 +485,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--orientations", type=int, default=0, help="use the first N catalog entries (profiling runs)")
     ap.add_argument("--no-extras", action="store_true", help="skip the roofline and e2e passes (profiling runs)")
+    ap.add_argument("--mode", default="learned", choices=["learned", "exhaustive"],
+                    help="headline path (the exhaustive path is always timed beside it)")
+    ap.add_argument("--k", type=int, default=32, help="orientations the proposal pages per step")
+    ap.add_argument("--weights", default="", help="proposal network parameters (.npz)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
