@@ -110,6 +110,90 @@ __global__ void edt_pass_kernel(std::int32_t* __restrict__ d2, std::int32_t* __r
     }
 }
 
+// The same 1D pass for lines of at most kSharedLineMax cells, with each
+// line's lower-envelope stack in shared memory: one warp handles 32 lines,
+// one per lane.  Lanes hold consecutive lines, so the loads and stores of the
+// y and z passes are coalesced across the warp.  A stack entry is the site q,
+// its value f and the first coordinate it wins from, clamped to
+// [-1, length]: a site whose interval lies wholly outside [0, length) wins no
+// cell, so the clamp changes no output value.
+constexpr int kSharedLineMax = 512;
+
+__global__ void __launch_bounds__(32) edt_pass_shared_kernel(std::int32_t* __restrict__ d2, int sx, int sy, int sz,
+                                                             int axis)
+{
+    extern __shared__ __align__(16) unsigned char stack_raw[];
+    const int length = axis == 0 ? sx : axis == 1 ? sy : sz;
+    std::int32_t* sf = reinterpret_cast<std::int32_t*>(stack_raw);       // [length][32]
+    std::int16_t* sq = reinterpret_cast<std::int16_t*>(sf + length * 32);  // [length][32]
+    std::int16_t* ss = sq + length * 32;                                  // [length][32]
+    const int lane = threadIdx.x;
+    const long long lines = static_cast<long long>(sx) * sy * sz / length;
+    const long long line = static_cast<long long>(blockIdx.x) * 32 + lane;
+    if (line >= lines) {
+        return;
+    }
+    long long base, stride;
+    if (axis == 0) {
+        base = line * sx;
+        stride = 1;
+    }
+    else if (axis == 1) {
+        const long long x = line % sx, z = line / sx;
+        base = x + z * static_cast<long long>(sx) * sy;
+        stride = sx;
+    }
+    else {
+        base = line;
+        stride = static_cast<long long>(sx) * sy;
+    }
+    int count = 0;
+    for (int q = 0; q < length; ++q) {
+        const std::int32_t f = d2[base + q * stride];
+        if (f == kInf) {
+            continue;
+        }
+        int start = -1;
+        while (count > 0) {
+            const int top = (count - 1) * 32 + lane;
+            const long long p = sq[top];
+            const long long numerator = static_cast<long long>(f) - sf[top] + 1LL * q * q - p * p;
+            const long long denominator = 2LL * (q - p);  // positive: q > p
+            long long quotient = numerator / denominator;
+            if (numerator % denominator != 0 && numerator < 0) {
+                --quotient;
+            }
+            const long long first = quotient + 1;
+            start = first < -1 ? -1 : first > length ? length : static_cast<int>(first);
+            if (start > ss[top]) {
+                break;
+            }
+            --count;
+        }
+        if (count == 0) {
+            start = -1;
+        }
+        const int slot = count * 32 + lane;
+        sf[slot] = f;
+        sq[slot] = static_cast<std::int16_t>(q);
+        ss[slot] = static_cast<std::int16_t>(start);
+        ++count;
+    }
+    int site = 0;
+    for (int q = 0; q < length; ++q) {
+        const long long at = base + q * stride;
+        if (count == 0) {
+            d2[at] = kInf;
+            continue;
+        }
+        while (site + 1 < count && ss[(site + 1) * 32 + lane] <= q) {
+            ++site;
+        }
+        const long long delta = q - sq[site * 32 + lane];
+        d2[at] = static_cast<std::int32_t>(sf[site * 32 + lane] + delta * delta);
+    }
+}
+
 __global__ void proximity_gather_kernel(const std::int32_t* __restrict__ d2, const double* __restrict__ table,
                                         double* __restrict__ out, long long n)
 {
@@ -185,10 +269,23 @@ int edt_squared(spk_context* ctx, const std::uint8_t* d_occupied, std::int32_t* 
     }
     edt_init_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(d_occupied, d_d2, n);
     ctx->launches++;
+    static std::once_flag attribute[64];
+    int device = 0;
+    cudaGetDevice(&device);
+    std::call_once(attribute[device & 63], [] {
+        cudaFuncSetAttribute(edt_pass_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSharedLineMax * 32 * 8);
+    });
     for (int axis = 0; axis != 3; ++axis) {
         const long long lines = n / shape[axis];
-        edt_pass_kernel<<<static_cast<unsigned>((lines + 127) / 128), 128, 0, stream>>>(
-            d_d2, line_f, site_q, site_s, shape[0], shape[1], shape[2], axis);
+        if (shape[axis] <= static_cast<std::uint32_t>(kSharedLineMax)) {
+            edt_pass_shared_kernel<<<static_cast<unsigned>((lines + 31) / 32), 32, shape[axis] * 32 * 8, stream>>>(
+                d_d2, shape[0], shape[1], shape[2], axis);
+        }
+        else {
+            edt_pass_kernel<<<static_cast<unsigned>((lines + 127) / 128), 128, 0, stream>>>(
+                d_d2, line_f, site_q, site_s, shape[0], shape[1], shape[2], axis);
+        }
         ctx->launches++;
     }
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -207,6 +208,7 @@ struct Session {
     bool dirty { true };
     __nv_bfloat16* items {};  // every orientation's kernel pooled to 32^3 (proposal input)
     bool items_ready {};
+    std::uint64_t items_tag {};  // unique per session: names the pooled items for the network's cache
 };
 
 Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
@@ -495,6 +497,8 @@ int session_items(spk_context* ctx, Session& s)
         cudaGetLastError();
         return kCuda;
     }
+    static std::atomic<std::uint64_t> next_tag { 1 };
+    s.items_tag = next_tag++;
     s.items_ready = true;
     return kOk;
 }
@@ -532,7 +536,8 @@ int session_predict(spk_context* ctx, Session& s, ProposalNet* net, std::vector<
     if (!d) {
         return status;
     }
-    if ((status = proposal_predict(ctx, net, static_cast<std::uint32_t>(O), crop, nullptr, s.items, nullptr, d))) {
+    if ((status = proposal_predict(ctx, net, static_cast<std::uint32_t>(O), crop, nullptr, s.items, nullptr, s.items_tag,
+                                   d))) {
         return status;
     }
     pred.resize(O);

@@ -203,6 +203,20 @@ __device__ __forceinline__ void warp_insert(unsigned long long& lo, unsigned lon
     hi = warp_bitonic_finish(hi < rev ? hi : rev, lane);
 }
 
+// Merges 32 keys (one per lane, any order) into the warp's 64 smallest.
+__device__ __forceinline__ void warp_merge32(unsigned long long& lo, unsigned long long& hi, unsigned long long key,
+                                             int lane)
+{
+    key = warp_sort32(key, lane);
+    unsigned long long rev = __shfl_sync(kFull, key, 31 - lane);
+    const unsigned long long small = lo < rev ? lo : rev;
+    const unsigned long long large = lo < rev ? rev : lo;
+    lo = warp_bitonic_finish(small, lane);
+    const unsigned long long spill = warp_bitonic_finish(large, lane);
+    rev = __shfl_sync(kFull, spill, 31 - lane);
+    hi = warp_bitonic_finish(hi < rev ? hi : rev, lane);
+}
+
 // Pass B2: inverse FFT along x for 8 legal rows, then the fused epilogue.
 // mode 0: warp top-32 lists + pruning bound in *tau; mode 1: append every
 // candidate whose approximate score is <= threshold and count every candidate
@@ -401,6 +415,7 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
 {
     __shared__ float2 tw[256];
     __shared__ float2 lines[16 * kRegLine];
+    __shared__ unsigned long long pending[8][64];  // per warp: keys waiting to be merged
     tw[threadIdx.x] = twiddles[threadIdx.x];
     __syncthreads();
     const int t = threadIdx.x & 15;  // lane within the row (coalesced direction)
@@ -429,6 +444,9 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     const double t65z = valid ? t65[zz] : 0.0;
     const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
     unsigned long long list_lo = kEmptyKey, list_hi = kEmptyKey;
+    unsigned long long worst = kEmptyKey;
+    int waiting = 0;  // warp-uniform count of staged keys
+    const int warp = threadIdx.x >> 5;
     float residual = 0.f;
     // Keys above the request's pruning bound cannot enter the merged top-64:
     // drop them before the warp sort (the bound only ever decreases).
@@ -456,7 +474,28 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
             }
         }
         if (mode == 0) {
-            warp_insert(list_lo, list_hi, key, lane);
+            // Stage keys below the warp's current 64th; merge 32 at a time.
+            const bool qualifies = key < worst;
+            const unsigned mask = __ballot_sync(kFull, qualifies);
+            if (mask) {
+                if (qualifies) {
+                    pending[warp][waiting + __popc(mask & ((1u << lane) - 1u))] = key;
+                }
+                waiting += __popc(mask);
+                if (waiting >= 32) {
+                    __syncwarp();
+                    warp_merge32(list_lo, list_hi, pending[warp][lane], lane);
+                    const int rest = waiting - 32;
+                    const unsigned long long carry = lane < rest ? pending[warp][32 + lane] : kEmptyKey;
+                    __syncwarp();
+                    if (lane < rest) {
+                        pending[warp][lane] = carry;
+                    }
+                    __syncwarp();
+                    waiting = rest;
+                    worst = __shfl_sync(kFull, list_hi, 31);
+                }
+            }
         }
         else {
             const unsigned mask = __ballot_sync(kFull, take);
@@ -479,45 +518,74 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     if (lane == 0 && residual > 0.f) {
         atomicMax(resid, static_cast<unsigned long long>(__float_as_uint(residual)));
     }
+    if (mode == 0 && waiting > 0) {
+        __syncwarp();
+        warp_merge32(list_lo, list_hi, lane < waiting ? pending[warp][lane] : kEmptyKey, lane);
+    }
     if (mode == 0) {
-        const unsigned long long bound = *reinterpret_cast<volatile unsigned long long*>(tau);
-        for (int half = 0; half < 2; ++half) {
-            const unsigned long long kv = half ? list_hi : list_lo;
-            const bool take = kv != kEmptyKey && kv <= bound;
-            const unsigned mask = __ballot_sync(kFull, take);
-            if (mask) {
-                unsigned int slot = 0;
-                if (lane == 0) {
-                    slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
-                }
-                slot = __shfl_sync(kFull, slot, 0);
-                const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
-                if (take && slot + rank < cap) {
-                    keys[slot + rank] = kv;
-                }
+        // Block top-64: the eight warp lists merge pairwise through shared
+        // memory, and only the block's list is emitted, so an orientation
+        // emits at most 64 keys per block and its key range never overflows.
+        __syncthreads();
+        pending[warp][lane] = list_lo;
+        pending[warp][32 + lane] = list_hi;
+        for (int step = 1; step < 8; step <<= 1) {
+            __syncthreads();
+            const bool merging = (warp & (2 * step - 1)) == 0;
+            if (merging) {
+                warp_merge32(list_lo, list_hi, pending[warp + step][lane], lane);
+                warp_merge32(list_lo, list_hi, pending[warp + step][32 + lane], lane);
+            }
+            __syncthreads();
+            if (merging) {
+                pending[warp][lane] = list_lo;
+                pending[warp][32 + lane] = list_hi;
             }
         }
-        const unsigned long long worst = __shfl_sync(kFull, list_hi, 31);
-        if (lane == 0 && worst != kEmptyKey) {
-            atomicMin(tau, worst);
+        if (warp == 0) {
+            const unsigned long long worst = __shfl_sync(kFull, list_hi, 31);
+            unsigned long long bound = 0;
+            if (lane == 0) {
+                if (worst != kEmptyKey) {
+                    const unsigned long long before = atomicMin(tau, worst);
+                    bound = before < worst ? before : worst;
+                }
+                else {
+                    bound = *reinterpret_cast<volatile unsigned long long*>(tau);
+                }
+            }
+            bound = __shfl_sync(kFull, bound, 0);
+            for (int half = 0; half < 2; ++half) {
+                const unsigned long long kv = half ? list_hi : list_lo;
+                const bool take = kv != kEmptyKey && kv <= bound;
+                const unsigned mask = __ballot_sync(kFull, take);
+                if (mask) {
+                    unsigned int slot = 0;
+                    if (lane == 0) {
+                        slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+                    }
+                    slot = __shfl_sync(kFull, slot, 0);
+                    const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+                    if (take && slot + rank < cap) {
+                        keys[slot + rank] = kv;
+                    }
+                }
+            }
         }
     }
 }
 
-// Sorts up to kKeyCapacity keys of one request and keeps the smallest
-// kExactPerOrientation + 1 (padded with kEmptyKey).
-__global__ void merge_kernel(const unsigned long long* __restrict__ keys, const unsigned int* __restrict__ counts,
-                             unsigned long long* __restrict__ selected)
+// Bitonic sort of n <= capacity keys in shared memory (padded with kEmptyKey
+// to a power of two); the block then holds them in ascending order in s[].
+__device__ unsigned int block_sort(const unsigned long long* __restrict__ src, unsigned int n,
+                                   unsigned long long* s)
 {
-    __shared__ unsigned long long s[kKeyCapacity];
-    const int r = blockIdx.x;
-    const unsigned int n = min(counts[r], kKeyCapacity);
     unsigned int size = 1;
     while (size < n) {
         size <<= 1;
     }
     for (unsigned int i = threadIdx.x; i < size; i += blockDim.x) {
-        s[i] = i < n ? keys[static_cast<long long>(r) * kKeyCapacity + i] : kEmptyKey;
+        s[i] = i < n ? src[i] : kEmptyKey;
     }
     __syncthreads();
     for (unsigned int k = 2; k <= size; k <<= 1) {
@@ -536,9 +604,47 @@ __global__ void merge_kernel(const unsigned long long* __restrict__ keys, const 
             __syncthreads();
         }
     }
+    return size;
+}
+
+// Keeps the smallest kExactPerOrientation + 1 keys of each request: request
+// r's keys start at keys + r * stride and number min(counts[r], limit) (or
+// `limit` when counts is null).  Dynamic shared memory holds `limit` keys.
+__global__ void merge_kernel(const unsigned long long* __restrict__ keys, long long stride,
+                             const unsigned int* __restrict__ counts, unsigned int limit,
+                             unsigned long long* __restrict__ selected)
+{
+    extern __shared__ unsigned long long sorted[];
+    const int r = blockIdx.x;
+    const unsigned int n = counts ? min(counts[r], limit) : limit;
+    const unsigned int size = block_sort(keys + static_cast<long long>(r) * stride, n, sorted);
     for (int i = threadIdx.x; i <= kExactPerOrientation; i += blockDim.x) {
         selected[static_cast<long long>(r) * (kExactPerOrientation + 1) + i] =
-            static_cast<unsigned int>(i) < size ? s[i] : kEmptyKey;
+            static_cast<unsigned int>(i) < size ? sorted[i] : kEmptyKey;
+    }
+}
+
+// First stage for large key ranges: chunk c (kKeyCapacity keys) of request r
+// keeps its smallest kExactPerOrientation + 1 keys in
+// partial[(r * chunks + c) * (kExactPerOrientation + 1) ...].
+__global__ void merge_chunk_kernel(const unsigned long long* __restrict__ keys, unsigned int cap,
+                                   const unsigned int* __restrict__ counts, unsigned long long* __restrict__ partial)
+{
+    __shared__ unsigned long long sorted[kKeyCapacity];
+    const int c = blockIdx.x, r = blockIdx.y, chunks = gridDim.x;
+    const unsigned int n_r = min(counts[r], cap);
+    const unsigned int begin = static_cast<unsigned int>(c) * kKeyCapacity;
+    const unsigned int n = begin < n_r ? min(kKeyCapacity, n_r - begin) : 0u;
+    unsigned long long* out = partial + (static_cast<long long>(r) * chunks + c) * (kExactPerOrientation + 1);
+    if (n == 0) {
+        for (int i = threadIdx.x; i <= kExactPerOrientation; i += blockDim.x) {
+            out[i] = kEmptyKey;
+        }
+        return;
+    }
+    const unsigned int size = block_sort(keys + static_cast<long long>(r) * cap + begin, n, sorted);
+    for (int i = threadIdx.x; i <= kExactPerOrientation; i += blockDim.x) {
+        out[i] = static_cast<unsigned int>(i) < size ? sorted[i] : kEmptyKey;
     }
 }
 
@@ -910,8 +1016,15 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
     cudaStream_t st = ctx_->stream;
     int status = kOk;
     const int per = kExactPerOrientation + 1;
+    // 256^3 grids emit at most 64 keys per pass-B2 block (4096 blocks at most),
+    // so their key range cannot overflow; other grids keep kKeyCapacity.
+    const bool large = L_[0] == 256 && L_[1] == 256 && L_[2] == 256;
+    const unsigned int cap = large ? kLargeKeyChunks * kKeyCapacity : kKeyCapacity;
     auto* keys = static_cast<unsigned long long*>(
-        device_buffer(ctx_, "pipe.keys", static_cast<std::size_t>(R) * kKeyCapacity * 8, status));
+        device_buffer(ctx_, "pipe.keys", static_cast<std::size_t>(R) * cap * 8, status));
+    auto* partial = large ? static_cast<unsigned long long*>(device_buffer(
+                                ctx_, "pipe.partial", static_cast<std::size_t>(R) * kLargeKeyChunks * per * 8, status))
+                          : nullptr;
     auto* meta = static_cast<unsigned long long*>(device_buffer(ctx_, "pipe.meta", static_cast<std::size_t>(R) * 24,
                                                                 status));
     auto* selected = static_cast<unsigned long long*>(
@@ -921,7 +1034,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         device_buffer(ctx_, "pipe.ecount", static_cast<std::size_t>(R) * per * 8, status));
     auto* p_out = static_cast<double*>(device_buffer(ctx_, "pipe.ep", static_cast<std::size_t>(R) * per * 8, status));
     auto* range_error = static_cast<int*>(device_buffer(ctx_, "pipe.rangeerr", 16, status));
-    if (!keys || !meta || !selected || !jobs || !counts_out || !p_out || !range_error) {
+    if (!keys || !meta || !selected || !jobs || !counts_out || !p_out || !range_error || (large && !partial)) {
         return status;
     }
     // meta layout: tau[R] (u64), resid[R] (u64), count[R] (u32, in the last third as u64 slots)
@@ -944,14 +1057,30 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         }
         eps_s[r] = approx_epsilon(s) + std::ldexp(1.0, -22);
         floor[r] = requests[r].has_cursor ? requests[r].cursor.score - eps_s[r] : -INFINITY;
-        if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * kKeyCapacity,
-                                      count + r, kKeyCapacity, tau + r, resid + r))) {
+        if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap, count + r, cap,
+                                      tau + r, resid + r))) {
             return status;
         }
     }
     cudaMemcpyAsync(jobs, host_jobs.data(), R * sizeof(ExactJob), cudaMemcpyHostToDevice, st);
     auto ev = pass_begin(ctx_);
-    merge_kernel<<<R, 1024, 0, st>>>(keys, count, selected);
+    if (large) {
+        // The second stage sorts 64 x 65 keys padded to 8192: 64 KB of shared memory.
+        constexpr unsigned padded = 8192;
+        static_assert(kLargeKeyChunks * (kExactPerOrientation + 1) <= padded, "second merge stage exceeds its buffer");
+        static bool merge_configured = false;
+        if (!merge_configured) {
+            cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, padded * 8);
+            merge_configured = true;
+        }
+        merge_chunk_kernel<<<dim3(kLargeKeyChunks, R), 1024, 0, st>>>(keys, cap, count, partial);
+        merge_kernel<<<R, 1024, padded * 8, st>>>(partial, static_cast<long long>(kLargeKeyChunks) * per, nullptr,
+                                                  kLargeKeyChunks * per, selected);
+        ctx_->launches++;
+    }
+    else {
+        merge_kernel<<<R, 1024, kKeyCapacity * 8, st>>>(keys, cap, count, kKeyCapacity, selected);
+    }
     exact_kernel<<<R * per, 256, 0, st>>>(selected, jobs, per, occ_, d2_, table_, E_[0], E_[1], counts_out, p_out,
                                           range_error);
     pass_end(ctx_, 3, ev);
@@ -1034,7 +1163,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
             all.resize(kPageSize);
         }
         unsigned long long excluded = kEmptyKey;
-        if (n > kKeyCapacity) {
+        if (n > cap) {
             excluded = 0;  // overflowed: nothing can be certified
         }
         else {

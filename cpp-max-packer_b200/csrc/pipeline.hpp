@@ -27,6 +27,7 @@ namespace spk {
 constexpr int kPageSize = 32;
 constexpr int kExactPerOrientation = 64;
 constexpr unsigned kKeyCapacity = 4096;
+constexpr unsigned kLargeKeyChunks = 64;  // key range of a 256^3 request: 64 x 4096 = 4096 blocks x 64 keys
 constexpr unsigned long long kEmptyKey = ~0ULL;
 
 struct Candidate {

@@ -50,6 +50,7 @@ struct ConvArgs {
     const bf16* w;       // [cout][kw], kw = 27 * cin_pad, zero padded channels
     const float* bias;   // [cout]
     bf16* out;           // forward: [batch][s_out^3][cout]; data: [batch][s_in^3][cin]
+    float* out_f32;      // forward, when set: the FP32 linear sums (no bias, no ReLU) instead of `out`
     float* partial;      // weight: [split][cout][kw + 1]
     unsigned* error;
     int batch, s_in, s_out, stride, cin, cinp, cout, kw;
@@ -310,7 +311,16 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
                 v[i] = 0.f;
             }
         }
-        if (MODE == kFwd) {
+        if (MODE == kFwd && a.out_f32) {
+            if (row < a.m_total) {
+                float4* dst = reinterpret_cast<float4*>(a.out_f32 + row * a.cout + c0);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+                }
+            }
+        }
+        else if (MODE == kFwd) {
             if (row < a.m_total) {
                 __align__(16) bf16 h[16];
 #pragma unroll
@@ -490,9 +500,23 @@ __global__ void assemble_kernel(const bf16* crops, const std::uint32_t* crop_ind
         const long long crop = crop_index ? crop_index[b] : 0;
         const long long item = item_index ? item_index[b] : b;
         __nv_bfloat162 pair;
-        pair.x = crops[crop * kProposalVoxels + v];
-        pair.y = items[item * kProposalVoxels + v];
+        pair.x = crops ? crops[crop * kProposalVoxels + v] : __float2bfloat16_rn(0.f);
+        pair.y = items ? items[item * kProposalVoxels + v] : __float2bfloat16_rn(0.f);
         reinterpret_cast<__nv_bfloat162*>(x0)[i] = pair;
+    }
+}
+
+// First-layer activation from its two linear halves: the item channel's sums
+// (per sample) plus the layout channel's sums (shared by every sample).
+__global__ void combine_first_kernel(const float* item_half, const float* crop_half, const float* bias, int batch,
+                                     int cout, bf16* act)
+{
+    const long long per = static_cast<long long>(kProposalVoxels) * cout;
+    const long long total = per * batch;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long j = i % per;
+        act[i] = __float2bfloat16_rn(fmaxf(item_half[i] + crop_half[j] + bias[j % cout], 0.f));
     }
 }
 
@@ -581,6 +605,15 @@ struct ProposalNet {
     float* partial {};
     std::size_t partial_bytes {};
     unsigned* error {};
+    // Parameter version (bumped whenever the parameters change) and the cached
+    // first-layer sums of a fixed set of item channels (the session path).
+    std::uint64_t version { 1 };
+    float* item_half {};
+    std::size_t item_half_capacity {};
+    std::uint64_t item_half_tag {};
+    std::uint32_t item_half_batch {};
+    std::uint64_t item_half_version {};
+    float* crop_half {};
     std::vector<void*> owned;
 };
 
@@ -601,13 +634,15 @@ int alloc(ProposalNet* net, T*& p, std::size_t count)
     return kOk;
 }
 
-void release(ProposalNet* net, void* p)
+template <typename T>
+void release(ProposalNet* net, T*& p)
 {
     if (!p) {
         return;
     }
     cudaFree(p);
-    net->owned.erase(std::remove(net->owned.begin(), net->owned.end(), p), net->owned.end());
+    net->owned.erase(std::remove(net->owned.begin(), net->owned.end(), static_cast<void*>(p)), net->owned.end());
+    p = nullptr;
 }
 
 int ensure_batch(ProposalNet* net, std::uint32_t batch)
@@ -620,9 +655,11 @@ int ensure_batch(ProposalNet* net, std::uint32_t batch)
         release(net, net->act[l]);
         release(net, net->dpre[l]);
     }
-    for (float* p : { net->pred, net->labels, net->pooled, net->dpred, net->loss_terms }) {
-        release(net, p);
-    }
+    release(net, net->pred);
+    release(net, net->labels);
+    release(net, net->pooled);
+    release(net, net->dpred);
+    release(net, net->loss_terms);
     net->capacity = 0;
     int s = alloc(net, net->x0, static_cast<std::size_t>(batch) * kProposalVoxels * 2);
     for (int l = 0; l < kProposalLayers && !s; ++l) {
@@ -671,18 +708,26 @@ ConvArgs layer_args(ProposalNet* net, int l, std::uint32_t batch)
     return a;
 }
 
-int launch_forward(spk_context* ctx, ProposalNet* net, std::uint32_t batch)
+void launch_conv_forward(spk_context* ctx, ProposalNet* net, int l, std::uint32_t batch, const bf16* x, bf16* out,
+                         float* out_f32)
+{
+    ConvArgs a = layer_args(net, l, batch);
+    a.x = x;
+    a.out = out;
+    a.out_f32 = out_f32;
+    a.m_total = static_cast<long long>(batch) * a.s_out * a.s_out * a.s_out;
+    a.k_total = a.kw;
+    const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
+    const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
+    conv_kernel<kFwd><<<blocks, kThreads, smem, ctx->stream>>>(a);
+    ctx->launches++;
+}
+
+int launch_forward(spk_context* ctx, ProposalNet* net, std::uint32_t batch, int first = 0)
 {
     set_smem_attribute<kFwd>();
-    for (int l = 0; l < kProposalLayers; ++l) {
-        ConvArgs a = layer_args(net, l, batch);
-        a.out = net->act[l];
-        a.m_total = static_cast<long long>(batch) * a.s_out * a.s_out * a.s_out;
-        a.k_total = a.kw;
-        const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
-        const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
-        conv_kernel<kFwd><<<blocks, kThreads, smem, ctx->stream>>>(a);
-        ctx->launches++;
+    for (int l = first; l < kProposalLayers; ++l) {
+        launch_conv_forward(ctx, net, l, batch, l == 0 ? net->x0 : net->act[l - 1], net->act[l], nullptr);
     }
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
@@ -718,7 +763,6 @@ int launch_gradients(spk_context* ctx, ProposalNet* net, std::uint32_t batch)
             const std::size_t need = static_cast<std::size_t>(splits) * a.cout * (a.kw + 1) * sizeof(float);
             if (need > net->partial_bytes) {
                 release(net, net->partial);
-                net->partial = nullptr;
                 net->partial_bytes = 0;
                 if ((status = alloc(net, net->partial, need / sizeof(float)))) {
                     return status;
@@ -803,17 +847,60 @@ std::uint64_t proposal_parameter_count()
 }
 
 int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const bf16* crops,
-                     const std::uint32_t* crop_index, const bf16* items, const std::uint32_t* item_index, float* pred)
+                     const std::uint32_t* crop_index, const bf16* items, const std::uint32_t* item_index,
+                     std::uint64_t items_tag, float* pred)
 {
     int status = ensure_batch(net, batch);
     if (status) {
         return status;
     }
-    assemble_kernel<<<grid_for(static_cast<long long>(batch) * kProposalVoxels), 256, 0, ctx->stream>>>(
-        crops, crop_index, items, item_index, static_cast<int>(batch), net->x0);
-    ctx->launches++;
-    if ((status = launch_forward(ctx, net, batch))) {
-        return status;
+    const int grid1 = kProposalGrid;  // first-layer output side (stride 1)
+    const int c1 = kProposalSpec[0].cout;
+    if (!crop_index && !item_index && crops && items && items_tag) {
+        // One layout scored against fixed items: the first convolution is
+        // linear in its two input channels, so the item channel's sums are
+        // computed once per (items, batch, parameters) and only the layout
+        // channel's sums (one sample) are computed per call.
+        set_smem_attribute<kFwd>();
+        const std::size_t half = static_cast<std::size_t>(batch) * grid1 * grid1 * grid1 * c1;
+        if (net->item_half_tag != items_tag || net->item_half_batch != batch ||
+            net->item_half_version != net->version) {
+            if (half > net->item_half_capacity) {
+                release(net, net->item_half);
+                net->item_half_capacity = 0;
+                if ((status = alloc(net, net->item_half, half))) {
+                    return status;
+                }
+                net->item_half_capacity = half;
+            }
+            assemble_kernel<<<grid_for(static_cast<long long>(batch) * kProposalVoxels), 256, 0, ctx->stream>>>(
+                nullptr, nullptr, items, nullptr, static_cast<int>(batch), net->x0);
+            launch_conv_forward(ctx, net, 0, batch, net->x0, nullptr, net->item_half);
+            ctx->launches++;
+            net->item_half_tag = items_tag;
+            net->item_half_batch = batch;
+            net->item_half_version = net->version;
+        }
+        if (!net->crop_half && (status = alloc(net, net->crop_half, static_cast<std::size_t>(kProposalVoxels) * c1))) {
+            return status;
+        }
+        assemble_kernel<<<grid_for(kProposalVoxels), 256, 0, ctx->stream>>>(crops, nullptr, nullptr, nullptr, 1,
+                                                                            net->x0);
+        launch_conv_forward(ctx, net, 0, 1, net->x0, nullptr, net->crop_half);
+        combine_first_kernel<<<grid_for(static_cast<long long>(half)), 256, 0, ctx->stream>>>(
+            net->item_half, net->crop_half, net->params + net->b_off[0], static_cast<int>(batch), c1, net->act[0]);
+        ctx->launches += 2;
+        if ((status = launch_forward(ctx, net, batch, 1))) {
+            return status;
+        }
+    }
+    else {
+        assemble_kernel<<<grid_for(static_cast<long long>(batch) * kProposalVoxels), 256, 0, ctx->stream>>>(
+            crops, crop_index, items, item_index, static_cast<int>(batch), net->x0);
+        ctx->launches++;
+        if ((status = launch_forward(ctx, net, batch))) {
+            return status;
+        }
     }
     head_kernel<<<batch, 64, 0, ctx->stream>>>(net->act[3], net->params + net->head_w, net->params + net->head_b,
                                                 static_cast<int>(batch), nullptr, pred, nullptr, nullptr, nullptr,
@@ -979,6 +1066,7 @@ int spk_proposal_set_parameters(spk_context* ctx, spk_proposal* p, const float* 
     cudaMemsetAsync(net->adam_m, 0, sizeof(float) * net->count, ctx->stream);
     cudaMemsetAsync(net->adam_v, 0, sizeof(float) * net->count, ctx->stream);
     net->adam_t = 0;
+    net->version++;
     int s = spk::pack_all(ctx, net);
     if (!s && cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         cudaGetLastError();
@@ -1105,6 +1193,7 @@ int spk_proposal_train(spk_context* ctx, spk_proposal* p, const spk_proposal_dat
                 return s;
             }
             net->adam_t += 1;
+            net->version++;
             const float c1 = 1.f - std::pow(b1, static_cast<float>(net->adam_t));
             const float c2 = 1.f - std::pow(b2, static_cast<float>(net->adam_t));
             spk::adam_kernel<<<spk::grid_for(static_cast<long long>(net->count)), 256, 0, ctx->stream>>>(

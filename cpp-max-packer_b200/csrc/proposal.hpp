@@ -46,10 +46,13 @@ std::uint64_t proposal_parameter_count();
 // Scores `batch` samples whose inputs are assembled on the device from pooled
 // layouts and pooled items: sample b uses crops[crop_index[b]] (or crops[0]
 // when crop_index is null) and items[item_index[b]] (or items[b] when null).
-// Predictions land in device memory `pred` (batch floats).
+// Predictions land in device memory `pred` (batch floats).  A nonzero
+// `items_tag` names an unchanging set of item channels (one layout scored
+// against the same items again and again, crop_index and item_index null):
+// the first layer's item sums are then cached per (tag, batch, parameters).
 int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const __nv_bfloat16* crops,
                      const std::uint32_t* crop_index, const __nv_bfloat16* items, const std::uint32_t* item_index,
-                     float* pred);
+                     std::uint64_t items_tag, float* pred);
 
 // Device pooling helpers (bf16 32^3 outputs, [z][y][x]).
 int pool_occupancy(spk_context* ctx, const std::uint8_t* occupancy, const int* shape, __nv_bfloat16* out);

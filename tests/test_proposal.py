@@ -173,3 +173,23 @@ def test_proposed_greedy_places_exact_copies(gpu_ctx, net):
     best, _ = proposal.propose(s, net, 3)
     assert len(best) == 3
     s.close()
+
+
+@pytest.mark.gpu
+def test_session_predictions_match_the_plain_forward(gpu_ctx, net):
+    # The session path caches the first layer's item-channel sums; it must
+    # score exactly what the plain forward pass scores on the same inputs, on
+    # later layouts, and again after the parameters change.
+    proposal = package("proposal")
+    _set_oracle_parameters(net, 4)
+    s, wl = _small_session(gpu_ctx)
+    _, items = proposal.session_features(s)
+    for step in range(3):
+        if step == 2:
+            _set_oracle_parameters(net, 5)
+        crop = proposal.session_crop(s)
+        _, pred = proposal.propose(s, net, 3)
+        want = net.forward(np.stack([np.broadcast_to(crop, items.shape), items], axis=-1))
+        assert np.abs(pred - want).max() <= 2e-3 * np.abs(want).max() + 1e-5, (step, pred, want)
+        s.greedy(1)
+    s.close()
