@@ -148,36 +148,48 @@ __global__ void __launch_bounds__(32) edt_pass_shared_kernel(std::int32_t* __res
         stride = static_cast<long long>(sx) * sy;
     }
     int count = 0;
-    for (int q = 0; q < length; ++q) {
-        const std::int32_t f = d2[base + q * stride];
-        if (f == kInf) {
-            continue;
+    for (int q0 = 0; q0 < length; q0 += 8) {
+        // Eight independent loads in flight before the envelope work.
+        std::int32_t fv[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            fv[i] = q0 + i < length ? d2[base + (q0 + i) * stride] : kInf;
         }
-        int start = -1;
-        while (count > 0) {
-            const int top = (count - 1) * 32 + lane;
-            const long long p = sq[top];
-            const long long numerator = static_cast<long long>(f) - sf[top] + 1LL * q * q - p * p;
-            const long long denominator = 2LL * (q - p);  // positive: q > p
-            long long quotient = numerator / denominator;
-            if (numerator % denominator != 0 && numerator < 0) {
-                --quotient;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int q = q0 + i;
+            const std::int32_t f = fv[i];
+            if (f == kInf) {
+                continue;
             }
-            const long long first = quotient + 1;
-            start = first < -1 ? -1 : first > length ? length : static_cast<int>(first);
-            if (start > ss[top]) {
-                break;
+            int start = -1;
+            while (count > 0) {
+                const int top = (count - 1) * 32 + lane;
+                const long long p = sq[top];
+                const long long numerator = static_cast<long long>(f) - sf[top] + 1LL * q * q - p * p;
+                const long long denominator = 2LL * (q - p);  // positive: q > p
+                // The top site keeps cells before floor(n / d) + 1 when that
+                // exceeds its own first cell S, i.e. when n >= S * d.
+                if (numerator >= static_cast<long long>(ss[top]) * denominator) {
+                    long long quotient = numerator / denominator;
+                    if (numerator % denominator != 0 && numerator < 0) {
+                        --quotient;
+                    }
+                    const long long first = quotient + 1;
+                    start = first < -1 ? -1 : first > length ? length : static_cast<int>(first);
+                    break;
+                }
+                --count;
             }
-            --count;
+            if (count == 0) {
+                start = -1;
+            }
+            const int slot = count * 32 + lane;
+            sf[slot] = f;
+            sq[slot] = static_cast<std::int16_t>(q);
+            ss[slot] = static_cast<std::int16_t>(start);
+            ++count;
         }
-        if (count == 0) {
-            start = -1;
-        }
-        const int slot = count * 32 + lane;
-        sf[slot] = f;
-        sq[slot] = static_cast<std::int16_t>(q);
-        ss[slot] = static_cast<std::int16_t>(start);
-        ++count;
     }
     int site = 0;
     for (int q = 0; q < length; ++q) {

@@ -507,16 +507,29 @@ __global__ void assemble_kernel(const bf16* crops, const std::uint32_t* crop_ind
 }
 
 // First-layer activation from its two linear halves: the item channel's sums
-// (per sample) plus the layout channel's sums (shared by every sample).
-__global__ void combine_first_kernel(const float* item_half, const float* crop_half, const float* bias, int batch,
-                                     int cout, bf16* act)
+// (per sample) plus the layout channel's sums (shared by every sample).  One
+// thread per 8 channels of one voxel (cout is a multiple of 8).
+__global__ void combine_first_kernel(const float* __restrict__ item_half, const float* __restrict__ crop_half,
+                                     const float* __restrict__ bias, int batch, int cout, bf16* __restrict__ act)
 {
-    const long long per = static_cast<long long>(kProposalVoxels) * cout;
+    const int groups = cout / 8;
+    const long long per = static_cast<long long>(kProposalVoxels) * groups;
     const long long total = per * batch;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
         const long long j = i % per;
-        act[i] = __float2bfloat16_rn(fmaxf(item_half[i] + crop_half[j] + bias[j % cout], 0.f));
+        const int c0 = static_cast<int>(j % groups) * 8;
+        const float4* a = reinterpret_cast<const float4*>(item_half + i * 8);
+        const float4* c = reinterpret_cast<const float4*>(crop_half + j * 8);
+        const float4 a0 = __ldcs(a), a1 = __ldcs(a + 1), b0 = c[0], b1 = c[1];
+        const float v[8] = { a0.x + b0.x, a0.y + b0.y, a0.z + b0.z, a0.w + b0.w,
+                             a1.x + b1.x, a1.y + b1.y, a1.z + b1.z, a1.w + b1.w };
+        __align__(16) bf16 h[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            h[k] = __float2bfloat16_rn(fmaxf(v[k] + bias[c0 + k], 0.f));
+        }
+        reinterpret_cast<uint4*>(act)[i] = *reinterpret_cast<const uint4*>(h);
     }
 }
 
@@ -887,7 +900,7 @@ int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, co
         assemble_kernel<<<grid_for(kProposalVoxels), 256, 0, ctx->stream>>>(crops, nullptr, nullptr, nullptr, 1,
                                                                             net->x0);
         launch_conv_forward(ctx, net, 0, 1, net->x0, nullptr, net->crop_half);
-        combine_first_kernel<<<grid_for(static_cast<long long>(half)), 256, 0, ctx->stream>>>(
+        combine_first_kernel<<<grid_for(static_cast<long long>(half / 8)), 256, 0, ctx->stream>>>(
             net->item_half, net->crop_half, net->params + net->b_off[0], static_cast<int>(batch), c1, net->act[0]);
         ctx->launches += 2;
         if ((status = launch_forward(ctx, net, batch, 1))) {

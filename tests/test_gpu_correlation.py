@@ -123,3 +123,18 @@ def test_proximity_field_bit_exact(gpu_ctx, oracle_c):
             got = compute.build_proximity(shape, occ, context=gpu_ctx)
             want, _ = oracle_c.build_proximity(shape, occ)
             assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), shape
+
+
+def test_proximity_long_lines_bit_exact(gpu_ctx, oracle_c):
+    # Lines of 256 and 512 cells (the shared-memory envelope's range) and one
+    # beyond it (the global-memory pass), with sparse sites, dense sites and
+    # runs of occupied cells.
+    compute = package("compute")
+    rng = np.random.default_rng(22)
+    for shape in [(256, 200, 40), (40, 256, 33), (17, 23, 512), (600, 9, 7)]:
+        n = int(np.prod(shape))
+        for density in (0.0005, 0.05, 0.7):
+            occ = (rng.random(n) < density).astype(np.uint8)
+            got = compute.build_proximity(shape, occ, context=gpu_ctx)
+            want, _ = oracle_c.build_proximity(shape, occ)
+            assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), (shape, density)
