@@ -523,25 +523,33 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
         warp_merge32(list_lo, list_hi, lane < waiting ? pending[warp][lane] : kEmptyKey, lane);
     }
     if (mode == 0) {
-        // Block top-64: the eight warp lists merge pairwise through shared
-        // memory, and only the block's list is emitted, so an orientation
-        // emits at most 64 keys per block and its key range never overflows.
+        // Block top-64: the eight sorted warp lists (odd warps stored in
+        // descending order, so neighbours form bitonic runs of 128) finish
+        // as one bitonic sort of 512 keys, one compare-exchange per thread
+        // per stage; only the block's 64 smallest are emitted, so an
+        // orientation emits at most 64 keys per block and its key range
+        // never overflows.
+        unsigned long long* merged = &pending[0][0];
         __syncthreads();
-        pending[warp][lane] = list_lo;
-        pending[warp][32 + lane] = list_hi;
-        for (int step = 1; step < 8; step <<= 1) {
-            __syncthreads();
-            const bool merging = (warp & (2 * step - 1)) == 0;
-            if (merging) {
-                warp_merge32(list_lo, list_hi, pending[warp + step][lane], lane);
-                warp_merge32(list_lo, list_hi, pending[warp + step][32 + lane], lane);
-            }
-            __syncthreads();
-            if (merging) {
-                pending[warp][lane] = list_lo;
-                pending[warp][32 + lane] = list_hi;
+        const bool descending = warp & 1;
+        merged[warp * 64 + (descending ? 63 - lane : lane)] = list_lo;
+        merged[warp * 64 + (descending ? 31 - lane : 32 + lane)] = list_hi;
+        for (int k = 128; k <= 512; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                __syncthreads();
+                const int t = threadIdx.x;
+                const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
+                const int p = i | j;
+                const unsigned long long a = merged[i], b = merged[p];
+                if ((a > b) == ((i & k) == 0)) {
+                    merged[i] = b;
+                    merged[p] = a;
+                }
             }
         }
+        __syncthreads();
+        list_lo = merged[lane];
+        list_hi = merged[32 + lane];
         if (warp == 0) {
             const unsigned long long worst = __shfl_sync(kFull, list_hi, 31);
             unsigned long long bound = 0;
