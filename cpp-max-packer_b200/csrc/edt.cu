@@ -110,6 +110,71 @@ __global__ void edt_pass_kernel(std::int32_t* __restrict__ d2, std::int32_t* __r
     }
 }
 
+// First pass (along x) straight from the occupancy: on a binary line the 1D
+// squared distance is the square of the distance to the nearest occupied
+// cell, found by a left-to-right and a right-to-left sweep.  One warp per
+// line, each lane a run of `per_lane` consecutive cells; warp max/min scans
+// carry the nearest occupied position across lanes.  Lines of up to
+// 32 * kFirstPassPerLane cells.
+constexpr int kFirstPassPerLane = 32;
+
+__global__ void __launch_bounds__(256) edt_first_pass_kernel(const std::uint8_t* __restrict__ occupied,
+                                                            std::int32_t* __restrict__ d2, int sx, long long lines)
+{
+    const int lane = threadIdx.x & 31;
+    const long long line = static_cast<long long>(blockIdx.x) * 8 + (threadIdx.x >> 5);
+    if (line >= lines) {
+        return;  // whole warp: the line index is warp-uniform
+    }
+    const int per_lane = (sx + 31) / 32;
+    const int begin = lane * per_lane;
+    const std::uint8_t* row = occupied + line * sx;
+    std::int32_t* out = d2 + line * sx;
+    constexpr int kNone = 1 << 24;  // beyond any line length
+    std::uint32_t bits = 0;  // occupied cells of this lane's run
+    for (int i = 0; i < per_lane; ++i) {
+        const int x = begin + i;
+        if (x < sx && row[x]) {
+            bits |= 1u << i;
+        }
+    }
+    // Nearest occupied position at or before the end of each earlier run.
+    int last = bits ? begin + 31 - __clz(bits) : -kNone;
+    int first = bits ? begin + __ffs(bits) - 1 : kNone;
+    int left = last, right = first;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int l = __shfl_up_sync(0xffffffffu, left, o);
+        const int r = __shfl_down_sync(0xffffffffu, right, o);
+        if (lane >= o) {
+            left = max(left, l);
+        }
+        if (lane + o < 32) {
+            right = min(right, r);
+        }
+    }
+    // Exclusive: occupied positions strictly in earlier / later runs.
+    int carry_left = __shfl_up_sync(0xffffffffu, left, 1);
+    int carry_right = __shfl_down_sync(0xffffffffu, right, 1);
+    if (lane == 0) {
+        carry_left = -kNone;
+    }
+    if (lane == 31) {
+        carry_right = kNone;
+    }
+    for (int i = 0; i < per_lane; ++i) {
+        const int x = begin + i;
+        if (x >= sx) {
+            break;
+        }
+        const std::uint32_t at_or_after = bits & (~0u << i);
+        const std::uint32_t at_or_before = bits & ((2u << i) - 1u);  // i = 31 wraps to every bit
+        const int nearest_right = at_or_after ? begin + __ffs(at_or_after) - 1 : carry_right;
+        const int nearest_left = at_or_before ? begin + 31 - __clz(at_or_before) : carry_left;
+        const int d = min(x - nearest_left, nearest_right - x);
+        out[x] = d >= kNone / 2 ? kInf : d * d;
+    }
+}
+
 // The same 1D pass for lines of at most kSharedLineMax cells, with each
 // line's lower-envelope stack in shared memory: one warp handles 32 lines,
 // one per lane.  Lanes hold consecutive lines, so the loads and stores of the
@@ -279,7 +344,15 @@ int edt_squared(spk_context* ctx, const std::uint8_t* d_occupied, std::int32_t* 
     if (!line_f || !site_q || !site_s) {
         return status;
     }
-    edt_init_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(d_occupied, d_d2, n);
+    const bool first_fused = shape[0] <= 32u * kFirstPassPerLane;
+    if (first_fused) {
+        const long long lines = n / shape[0];
+        edt_first_pass_kernel<<<static_cast<unsigned>((lines + 7) / 8), 256, 0, stream>>>(d_occupied, d_d2,
+                                                                                          shape[0], lines);
+    }
+    else {
+        edt_init_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(d_occupied, d_d2, n);
+    }
     ctx->launches++;
     static std::once_flag attribute[64];
     int device = 0;
@@ -288,7 +361,7 @@ int edt_squared(spk_context* ctx, const std::uint8_t* d_occupied, std::int32_t* 
         cudaFuncSetAttribute(edt_pass_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSharedLineMax * 32 * 8);
     });
-    for (int axis = 0; axis != 3; ++axis) {
+    for (int axis = first_fused ? 1 : 0; axis != 3; ++axis) {
         const long long lines = n / shape[axis];
         if (shape[axis] <= static_cast<std::uint32_t>(kSharedLineMax)) {
             edt_pass_shared_kernel<<<static_cast<unsigned>((lines + 31) / 32), 32, shape[axis] * 32 * 8, stream>>>(

@@ -94,6 +94,22 @@ __device__ __forceinline__ void put(unsigned char* base, std::uint32_t offset, u
     *reinterpret_cast<uint4*>(base + offset) = v;
 }
 
+// Asynchronous 16-byte copy global -> shared; when `valid` is false nothing
+// is read and the 16 bytes are zero-filled (src is then any mapped address).
+__device__ __forceinline__ void copy16(unsigned char* base, std::uint32_t offset, const void* src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;"
+                 :
+                 : "r"(umma::smem_addr(base + offset)), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void copy_wait()
+{
+    asm volatile("cp.async.wait_group %0;" : : "n"(N) : "memory");
+}
+
 // Input voxel of output voxel `o` through tap (kz, ky, kx); false outside.
 __device__ __forceinline__ bool tap_input(const Vox& o, int tap, int stride, int s_in, int& iz, int& iy, int& ix)
 {
@@ -122,14 +138,15 @@ template <int MODE>
 __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, long long m0, int chunk, int tid,
                                          const Vox& row_vox, bool row_ok)
 {
-    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
     if (MODE == kFwd || MODE == kData) {
         // K-major: thread tid owns row tid; unit j covers K half (j & 1) of K-step (j >> 1).
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int ks = j >> 1, c = j & 1;
             const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + c * 8;
-            uint4 v = zero;
+            const std::uint32_t off = ks * kStepBytesA + umma::unit_offset(tid >> 3, c, tid & 7);
+            const void* src = a.w;
+            bool valid = false;
             if (row_ok && k < a.k_total) {
                 if (MODE == kFwd) {
                     const int tap = static_cast<int>(k / a.cinp), ci0 = static_cast<int>(k % a.cinp);
@@ -137,7 +154,12 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
                     if (tap < 27 && (a.cin >= 8 || ci0 == 0) && tap_input(row_vox, tap, a.stride, a.s_in, iz, iy, ix)) {
                         const long long vi =
                             ((static_cast<long long>(row_vox.n) * a.s_in + iz) * a.s_in + iy) * a.s_in + ix;
-                        v = load_channels(a.x + vi * a.cin, a.cin, ci0);
+                        if (a.cin < 8) {
+                            put(A, off, load_channels(a.x + vi * a.cin, a.cin, ci0));
+                            continue;
+                        }
+                        src = a.x + vi * a.cin + ci0;
+                        valid = true;
                     }
                 }
                 else {
@@ -146,11 +168,12 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
                     if (tap < 27 && tap_output(row_vox, tap, a.stride, a.s_out, qz, qy, qx)) {
                         const long long qi =
                             ((static_cast<long long>(row_vox.n) * a.s_out + qz) * a.s_out + qy) * a.s_out + qx;
-                        v = __ldg(reinterpret_cast<const uint4*>(a.dy + qi * a.cout + co0));
+                        src = a.dy + qi * a.cout + co0;
+                        valid = true;
                     }
                 }
             }
-            put(A, ks * kStepBytesA + umma::unit_offset(tid >> 3, c, tid & 7), v);
+            copy16(A, off, src, valid);
         }
     }
     else {
@@ -161,7 +184,9 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
             const int ks = e >> 8, kk = e & 15, g = (e & 255) >> 4;
             const long long r0 = m0 + 8 * g;
             const long long q = static_cast<long long>(chunk) * kKC + ks * 16 + kk;
-            uint4 v = zero;
+            const std::uint32_t off = ks * kStepBytesA + umma::unit_offset(g, kk >> 3, kk & 7);
+            const void* src = a.w;
+            bool valid = false;
             if (q < a.k_total) {
                 if (r0 < a.kw) {
                     const int tap = static_cast<int>(r0 / a.cinp), ci0 = static_cast<int>(r0 % a.cinp);
@@ -169,14 +194,20 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
                     int iz, iy, ix;
                     if ((a.cin >= 8 || ci0 == 0) && tap_input(o, tap, a.stride, a.s_in, iz, iy, ix)) {
                         const long long vi = ((static_cast<long long>(o.n) * a.s_in + iz) * a.s_in + iy) * a.s_in + ix;
-                        v = load_channels(a.x + vi * a.cin, a.cin, ci0);
+                        if (a.cin < 8) {
+                            put(A, off, load_channels(a.x + vi * a.cin, a.cin, ci0));
+                            continue;
+                        }
+                        src = a.x + vi * a.cin + ci0;
+                        valid = true;
                     }
                 }
                 else if (r0 == a.kw) {
-                    v.x = 0x3F80u;  // bf16 1.0 in row kw: the bias-gradient row
+                    put(A, off, make_uint4(0x3F80u, 0u, 0u, 0u));  // bf16 1.0 in row kw: the bias-gradient row
+                    continue;
                 }
             }
-            put(A, ks * kStepBytesA + umma::unit_offset(g, kk >> 3, kk & 7), v);
+            copy16(A, off, src, valid);
         }
     }
 }
@@ -184,18 +215,19 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
 template <int MODE>
 __device__ __forceinline__ void gather_b(const ConvArgs& a, unsigned char* B, int N, int chunk, int tid)
 {
-    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
     const int units = 4 * N;  // (N / 8) groups x 2 halves x 8 x 2 K-steps
     for (int e = tid; e < units; e += kThreads) {
         const int ks = e / (2 * N), rem = e % (2 * N);
-        uint4 v = zero;
+        const void* src = a.w;
+        bool valid = false;
         std::uint32_t off;
         if (MODE == kFwd) {
             // K-major rows cout.
             const int c = rem / N, co = rem % N;
             const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + c * 8;
             if (k < a.kw) {
-                v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<long long>(co) * a.kw + k));
+                src = a.w + static_cast<long long>(co) * a.kw + k;
+                valid = true;
             }
             off = umma::unit_offset(co >> 3, c, co & 7);
         }
@@ -206,16 +238,17 @@ __device__ __forceinline__ void gather_b(const ConvArgs& a, unsigned char* B, in
             if (MODE == kData) {
                 const int tap = static_cast<int>(k / a.cout), co = static_cast<int>(k % a.cout);
                 if (k < a.k_total && tap < 27) {
-                    v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<long long>(co) * a.kw +
-                                                             tap * a.cinp + 8 * g));
+                    src = a.w + static_cast<long long>(co) * a.kw + tap * a.cinp + 8 * g;
+                    valid = true;
                 }
             }
             else if (k < a.k_total) {
-                v = __ldg(reinterpret_cast<const uint4*>(a.dy + k * a.cout + 8 * g));
+                src = a.dy + k * a.cout + 8 * g;
+                valid = true;
             }
             off = umma::unit_offset(g, kk >> 3, kk & 7);
         }
-        put(B, ks * (N * 32) + off, v);
+        copy16(B, ks * (N * 32) + off, src, valid);
     }
 }
 
@@ -264,20 +297,32 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
     constexpr bool b_mn = MODE != kFwd;
     const std::uint32_t idesc = umma::idesc_bf16(kRows, N, a_mn, b_mn);
 
+    // Gathers run kAhead chunks in front of the MMA as asynchronous copies;
+    // every iteration commits one copy group (possibly empty), so waiting
+    // for all but the newest kAhead - 1 groups means chunk `it` has landed.
+    constexpr int kAhead = kStages - 1;
+    const int n_chunks = c_end - c_begin;
+    auto gather = [&](int it) {
+        unsigned char* A = smem + (it % kStages) * stage_bytes;
+        gather_a<MODE>(a, A, m0, c_begin + it, tid, row_vox, row_ok);
+        gather_b<MODE>(a, A + kRows * kKC * 2, N, c_begin + it, tid);
+    };
     bool ok = true;
-    for (int c = c_begin; c < c_end; ++c) {
-        const int it = c - c_begin, st = it % kStages;
-        if (it >= kStages && !umma::bar_wait(&bars[st], static_cast<std::uint32_t>((it / kStages - 1) & 1))) {
-            ok = false;
+    for (int it = 0; it < kAhead; ++it) {
+        if (it < n_chunks) {
+            gather(it);
         }
-        unsigned char* A = smem + st * stage_bytes;
-        unsigned char* B = A + kRows * kKC * 2;
-        gather_a<MODE>(a, A, m0, c, tid, row_vox, row_ok);
-        gather_b<MODE>(a, B, N, c, tid);
+        copy_commit();
+    }
+    for (int it = 0; it < n_chunks; ++it) {
+        const int st = it % kStages;
+        copy_wait<kAhead - 1>();
         umma::fence_async_smem();
         __syncthreads();
         if (tid == 0) {
             umma::fence_after();
+            unsigned char* A = smem + st * stage_bytes;
+            unsigned char* B = A + kRows * kKC * 2;
 #pragma unroll
             for (int ks = 0; ks < 2; ++ks) {
                 const std::uint64_t da = umma::desc(umma::smem_addr(A + ks * kStepBytesA));
@@ -286,6 +331,15 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
             }
             umma::commit(&bars[st]);
         }
+        const int next = it + kAhead;
+        if (next < n_chunks) {
+            // Stage next % kStages was last read by the MMA of chunk it - 1.
+            if (it >= 1 && !umma::bar_wait(&bars[(it - 1) % kStages], static_cast<std::uint32_t>(((it - 1) / kStages) & 1))) {
+                ok = false;
+            }
+            gather(next);
+        }
+        copy_commit();
     }
     const int n_it = c_end - c_begin;
     if (n_it > 0) {

@@ -131,7 +131,7 @@ def test_proximity_long_lines_bit_exact(gpu_ctx, oracle_c):
     # runs of occupied cells.
     compute = package("compute")
     rng = np.random.default_rng(22)
-    for shape in [(256, 200, 40), (40, 256, 33), (17, 23, 512), (600, 9, 7)]:
+    for shape in [(256, 200, 40), (40, 256, 33), (17, 23, 512), (600, 9, 7), (1100, 5, 3), (1, 300, 2)]:
         n = int(np.prod(shape))
         for density in (0.0005, 0.05, 0.7):
             occ = (rng.random(n) < density).astype(np.uint8)
