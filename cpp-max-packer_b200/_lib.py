@@ -83,6 +83,7 @@ def _declare(h):
     h.spk_context_stream.restype = ctypes.c_void_p
     h.spk_context_set_profiling.argtypes = [P, ctypes.c_int]
     h.spk_context_pass_times.argtypes = [P, P, P, ctypes.c_uint32]
+    h.spk_context_pass_bytes.argtypes = [P, P, ctypes.c_uint32]
     h.spk_estimate_correlation.argtypes = [ctypes.POINTER(CorrelationSpec), ctypes.c_uint32,
                                            ctypes.POINTER(CorrelationEstimateC)]
     for name in ("spk_correlate_binary", "spk_correlate_proximity"):

@@ -1,0 +1,108 @@
+"""Full greedy fill with the learned proposal against the exhaustive fill.
+
+    python cpp-max-packer_b200/compare_fill.py [--workload rounded256_blob_hopf512] [--k 32]
+
+Both fills start from the empty container and run until no orientation
+admits a copy.
+- The exhaustive fill pages every orientation at every step.
+- The learned fill pages the k proposed orientations. It falls back to the
+  exhaustive step whenever none of them admits a copy, so it also ends only
+  when no orientation admits one.
+
+Every placement of either fill is an exact candidate: it has a zero exact
+overlap recount, and its score is the exact FP64 score. Printed per fill:
+- copies placed and the device time;
+- for the learned fill, its fallback steps;
+- the packed-count ratio, learned copies over exhaustive copies.
+"""
+
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pkg(name):
+    return importlib.import_module("cpp-max-packer_b200." + name)
+
+
+def fill(session, step, chunk=64, max_copies=100000, log=print):
+    """Runs `step(n)` (returns the copies placed, and the fallback count)
+    until a call places fewer than asked; returns (copies, fallbacks, seconds)."""
+    copies, fallbacks = 0, 0
+    t0 = time.perf_counter()
+    while copies < max_copies:
+        placed, fb = step(chunk)
+        copies += placed
+        fallbacks += fb
+        if placed < chunk:
+            break
+        if copies % (chunk * 8) == 0:
+            log(f"  {copies} copies, {time.perf_counter() - t0:.1f} s")
+    return copies, fallbacks, time.perf_counter() - t0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="rounded256_blob_hopf512")
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--k", type=int, default=32)
+    ap.add_argument("--weights", default=os.path.join(HERE, "weights", "proposal_rounded256.npz"))
+    ap.add_argument("--max-copies", type=int, default=100000)
+    ap.add_argument("--report", default="")
+    args = ap.parse_args()
+    compute, session_mod, workloads, proposal = pkg("compute"), pkg("session"), pkg("workloads"), pkg("proposal")
+    ctx = compute.Context(0)
+    wl = workloads.WORKLOADS[args.workload](seed=args.seed)
+
+    def open_session():
+        return session_mod.Session(wl.obj, wl.container, wl.origin, wl.pitch, wl.catalog, wl.pair_clearance,
+                                   wl.wall_clearance, context=ctx)
+
+    s = open_session()
+    print("exhaustive fill", flush=True)
+    ex = fill(s, lambda n: (len(s.greedy(n)), 0), max_copies=args.max_copies)
+    ex_scores = [p.score for p in s.placements]
+    s.close()
+    net = proposal.Proposal(seed=0, context=ctx)
+    net.load(args.weights)
+    s = open_session()
+    print("learned fill", flush=True)
+
+    def learned(n):
+        placed, fb = proposal.greedy_proposed(s, net, args.k, n)
+        return len(placed), fb
+
+    ln = fill(s, learned, max_copies=args.max_copies)
+    ln_scores = [p.score for p in s.placements]
+    s.close()
+    report = {
+        "workload": wl.name, "orientations": len(wl.catalog), "k": args.k,
+        "exhaustive": {"copies": ex[0], "seconds": round(ex[2], 2), "placements_per_s": round(ex[0] / ex[2], 3)},
+        "learned": {"copies": ln[0], "fallback_steps": ln[1], "seconds": round(ln[2], 2),
+                    "placements_per_s": round(ln[0] / ln[2], 3)},
+        "packed_count_ratio": round(ln[0] / ex[0], 4) if ex[0] else None,
+        "same_prefix": next((i for i, (a, b) in enumerate(zip(ex_scores, ln_scores)) if a != b),
+                            min(len(ex_scores), len(ln_scores))),
+        "mean_score": {"exhaustive": sum(ex_scores) / max(len(ex_scores), 1),
+                       "learned": sum(ln_scores) / max(len(ln_scores), 1)},
+    }
+    print(json.dumps(report), flush=True)
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(report, f, indent=1)
+    net.close()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

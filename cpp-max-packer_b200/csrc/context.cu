@@ -74,6 +74,18 @@ int spk_context_set_profiling(spk_context* ctx, int enabled)
     for (int i = 0; i < 4; ++i) {
         ctx->pass_launches[i] = 0;
         ctx->pass_ms[i] = 0;
+        ctx->pass_bytes[i] = 0;
+    }
+    return spk::kOk;
+}
+
+int spk_context_pass_bytes(const spk_context* ctx, double* bytes, uint32_t capacity)
+{
+    if (!ctx || !bytes) {
+        return spk::kInvalidArgument;
+    }
+    for (uint32_t i = 0; i < capacity && i < 4; ++i) {
+        bytes[i] = ctx->pass_bytes[i];
     }
     return spk::kOk;
 }

@@ -34,6 +34,7 @@ struct spk_context {
     bool profiling {};
     std::uint64_t pass_launches[4] {};
     double pass_ms[4] {};
+    double pass_bytes[4] {};  // algorithmic bytes of the profiled launches
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;  // (pass, events)
 };
 
@@ -155,11 +156,12 @@ inline std::pair<cudaEvent_t, cudaEvent_t> pass_begin(spk_context* ctx)
     }
     return ev;
 }
-inline void pass_end(spk_context* ctx, int pass, std::pair<cudaEvent_t, cudaEvent_t> ev)
+inline void pass_end(spk_context* ctx, int pass, std::pair<cudaEvent_t, cudaEvent_t> ev, double bytes = 0.0)
 {
     if (ctx->profiling && ev.first) {
         cudaEventRecord(ev.second, ctx->stream);
         ctx->pending.push_back({ pass, ev });
+        ctx->pass_bytes[pass] += bytes;
     }
 }
 inline void pass_collect(spk_context* ctx)

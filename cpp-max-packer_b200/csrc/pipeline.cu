@@ -978,18 +978,9 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
     if (L_[0] == 256 && L_[1] == 256 && L_[2] == 256) {
         auto ev = pass_begin(ctx_);
         pass_a256_kernel<<<16 * 256, 256, 0, st>>>(spectrum_, s.partial, inter_, s.K[2], s.legal[2], tw2);
-        pass_end(ctx_, 0, ev);
-        ev = pass_begin(ctx_);
-        pass_b1_256_kernel<<<16 * s.legal[2], 256, 0, st>>>(inter_, s.legal[1], tw1);
-        pass_end(ctx_, 1, ev);
-        const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
-        ev = pass_begin(ctx_);
-        pass_b2_256_kernel<<<static_cast<unsigned>((rows + 15) / 16), 256, 0, st>>>(
-            inter_, s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied), mode,
-            threshold, cursor_floor, keys, count, cap, tau, resid);
-        pass_end(ctx_, 2, ev);
-        ctx_->launches += 3;
-        return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+        pass_end(ctx_, 0, ev, pass_a_bytes(s));
+        ctx_->launches++;
+        return run_b256(s, inter_, mode, threshold, cursor_floor, keys, count, cap, tau, resid);
     }
     const std::size_t smem_a = sizeof(float2) * (L_[2] + 2 * kColumnGroup * (L_[2] + 1) + kColumnGroup * L_[2]);
     auto ev = pass_begin(ctx_);
@@ -1011,6 +1002,36 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
         mode, threshold, cursor_floor, keys, count, cap, tau, resid);
     pass_end(ctx_, 2, ev);
     ctx_->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+double Pipeline::pass_a_bytes(const KernelSlot& s) const
+{
+    const double plane = static_cast<double>(L_[0]) * L_[1] * sizeof(float2);
+    return plane * L_[2] + plane * (s.K[2] + s.legal[2]);
+}
+
+int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double threshold, double cursor_floor,
+                       unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
+                       unsigned long long* resid)
+{
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
+    const auto* tw0 = twiddle_table<float>(ctx_, L_[0], status);
+    const auto* tw1 = twiddle_table<float>(ctx_, L_[1], status);
+    if (!tw0 || !tw1) {
+        return status;
+    }
+    auto ev = pass_begin(ctx_);
+    pass_b1_256_kernel<<<16 * s.legal[2], 256, 0, st>>>(inter, s.legal[1], tw1);
+    pass_end(ctx_, 1, ev);
+    const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
+    ev = pass_begin(ctx_);
+    pass_b2_256_kernel<<<static_cast<unsigned>((rows + 15) / 16), 256, 0, st>>>(
+        inter, s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied), mode, threshold,
+        cursor_floor, keys, count, cap, tau, resid);
+    pass_end(ctx_, 2, ev);
+    ctx_->launches += 2;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
@@ -1057,6 +1078,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
     cudaMemsetAsync(range_error, 0, 16, st);
     std::vector<ExactJob> host_jobs(R);
     std::vector<double> eps_s(R), floor(R);
+    std::vector<int> runnable;
     for (int r = 0; r < R; ++r) {
         const auto& s = slots_[requests[r].slot];
         host_jobs[r] = { s.ones, static_cast<int>(s.occupied), std::max(s.legal[0], 1), std::max(s.legal[1], 1) };
@@ -1065,6 +1087,11 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         }
         eps_s[r] = approx_epsilon(s) + std::ldexp(1.0, -22);
         floor[r] = requests[r].has_cursor ? requests[r].cursor.score - eps_s[r] : -INFINITY;
+        runnable.push_back(r);
+    }
+    for (std::size_t i = 0; i < runnable.size(); ++i) {
+        const int r = runnable[i];
+        const auto& s = slots_[requests[r].slot];
         if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap, count + r, cap,
                                       tau + r, resid + r))) {
             return status;

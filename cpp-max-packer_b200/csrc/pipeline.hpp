@@ -101,6 +101,10 @@ private:
     int run_orientation(const KernelSlot& s, int mode, double threshold, double cursor_floor, unsigned long long* keys,
                         unsigned int* count, unsigned int cap, unsigned long long* tau,
                         unsigned long long* resid);
+    int run_b256(const KernelSlot& s, float2* inter, int mode, double threshold, double cursor_floor,
+                 unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
+                 unsigned long long* resid);
+    double pass_a_bytes(const KernelSlot& s) const;
     double score(const KernelSlot& s, const std::int64_t* t, double p) const;
     double approx_epsilon(const KernelSlot& s) const;
 

@@ -12,6 +12,11 @@ Labels come from the exhaustive GPU path.
   that orientation's best exact score among copies that pass the exact recount.
   The label is the orientation's gap to the layout's best score, clipped to
   `--cap` and scaled to [0, 1]. Orientations with no admissible copy get 1.
+- **Policy layouts.** A second set of layouts follows the proposal policy
+  itself (a DAgger round). A given network fills the container with the
+  proposed greedy, and a layout is labelled every `--policy-stride` steps through
+  the whole fill. The states the learned fill reaches late, in a nearly full
+  container, are then covered too.
 - **Training.** Runs on the device with the library's own forward and backward
   kernels (Adam, mean squared error).
 - **Evaluation.** Held-out seeds measure the regret of paging only the top-k
@@ -104,6 +109,62 @@ def generate(seeds, total_steps, dense, stride, orientations, cap, context, log=
                                     np.concatenate(sl))
 
 
+def generate_policy(seeds, net, k, stride, orientations, cap, context, item_base_count=0, log=print):
+    """Layouts along the proposed-greedy fill of `net`, labelled every `stride` steps until the fill ends."""
+    proposal = pkg("proposal")
+    crops, items, sc, si, sl = [], [], [], [], []
+    for seed in seeds:
+        t0 = time.time()
+        s, wl = open_session(seed, orientations, context)
+        O = len(wl.catalog)
+        _, it = proposal.session_features(s)
+        item_base = item_base_count + sum(len(x) for x in items)
+        items.append(it)
+        copies = 0
+        while True:
+            best = best_scores(s, range(O))
+            lab = labels_from(best, cap)
+            if lab is None:
+                break
+            crops.append(proposal.session_crop(s))
+            sc.append(np.full(O, len(crops) - 1, np.uint32))
+            si.append(item_base + np.arange(O, dtype=np.uint32))
+            sl.append(lab)
+            placed, _ = proposal.greedy_proposed(s, net, k, stride)
+            copies += len(placed)
+            if len(placed) < stride:
+                break
+        s.close()
+        log(f"policy seed {seed}: {copies} copies, {len(crops)} layouts so far, {time.time() - t0:.1f} s")
+    return crops, items, sc, si, sl
+
+
+def merge_datasets(a, crops, items, sc, si, sl):
+    """Appends policy layouts (indices relative to their own lists) to dataset a."""
+    proposal = pkg("proposal")
+    if not crops:
+        return a
+    sc = [x + len(a.crops) for x in sc]
+    return proposal.ProposalDataset(np.concatenate([a.crops, np.stack(crops)]), np.concatenate([a.items] + items),
+                                    np.concatenate([a.sample_crop] + sc), np.concatenate([a.sample_item] + si),
+                                    np.concatenate([a.sample_label] + sl))
+
+
+def fill_copies(seed, net, k, orientations, context, chunk=64):
+    """Copies placed by a full proposed-greedy fill (and its fallback steps)."""
+    proposal = pkg("proposal")
+    s, _ = open_session(seed, orientations, context)
+    copies, fallbacks = 0, 0
+    while True:
+        placed, fb = proposal.greedy_proposed(s, net, k, chunk)
+        copies += len(placed)
+        fallbacks += fb
+        if len(placed) < chunk:
+            break
+    s.close()
+    return copies, fallbacks
+
+
 def evaluate(nets, seeds, steps, orientations, k, context, rng_seed=0, log=print):
     """Mean regret and top-k hit rate of each net (and a random subset) on
     held-out seeds, following the exhaustive greedy's layouts."""
@@ -154,6 +215,10 @@ def main():
     ap.add_argument("--k", type=int, default=32)
     ap.add_argument("--eval-steps", type=int, default=15)
     ap.add_argument("--init-seed", type=int, default=7)
+    ap.add_argument("--policy-seeds", type=int, nargs="*", default=list(range(200, 208)))
+    ap.add_argument("--policy-stride", type=int, default=25)
+    ap.add_argument("--policy-weights", default="", help="network whose fills give the policy layouts")
+    ap.add_argument("--fill-seed", type=int, default=-1, help="held-out item for a full learned fill after training")
     ap.add_argument("--out", default=os.path.join(HERE, "weights", "proposal_rounded256.npz"))
     ap.add_argument("--report", default="")
     args = ap.parse_args()
@@ -162,6 +227,13 @@ def main():
     ctx = compute.Context(0)
     t0 = time.time()
     data = generate(args.train_seeds, args.steps, args.dense, args.stride, args.orientations, args.cap, ctx)
+    if args.policy_weights and args.policy_seeds:
+        policy = proposal.Proposal(seed=0, context=ctx)
+        policy.load(args.policy_weights)
+        extra = generate_policy(args.policy_seeds, policy, args.k, args.policy_stride, args.orientations, args.cap,
+                                ctx, item_base_count=len(data.items))
+        data = merge_datasets(data, *extra)
+        policy.close()
     t_gen = time.time() - t0
     print(f"dataset: {len(data.crops)} layouts, {len(data.sample_label)} samples, {t_gen:.1f} s", flush=True)
     net = proposal.Proposal(seed=args.init_seed, context=ctx)
@@ -176,7 +248,9 @@ def main():
           f"{losses[-50:].mean():.4f}", flush=True)
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     np.savez_compressed(args.out, parameters=net.get_parameters(),
-                        meta=json.dumps({"train_seeds": args.train_seeds, "steps": args.steps, "dense": args.dense,
+                        meta=json.dumps({"train_seeds": args.train_seeds, "policy_seeds": args.policy_seeds
+                                         if args.policy_weights else [], "policy_stride": args.policy_stride,
+                                         "steps": args.steps, "dense": args.dense,
                                          "stride": args.stride, "orientations": args.orientations, "cap": args.cap,
                                          "batch": args.batch, "train_steps": args.train_steps, "lr": args.lr,
                                          "init_seed": args.init_seed, "layouts": len(data.crops),
@@ -186,6 +260,9 @@ def main():
     report = {"layouts": len(data.crops), "samples": int(len(data.sample_label)), "generate_s": t_gen,
               "train_s": t_train, "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean()),
               "eval": ev, "k": args.k}
+    if args.fill_seed >= 0:
+        copies, fallbacks = fill_copies(args.fill_seed, net, args.k, args.orientations, ctx)
+        report["fill"] = {"seed": args.fill_seed, "copies": copies, "fallback_steps": fallbacks}
     print(json.dumps(report), flush=True)
     if args.report:
         with open(args.report, "w") as f:

@@ -91,6 +91,10 @@ void* spk_context_stream(const spk_context* context);
  * for passes 0 spectrum-A, 1 inverse-y, 2 inverse-x+epilogue, 3 merge+exact. */
 int spk_context_set_profiling(spk_context* context, int enabled);
 int spk_context_pass_times(const spk_context* context, uint64_t* launches, double* total_ms, uint32_t capacity);
+/* Algorithmic HBM bytes of the profiled launches of each pass (pass 0: the
+ * spectrum read once per launch, each orientation's kernel planes read and
+ * legal-z planes written), for achieved-bandwidth figures. */
+int spk_context_pass_bytes(const spk_context* context, double* bytes, uint32_t capacity);
 
 /* ---- full-range correlation drop-in ----------------------------------- */
 
