@@ -23,6 +23,7 @@ from ._lib import SpkError, check, lib
 
 FP32 = 0
 FP64 = 1
+FP16 = 2  # FP32 transforms, joint spectrum stored in FP16 before the product
 
 _MESSAGES = {
     "CORRELATION_SHAPE_OVERFLOW": "Correlation extents must be positive and representable.",

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 
 #define SPK_HD __host__ __device__ __forceinline__
 
@@ -105,5 +106,15 @@ SPK_HD int ilog2(unsigned v)
 }
 
 SPK_HD bool is_pow2(std::uint64_t v) { return v && !(v & (v - 1)); }
+
+// Runs `set_up` once per device (kernel attributes are per device), safely
+// from any number of host threads.
+template <typename F>
+inline void once_per_device(std::once_flag (&flags)[64], F set_up)
+{
+    int device = 0;
+    cudaGetDevice(&device);
+    std::call_once(flags[device & 63], set_up);
+}
 
 }  // namespace spk

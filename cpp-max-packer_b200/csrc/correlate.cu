@@ -13,6 +13,7 @@
 // (correlation.cpp:494-540); mass and the 8 direct probes
 // (correlation.cpp:542-577) run on the host over the same input buffers.
 
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -86,6 +87,40 @@ __global__ void spectrum_product_kernel(const cplx_t<T>* __restrict__ z, cplx_t<
         const C e = cscale(cadd(a, b), static_cast<T>(0.5));
         const C d = csub(a, b);  // = 2i K^
         const C k = cmake<C>(d.y * static_cast<T>(0.5), -d.x * static_cast<T>(0.5));
+        w[i] = cmulconj(e, k);
+    }
+}
+
+// FP16 storage of the joint spectrum: z * scale rounded to half precision.
+__global__ void spectrum_to_half_kernel(const float2* __restrict__ z, __half2* __restrict__ zh, long long n, float scale)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        zh[i] = __floats2half2_rn(z[i].x * scale, z[i].y * scale);
+    }
+}
+
+// The spectrum product of spectrum_product_kernel reading the FP16 spectrum.
+__global__ void spectrum_product_half_kernel(const __half2* __restrict__ zh, float2* __restrict__ w, Grid g,
+                                             float unscale)
+{
+    const long long n = g.n();
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % g.L[0]);
+        const long long r = i / g.L[0];
+        const int y = static_cast<int>(r % g.L[1]);
+        const int zz = static_cast<int>(r / g.L[1]);
+        const int mx = (g.L[0] - x) & (g.L[0] - 1);
+        const int my = (g.L[1] - y) & (g.L[1] - 1);
+        const int mz = (g.L[2] - zz) & (g.L[2] - 1);
+        const float2 a0 = __half22float2(zh[i]);
+        const float2 b0 = __half22float2(zh[mx + static_cast<long long>(g.L[0]) * (my + static_cast<long long>(g.L[1]) * mz)]);
+        const float2 a = make_float2(a0.x * unscale, a0.y * unscale);
+        const float2 b = make_float2(b0.x * unscale, -b0.y * unscale);
+        const float2 e = cscale(cadd(a, b), 0.5f);
+        const float2 d = csub(a, b);
+        const float2 k = make_float2(d.y * 0.5f, -d.x * 0.5f);
         w[i] = cmulconj(e, k);
     }
 }
@@ -269,7 +304,7 @@ int grid_blocks(long long n, int threads)
 template <typename T, typename E>
 int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* environment, const std::uint8_t* kernel,
               const spk_correlation_limits* limits_ptr, const spk_control* control, double* out_values,
-              std::uint64_t out_capacity, spk_correlation_result* result)
+              std::uint64_t out_capacity, spk_correlation_result* result, bool half_spectra = false)
 {
     constexpr bool binary = std::is_same_v<E, std::uint8_t>;
     if (!ctx || !spec_ptr || !environment || !kernel || !result) {
@@ -367,8 +402,9 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     const std::uint64_t out_bytes = padded_count * sizeof(double);
     const int extract_threads = 256;
     const int extract_blocks = grid_blocks(static_cast<long long>(padded_count), extract_threads);
-    const std::uint64_t working = limits.reserved_bytes + 2 * grid_bytes + out_bytes + env_count * sizeof(E) +
-                                  ker_count + extract_blocks * sizeof(ExtractStats) + 64;
+    const std::uint64_t half_bytes = half_spectra ? static_cast<std::uint64_t>(g.n()) * 4 : 0;
+    const std::uint64_t working = limits.reserved_bytes + 2 * grid_bytes + half_bytes + out_bytes +
+                                  env_count * sizeof(E) + ker_count + extract_blocks * sizeof(ExtractStats) + 64;
     if (working > limits.max_working_bytes) {
         return kMemoryLimit;
     }
@@ -404,8 +440,26 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     if (int s = poll(control)) {
         return s;
     }
-    spectrum_product_kernel<T><<<grid_blocks(g.n(), threads), threads, 0, st>>>(z, w, g);
-    ctx->launches++;
+    if constexpr (std::is_same_v<T, float>) {
+        if (half_spectra) {
+            // |Z(k)| <= sum |e| + sum |k|: a power-of-two scale puts that bound at 2^15 or below.
+            const double bound = environment_mass + static_cast<double>(ker_ones);
+            const int shift = bound > 0 ? 15 - static_cast<int>(std::ceil(std::log2(bound))) : 0;
+            auto* zh = static_cast<__half2*>(device_buffer(ctx, "corr.zh", half_bytes, status));
+            if (!zh) {
+                return status;
+            }
+            spectrum_to_half_kernel<<<grid_blocks(g.n(), threads), threads, 0, st>>>(
+                z, zh, g.n(), std::ldexp(1.0f, shift));
+            spectrum_product_half_kernel<<<grid_blocks(g.n(), threads), threads, 0, st>>>(zh, w, g,
+                                                                                         std::ldexp(1.0f, -shift));
+            ctx->launches += 2;
+        }
+    }
+    if (!half_spectra) {
+        spectrum_product_kernel<T><<<grid_blocks(g.n(), threads), threads, 0, st>>>(z, w, g);
+        ctx->launches++;
+    }
     if ((status = run_fft3<T>(ctx, w, g, true, static_cast<T>(1.0 / static_cast<double>(g.n()))))) {
         return status;
     }
@@ -416,7 +470,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
                                          : std::min(environment_mass, static_cast<double>(ker_ones));
     // FP64 keeps the reference's 1e-10 proximity tolerance; FP32 states its
     // own bound, 2^-13 relative to the output scale.
-    const double rel = sizeof(T) == 8 ? 1e-10 : 1.0 / 8192.0;
+    const double rel = sizeof(T) == 8 ? 1e-10 : half_spectra ? 1.0 / 256.0 : 1.0 / 8192.0;
     const double proximity_tolerance = rel * std::max(1.0, maximum_output);
     const double imag_tolerance = binary ? 0.25 : proximity_tolerance;
     extract_kernel<T><<<extract_blocks, extract_threads, 0, st>>>(
@@ -488,7 +542,9 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         }
         const double error = std::fabs(out_values[probes[p]] - expected);
         max_probe_error = std::max(max_probe_error, error);
-        const double tolerance = binary ? 0.25 : rel * std::max(1.0, std::fabs(expected));
+        // FP16 spectra state their bound relative to the output scale.
+        const double tolerance =
+            binary ? 0.25 : rel * std::max(1.0, half_spectra ? maximum_output : std::fabs(expected));
         if (!std::isfinite(error) || (binary ? error >= tolerance : error > tolerance)) {
             result->direct_terms = terms;
             return kNumeric;
@@ -529,7 +585,8 @@ int spk_estimate_correlation(const spk_correlation_spec* spec, uint32_t precisio
         grid *= L;
     }
     out->padded_cells = padded_cells;
-    out->working_bytes = 2 * grid * (precision == SPK_FP64 ? 16 : 8) + padded_cells * 8;
+    out->working_bytes = 2 * grid * (precision == SPK_FP64 ? 16 : 8) + (precision == SPK_FP16 ? 4 * grid : 0) +
+                         padded_cells * 8;
     return kOk;
 }
 
@@ -541,10 +598,14 @@ int spk_correlate_binary(spk_context* ctx, const spk_correlation_spec* spec, con
         if (ctx && cudaSetDevice(ctx->device) != cudaSuccess) {
             return kCuda;
         }
+        if (precision > SPK_FP16) {
+            return kInvalidArgument;
+        }
         return precision == SPK_FP64 ? correlate<double, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
                                                                        out_values, out_capacity, result)
                                      : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
-                                                                      out_values, out_capacity, result);
+                                                                      out_values, out_capacity, result,
+                                                                      precision == SPK_FP16);
     }
     catch (...) {
         return kAllocation;
@@ -560,10 +621,14 @@ int spk_correlate_proximity(spk_context* ctx, const spk_correlation_spec* spec, 
         if (ctx && cudaSetDevice(ctx->device) != cudaSuccess) {
             return kCuda;
         }
+        if (precision > SPK_FP16) {
+            return kInvalidArgument;
+        }
         return precision == SPK_FP64 ? correlate<double, double>(ctx, spec, environment, kernel, limits, control,
                                                                  out_values, out_capacity, result)
                                      : correlate<float, double>(ctx, spec, environment, kernel, limits, control,
-                                                                out_values, out_capacity, result);
+                                                                out_values, out_capacity, result,
+                                                                precision == SPK_FP16);
     }
     catch (...) {
         return kAllocation;

@@ -355,9 +355,7 @@ int edt_squared(spk_context* ctx, const std::uint8_t* d_occupied, std::int32_t* 
     }
     ctx->launches++;
     static std::once_flag attribute[64];
-    int device = 0;
-    cudaGetDevice(&device);
-    std::call_once(attribute[device & 63], [] {
+    once_per_device(attribute, [] {
         cudaFuncSetAttribute(edt_pass_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kSharedLineMax * 32 * 8);
     });

@@ -15,6 +15,8 @@
 #include <cstring>
 #include <memory>
 #include <optional>
+#include <set>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -1140,6 +1142,47 @@ int spk_session_greedy_proposed(spk_context* ctx, spk_proposal* proposal, uint32
             }
             record(*chosen, *placed, orientations, translations, scores);
             ++*placed;
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_jobs_greedy(spk_job* jobs, uint64_t count)
+{
+    try {
+        if (count && !jobs) {
+            return kInvalidArgument;
+        }
+        std::set<const void*> contexts, proposals;
+        for (std::uint64_t j = 0; j < count; ++j) {
+            if (!jobs[j].context || !contexts.insert(jobs[j].context).second ||
+                (jobs[j].proposal && !proposals.insert(jobs[j].proposal).second)) {
+                return kInvalidArgument;
+            }
+        }
+        std::vector<std::thread> threads;
+        threads.reserve(count);
+        for (std::uint64_t j = 0; j < count; ++j) {
+            threads.emplace_back([job = &jobs[j]] {
+                job->placed = 0;
+                job->fallbacks = 0;
+                if (cudaSetDevice(job->context->device) != cudaSuccess) {
+                    job->status = kCuda;
+                    return;
+                }
+                job->status = job->proposal
+                                  ? spk_session_greedy_proposed(job->context, job->proposal, job->k, job->max_steps,
+                                                                &job->placed, job->orientations, job->translations,
+                                                                job->scores, &job->fallbacks)
+                                  : spk_session_greedy(job->context, job->max_steps, &job->placed, job->orientations,
+                                                       job->translations, job->scores);
+            });
+        }
+        for (auto& t : threads) {
+            t.join();
         }
         return kOk;
     }

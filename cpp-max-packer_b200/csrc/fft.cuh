@@ -172,11 +172,10 @@ cudaError_t fft_axis(cplx_t<T>* data, int Lx, int Ly, int Lz, int axis, bool inv
         group >>= 1;
     }
     const size_t smem = sizeof(C) * (L + 2 * static_cast<size_t>(group) * (L + 1));
-    static bool attribute_set = false;
-    if (!attribute_set) {
+    static std::once_flag attribute[64];
+    once_per_device(attribute, [] {
         cudaFuncSetAttribute(fft_axis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        attribute_set = true;
-    }
+    });
     const int threads = 256;
     const long long blocks = lines / group;
     fft_axis_kernel<T><<<static_cast<unsigned>(blocks), threads, smem, stream>>>(data, Lx, Ly, Lz, axis,

@@ -963,12 +963,11 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
         }
         inter_bytes_ = inter;
     }
-    static bool configured = false;
-    if (!configured) {
+    static std::once_flag configured[64];
+    once_per_device(configured, [] {
         allow_large_smem(pass_a_kernel);
         allow_large_smem(pass_b2_kernel);
-        configured = true;
-    }
+    });
     const auto* tw0 = twiddle_table<float>(ctx_, L_[0], status);
     const auto* tw1 = twiddle_table<float>(ctx_, L_[1], status);
     const auto* tw2 = twiddle_table<float>(ctx_, L_[2], status);
@@ -1103,11 +1102,10 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         // The second stage sorts 64 x 65 keys padded to 8192: 64 KB of shared memory.
         constexpr unsigned padded = 8192;
         static_assert(kLargeKeyChunks * (kExactPerOrientation + 1) <= padded, "second merge stage exceeds its buffer");
-        static bool merge_configured = false;
-        if (!merge_configured) {
+        static std::once_flag merge_configured[64];
+        once_per_device(merge_configured, [] {
             cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, padded * 8);
-            merge_configured = true;
-        }
+        });
         merge_chunk_kernel<<<dim3(kLargeKeyChunks, R), 1024, 0, st>>>(keys, cap, count, partial);
         merge_kernel<<<R, 1024, padded * 8, st>>>(partial, static_cast<long long>(kLargeKeyChunks) * per, nullptr,
                                                   kLargeKeyChunks * per, selected);

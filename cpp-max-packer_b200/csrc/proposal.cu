@@ -58,11 +58,34 @@ struct ConvArgs {
     long long k_total;   // GEMM K
     int chunks_per_split;
     int relu_mask;       // data gradient: multiply by (x > 0)
+    // log2 of the power-of-two extents and channel counts (every layer of the
+    // network has them), so the gathers index with shifts and masks.
+    int lg_s_in, lg_s_out, lg_cin, lg_cinp, lg_cout;
 };
 
 struct Vox {
     int n, z, y, x;
 };
+
+// Voxel of row m in a batch of cubes of side 2^lg (rows < 2^32).
+__device__ __forceinline__ Vox decode_pow2(unsigned m, int lg)
+{
+    const unsigned mask = (1u << lg) - 1u;
+    Vox v;
+    v.x = static_cast<int>(m & mask);
+    v.y = static_cast<int>((m >> lg) & mask);
+    v.z = static_cast<int>((m >> (2 * lg)) & mask);
+    v.n = static_cast<int>(m >> (3 * lg));
+    return v;
+}
+
+// Channel-0 element offset of a voxel of a cube of side 2^lg with 2^lg_c channels.
+__device__ __forceinline__ long long voxel_offset(const Vox& v, int iz, int iy, int ix, int lg, int lg_c)
+{
+    const unsigned cell = ((((static_cast<unsigned>(v.n) << lg | static_cast<unsigned>(iz)) << lg) |
+                            static_cast<unsigned>(iy)) << lg) | static_cast<unsigned>(ix);
+    return static_cast<long long>(cell) << lg_c;
+}
 
 __device__ __forceinline__ Vox decode(long long m, int s)
 {
@@ -148,27 +171,25 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
             const void* src = a.w;
             bool valid = false;
             if (row_ok && k < a.k_total) {
+                const int kk = static_cast<int>(k);
                 if (MODE == kFwd) {
-                    const int tap = static_cast<int>(k / a.cinp), ci0 = static_cast<int>(k % a.cinp);
+                    const int tap = kk >> a.lg_cinp, ci0 = kk & ((1 << a.lg_cinp) - 1);
                     int iz, iy, ix;
                     if (tap < 27 && (a.cin >= 8 || ci0 == 0) && tap_input(row_vox, tap, a.stride, a.s_in, iz, iy, ix)) {
-                        const long long vi =
-                            ((static_cast<long long>(row_vox.n) * a.s_in + iz) * a.s_in + iy) * a.s_in + ix;
+                        const long long at = voxel_offset(row_vox, iz, iy, ix, a.lg_s_in, a.lg_cin);
                         if (a.cin < 8) {
-                            put(A, off, load_channels(a.x + vi * a.cin, a.cin, ci0));
+                            put(A, off, load_channels(a.x + at, a.cin, ci0));
                             continue;
                         }
-                        src = a.x + vi * a.cin + ci0;
+                        src = a.x + at + ci0;
                         valid = true;
                     }
                 }
                 else {
-                    const int tap = static_cast<int>(k / a.cout), co0 = static_cast<int>(k % a.cout);
+                    const int tap = kk >> a.lg_cout, co0 = kk & ((1 << a.lg_cout) - 1);
                     int qz, qy, qx;
                     if (tap < 27 && tap_output(row_vox, tap, a.stride, a.s_out, qz, qy, qx)) {
-                        const long long qi =
-                            ((static_cast<long long>(row_vox.n) * a.s_out + qz) * a.s_out + qy) * a.s_out + qx;
-                        src = a.dy + qi * a.cout + co0;
+                        src = a.dy + voxel_offset(row_vox, qz, qy, qx, a.lg_s_out, a.lg_cout) + co0;
                         valid = true;
                     }
                 }
@@ -189,16 +210,17 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
             bool valid = false;
             if (q < a.k_total) {
                 if (r0 < a.kw) {
-                    const int tap = static_cast<int>(r0 / a.cinp), ci0 = static_cast<int>(r0 % a.cinp);
-                    const Vox o = decode(q, a.s_out);
+                    const int r = static_cast<int>(r0);
+                    const int tap = r >> a.lg_cinp, ci0 = r & ((1 << a.lg_cinp) - 1);
+                    const Vox o = decode_pow2(static_cast<unsigned>(q), a.lg_s_out);
                     int iz, iy, ix;
                     if ((a.cin >= 8 || ci0 == 0) && tap_input(o, tap, a.stride, a.s_in, iz, iy, ix)) {
-                        const long long vi = ((static_cast<long long>(o.n) * a.s_in + iz) * a.s_in + iy) * a.s_in + ix;
+                        const long long at = voxel_offset(o, iz, iy, ix, a.lg_s_in, a.lg_cin);
                         if (a.cin < 8) {
-                            put(A, off, load_channels(a.x + vi * a.cin, a.cin, ci0));
+                            put(A, off, load_channels(a.x + at, a.cin, ci0));
                             continue;
                         }
-                        src = a.x + vi * a.cin + ci0;
+                        src = a.x + at + ci0;
                         valid = true;
                     }
                 }
@@ -236,7 +258,7 @@ __device__ __forceinline__ void gather_b(const ConvArgs& a, unsigned char* B, in
             const int kk = rem & 15, g = rem >> 4;
             const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + kk;
             if (MODE == kData) {
-                const int tap = static_cast<int>(k / a.cout), co = static_cast<int>(k % a.cout);
+                const int tap = static_cast<int>(k) >> a.lg_cout, co = static_cast<int>(k) & ((1 << a.lg_cout) - 1);
                 if (k < a.k_total && tap < 27) {
                     src = a.w + static_cast<long long>(co) * a.kw + tap * a.cinp + 8 * g;
                     valid = true;
@@ -291,7 +313,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
     if (MODE != kWeight) {
         const long long m = m0 + tid;
         row_ok = m < a.m_total;
-        row_vox = decode(row_ok ? m : 0, MODE == kFwd ? a.s_out : a.s_in);
+        row_vox = decode_pow2(static_cast<unsigned>(row_ok ? m : 0), MODE == kFwd ? a.lg_s_out : a.lg_s_in);
     }
     constexpr bool a_mn = MODE == kWeight;
     constexpr bool b_mn = MODE != kFwd;
@@ -628,9 +650,7 @@ template <int MODE>
 void set_smem_attribute()
 {
     static std::once_flag flag[64];
-    int dev = 0;
-    cudaGetDevice(&dev);
-    std::call_once(flag[dev & 63], [] {
+    once_per_device(flag, [] {
         cudaFuncSetAttribute(conv_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              kStages * (kRows * kKC * 2 + 64 * kKC * 2));
     });
@@ -687,6 +707,18 @@ struct ProposalNet {
 namespace {
 
 int out_side(const ProposalLayer& l) { return l.s_in / l.stride; }
+
+constexpr bool pow2(int v) { return v > 0 && (v & (v - 1)) == 0; }
+constexpr bool shapes_are_pow2()
+{
+    for (const ProposalLayer& l : kProposalSpec) {
+        if (!pow2(l.cin) || !pow2(l.cout) || !pow2(l.s_in) || !pow2(l.s_in / l.stride)) {
+            return false;
+        }
+    }
+    return true;
+}
+static_assert(shapes_are_pow2(), "the convolution gathers index power-of-two extents and channel counts");
 
 template <typename T>
 int alloc(ProposalNet* net, T*& p, std::size_t count)
@@ -772,6 +804,11 @@ ConvArgs layer_args(ProposalNet* net, int l, std::uint32_t batch)
     a.cinp = cin_pad(L.cin);
     a.cout = L.cout;
     a.kw = 27 * a.cinp;
+    a.lg_s_in = ilog2(static_cast<unsigned>(a.s_in));
+    a.lg_s_out = ilog2(static_cast<unsigned>(a.s_out));
+    a.lg_cin = ilog2(static_cast<unsigned>(a.cin));
+    a.lg_cinp = ilog2(static_cast<unsigned>(a.cinp));
+    a.lg_cout = ilog2(static_cast<unsigned>(a.cout));
     return a;
 }
 
@@ -917,6 +954,9 @@ int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, co
                      const std::uint32_t* crop_index, const bf16* items, const std::uint32_t* item_index,
                      std::uint64_t items_tag, float* pred)
 {
+    if (batch == 0 || batch > (1u << 16)) {
+        return kInvalidArgument;  // row indices of the gathers are 32-bit
+    }
     int status = ensure_batch(net, batch);
     if (status) {
         return status;

@@ -170,3 +170,46 @@ class Session:
                                               shape.ctypes.data, out.ctypes.data, out.nbytes), "spk_session_field")
         self.last_window = (tuple(int(v) for v in first), tuple(int(v) for v in shape))
         return out
+
+
+class JobC(ctypes.Structure):
+    _fields_ = [("context", P), ("proposal", P), ("k", ctypes.c_uint32), ("reserved", ctypes.c_uint32),
+                ("max_steps", ctypes.c_uint64), ("orientations", P), ("translations", P), ("scores", P),
+                ("placed", ctypes.c_uint64), ("fallbacks", ctypes.c_uint64), ("status", ctypes.c_int32),
+                ("reserved2", ctypes.c_int32)]
+
+
+def run_jobs(jobs) -> list:
+    """Fills several sessions concurrently (spk_jobs_greedy).  `jobs` holds
+    (session, proposal or None, k, max_steps) tuples, every session on its own
+    context; returns (placements, fallback steps) per job, in order."""
+    lib = _lib_ready()
+    _declare(lib)
+    if not getattr(lib, "_jobs_declared", False):
+        lib.spk_jobs_greedy.argtypes = [ctypes.POINTER(JobC), ctypes.c_uint64]
+        lib._jobs_declared = True
+    arr = (JobC * len(jobs))()
+    keep = []
+    for i, (session, net, k, max_steps) in enumerate(jobs):
+        n = max(int(max_steps), 1)
+        ori = np.zeros(n, np.uint64)
+        t = np.zeros((n, 3), np.int64)
+        scores = np.zeros(n, np.float64)
+        keep.append((ori, t, scores))
+        arr[i].context = session.context.handle
+        arr[i].proposal = net.handle if net is not None else None
+        arr[i].k = int(k)
+        arr[i].max_steps = int(max_steps)
+        arr[i].orientations = ori.ctypes.data
+        arr[i].translations = t.ctypes.data
+        arr[i].scores = scores.ctypes.data
+    _lib.check(lib.spk_jobs_greedy(arr, len(jobs)), "spk_jobs_greedy")
+    out = []
+    for i, (session, _, _, _) in enumerate(jobs):
+        _lib.check(arr[i].status, f"spk_jobs_greedy job {i}")
+        ori, t, scores = keep[i]
+        placed = [Placement(int(ori[j]), tuple(int(v) for v in t[j]), float(scores[j]))
+                  for j in range(arr[i].placed)]
+        session.placements += placed
+        out.append((placed, int(arr[i].fallbacks)))
+    return out

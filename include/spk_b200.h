@@ -25,8 +25,12 @@ extern "C" {
 
 typedef struct spk_context spk_context;
 
-/* Arithmetic used by the FFT correlation. */
-enum { SPK_FP32 = 0, SPK_FP64 = 1 };
+/* Arithmetic used by the FFT correlation.  SPK_FP16: FP32 transforms with the
+ * joint spectrum stored in FP16 (power-of-two scaled) before the product;
+ * the integer residual, mass and probe checks decide whether a result is
+ * admissible (CORRELATION_NUMERIC otherwise; proximity tolerance 2^-8 of
+ * the output scale). */
+enum { SPK_FP32 = 0, SPK_FP64 = 1, SPK_FP16 = 2 };
 
 /* Reference: compute::CorrelationSpec, correlation.hpp:22-27. */
 typedef struct spk_correlation_spec {
@@ -371,6 +375,30 @@ int spk_session_propose(spk_context* context, spk_proposal* proposal, uint32_t k
 int spk_session_greedy_proposed(spk_context* context, spk_proposal* proposal, uint32_t k, uint64_t max_steps,
                                 uint64_t* placed, uint64_t* orientations, int64_t* translations, double* scores,
                                 uint64_t* fallbacks);
+
+/* ---- independent jobs -------------------------------------------------------
+ * No counterpart in the reference: several packing jobs (each a context with
+ * an open session, of any grid size and catalog) filled concurrently.  Each
+ * job runs on its own host thread and its own context's stream, so the jobs'
+ * kernels share the GPU; results equal running each job alone. */
+typedef struct spk_job {
+    spk_context* context;    /* with an open session; one job per context */
+    spk_proposal* proposal;  /* NULL: exhaustive greedy; else proposed greedy (one job per proposal) */
+    uint32_t k;              /* proposed orientations per step */
+    uint32_t reserved;
+    uint64_t max_steps;
+    uint64_t* orientations;  /* max_steps entries, or NULL */
+    int64_t* translations;   /* 3 x max_steps entries, or NULL */
+    double* scores;          /* max_steps entries, or NULL */
+    uint64_t placed;         /* out: copies placed */
+    uint64_t fallbacks;      /* out: exhaustive fallback steps (proposed greedy) */
+    int32_t status;          /* out: the job's status */
+    int32_t reserved2;
+} spk_job;
+
+/* Runs every job to completion (or max_steps); returns SPK_INVALID_ARGUMENT
+ * when two jobs share a context or a proposal, else OK with per-job status. */
+int spk_jobs_greedy(spk_job* jobs, uint64_t count);
 
 #ifdef __cplusplus
 }

@@ -138,3 +138,70 @@ def test_proximity_long_lines_bit_exact(gpu_ctx, oracle_c):
             got = compute.build_proximity(shape, occ, context=gpu_ctx)
             want, _ = oracle_c.build_proximity(shape, occ)
             assert np.array_equal(got.view(np.uint64), want.view(np.uint64)), (shape, density)
+
+
+def _blob(shape, rng):
+    zz, yy, xx = np.mgrid[0:shape[2], 0:shape[1], 0:shape[0]]
+    c = (np.array(shape) - 1) / 2
+    d = ((xx - c[0]) / (shape[0] / 2)) ** 2 + ((yy - c[1]) / (shape[1] / 2)) ** 2 + ((zz - c[2]) / (shape[2] / 2)) ** 2
+    return (d + rng.normal(0, 0.1, d.shape) < 1).astype(np.uint8).reshape(-1)
+
+
+def test_fp16_spectra_fail_closed_or_exact(gpu_ctx, oracle_c):
+    # FP16 spectra round the DC term by ~2^-11 of the overlap mass, so the
+    # reference's mass check (sum of unrounded counts within 0.25 of the exact
+    # mass) refuses them beyond tiny fields; whatever is returned is exact.
+    compute = package("compute")
+    rng = np.random.default_rng(31)
+    cases = [((6, 6, 5), (3, 1, 1), 0.2, True), ((20, 18, 16), (4, 5, 3), 0.3, False),
+             ((33, 9, 12), (6, 3, 5), 0.3, False)]
+    for es, ks, density, must_pass in cases:
+        env = (rng.random(int(np.prod(es))) < density).astype(np.uint8)
+        ker = _blob(ks, rng) if min(ks) > 1 else np.ones(int(np.prod(ks)), np.uint8)
+        got = compute.correlate_binary(compute.CorrelationSpec(es, ks), env, ker, precision=compute.FP16,
+                                       context=gpu_ctx)
+        _, _, want = oracle_c.correlate(False, es, ks, (0, 0, 0), (0, 0, 0), env, ker)
+        if isinstance(got, compute.CorrelationResult):
+            assert np.array_equal(got.values, want)
+        else:
+            assert not must_pass and got.code == "CORRELATION_NUMERIC", got
+
+
+def test_fp16_spectra_proximity_within_stated_bound(gpu_ctx, oracle_c):
+    # Real-valued proximity correlations with FP16 spectra: values within
+    # 2^-8 of the output scale (the largest possible output) of the exact result.
+    compute = package("compute")
+    rng = np.random.default_rng(33)
+    for es, ks in [((24, 20, 18), (5, 4, 3)), ((40, 40, 40), (7, 7, 7))]:
+        env = rng.random(int(np.prod(es)))
+        ker = _blob(ks, rng)
+        got = compute.correlate_proximity(compute.CorrelationSpec(es, ks), env, ker, precision=compute.FP16,
+                                          context=gpu_ctx)
+        _, _, want = oracle_c.correlate(True, es, ks, (0, 0, 0), (0, 0, 0), env, ker)
+        assert isinstance(got, compute.CorrelationResult), got
+        # The stated FP16 scale: 2^-8 of the largest possible output, min(environment mass, kernel cells).
+        assert np.abs(got.values - want).max() <= max(1.0, min(env.sum(), float(ker.sum()))) / 256
+
+
+def test_fp16_spectra_refused_at_the_medium_scale(gpu_ctx):
+    # A 128^3 half-occupied environment against a 21^3 blob: FP64 (pinned to
+    # the oracle on smaller fields) passes the reference's checks; FP16 spectra
+    # exceed the integer bound and are refused.
+    compute = package("compute")
+    rng = np.random.default_rng(32)
+    es, ks = (128, 128, 128), (21, 21, 21)
+    env = (rng.random(int(np.prod(es))) < 0.5).astype(np.uint8)
+    ker = _blob(ks, rng)
+    spec = compute.CorrelationSpec(es, ks)
+    lim = compute.CorrelationLimits(max_working_bytes=4 << 30)  # the FP64 grid alone is 537 MB
+    want = compute.correlate_binary(spec, env, ker, limits=lim, precision=compute.FP64, context=gpu_ctx)
+    got32 = compute.correlate_binary(spec, env, ker, limits=lim, precision=compute.FP32, context=gpu_ctx)
+    got16 = compute.correlate_binary(spec, env, ker, limits=lim, precision=compute.FP16, context=gpu_ctx)
+    assert isinstance(want, compute.CorrelationResult)
+    # FP32 passes the reference's checks or is refused by them (at this mass the
+    # 0.25 mass check is beyond FP32 accumulation); it is never wrong.
+    if isinstance(got32, compute.CorrelationResult):
+        assert np.array_equal(got32.values, want.values)
+    else:
+        assert got32.code == "CORRELATION_NUMERIC", got32
+    assert isinstance(got16, compute.CorrelationFailure) and got16.code == "CORRELATION_NUMERIC", got16
