@@ -34,9 +34,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = "placements/s at 256^3 grid x512 orients: learned-proposal vs exhaustive GPU"
 UNIT = "placements/s"
-# dram__bytes_read.sum + dram__bytes_write.sum of one pass_a256_kernel launch
-# (profiles/pass_a256_pass_b2_256_blob256_o16.md): 143,679,744 + 67,410,688.
-PASS_A256_DRAM_BYTES = 211090432
+# dram__bytes_read.sum + dram__bytes_write.sum of one pass_a256_kernel launch,
+# mean of the four launches captured in profiles/step_kernels_rounded256_o16.md
+# (211,964,672 / 211,798,016 / 211,456,000 / 211,373,312 bytes).
+PASS_A256_DRAM_BYTES = 211648000
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp-max-packer_b200", "weights",
                                "proposal_rounded256.npz")
 
@@ -176,12 +177,14 @@ def run_ours(args, rank, world, local_rank):
         ex_sequence = [(p.orientation_index, p.translation) for p in session.placements]
 
         ln_value, ln_ms, ln_placed, fallbacks, ln_launches, ln_sequence = None, None, [], 0, 0, []
+        learned_offset = None
         if learned:
             net = proposal.Proposal(seed=0, context=ctx)
             net.load(weights)
             reset_layout(session)
             proposal.greedy_proposed(session, net, k, args.warmup)
             launches0 = ctx.launches
+            learned_offset = int(launches0)
             ln_ms, (ln_placed, fallbacks) = timed_steps(
                 stream, lambda: proposal.greedy_proposed(session, net, k, args.steps), dist)
             ln_launches = ctx.launches - launches0
@@ -195,6 +198,8 @@ def run_ours(args, rank, world, local_rank):
                               "profiling_run": True, "exhaustive_value": round(ex_value, 4),
                               "ms_per_step": round((ln_ms if learned else ex_ms) / max(args.steps, 1), 4),
                               "gpu_launches": int(ln_launches if learned else ex_launches),
+                              # library launches before the learned timed steps (an ncu -s skip count)
+                              "launches_before_learned_steps": learned_offset,
                               "page_stats": page_stats}))
         session.close()
         ctx.close()

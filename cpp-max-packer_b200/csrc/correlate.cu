@@ -469,7 +469,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     const double maximum_output = binary ? static_cast<double>(std::min(env_ones, ker_ones))
                                          : std::min(environment_mass, static_cast<double>(ker_ones));
     // FP64 keeps the reference's 1e-10 proximity tolerance; FP32 states its
-    // own bound, 2^-13 relative to the output scale.
+    // own bound, 2^-13 relative to the output scale (2^-8 with FP16 spectra).
     const double rel = sizeof(T) == 8 ? 1e-10 : half_spectra ? 1.0 / 256.0 : 1.0 / 8192.0;
     const double proximity_tolerance = rel * std::max(1.0, maximum_output);
     const double imag_tolerance = binary ? 0.25 : proximity_tolerance;
@@ -542,9 +542,10 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         }
         const double error = std::fabs(out_values[probes[p]] - expected);
         max_probe_error = std::max(max_probe_error, error);
-        // FP16 spectra state their bound relative to the output scale.
+        // FP64 keeps the reference's per-probe relative tolerance; FP32 and
+        // FP16 state their bounds relative to the output scale.
         const double tolerance =
-            binary ? 0.25 : rel * std::max(1.0, half_spectra ? maximum_output : std::fabs(expected));
+            binary ? 0.25 : rel * std::max(1.0, sizeof(T) == 8 ? std::fabs(expected) : maximum_output);
         if (!std::isfinite(error) || (binary ? error >= tolerance : error > tolerance)) {
             result->direct_terms = terms;
             return kNumeric;

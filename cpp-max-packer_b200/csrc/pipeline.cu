@@ -377,6 +377,82 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
     }
 }
 
+// Environment spectrum on 256^3 grids, register four-step FFTs (see
+// fft_reg.cuh).  The row kernel packs Z = B + iP straight from the occupancy,
+// squared distances and the proximity table, accumulates sum(b^2 + p^2) for
+// the error bound, and transforms along x; the column kernel transforms y or
+// z in place (16 adjacent columns per block, coalesced along x).
+__global__ void __launch_bounds__(256) env_row256_kernel(float2* __restrict__ spectrum, int E0, int E1, int E2,
+                                                        const std::uint8_t* __restrict__ occ,
+                                                        const std::int32_t* __restrict__ d2,
+                                                        const double* __restrict__ table,
+                                                        const float2* __restrict__ twiddles,
+                                                        double* __restrict__ norm_partial)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    __shared__ double red[256];
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int t = threadIdx.x & 15, j = threadIdx.x >> 4;
+    const int row = blockIdx.x * 16 + j;  // y + 256 z
+    const int y = row & 255, z = row >> 8;
+    float2 v[16];
+    double acc = 0;
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        const int x = 16 * n1 + t;
+        float b = 0.f, p = 0.f;
+        if (x < E0 && y < E1 && z < E2) {
+            const long long e = x + static_cast<long long>(E0) * (y + static_cast<long long>(E1) * z);
+            b = occ[e] ? 1.f : 0.f;
+            const std::int32_t dv = d2[e];
+            p = dv == kInf ? 0.f : static_cast<float>(table[dv]);
+        }
+        acc += static_cast<double>(b) * b + static_cast<double>(p) * p;
+        v[n1] = make_float2(b, p);
+    }
+    fft256<false>(v, lines + j * kRegLine, t, tw);
+    float2* out = spectrum + 256LL * row;
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+        out[t + 16 * k2] = v[k2];
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            red[threadIdx.x] += red[threadIdx.x + h];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        norm_partial[blockIdx.x] = red[0];
+    }
+}
+
+__global__ void __launch_bounds__(256) env_column256_kernel(float2* __restrict__ spectrum, long long line_stride,
+                                                           long long other_stride, float scale,
+                                                           const float2* __restrict__ twiddles)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int j = threadIdx.x & 15, t = threadIdx.x >> 4;
+    const long long col = 16 * (blockIdx.x & 15) + j + other_stride * (blockIdx.x >> 4);
+    float2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        v[n1] = spectrum[col + line_stride * (16 * n1 + t)];
+    }
+    fft256<false>(v, lines + j * kRegLine, t, tw);
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+        spectrum[col + line_stride * (t + 16 * k2)] = make_float2(v[k2].x * scale, v[k2].y * scale);
+    }
+}
+
 __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ inter, int legal_y,
                                                          const float2* __restrict__ twiddles)
 {
@@ -817,24 +893,41 @@ int Pipeline::set_occupancy(const std::uint8_t* d_occupancy)
         return status;
     }
     const long long grid = static_cast<long long>(L_[0]) * L_[1] * L_[2];
-    const int blocks = launch_blocks(grid, 256);
+    const bool reg256 = L_[0] == 256 && L_[1] == 256 && L_[2] == 256;
+    const int blocks = reg256 ? 256 * 256 / 16 : launch_blocks(grid, 256);
     auto* partial = static_cast<double*>(device_buffer(ctx_, "pipe.norm", blocks * sizeof(double), status));
     if (!partial) {
         return status;
     }
-    env_pack_kernel<<<blocks, 256, 0, st>>>(spectrum_, L_[0], L_[1], L_[2], E_[0], E_[1], E_[2], occ_, d2_, table_,
-                                             partial);
-    ctx_->launches++;
-    for (int axis = 0; axis != 3; ++axis) {
-        const auto* tw = twiddle_table<float>(ctx_, L_[axis], status);
+    if (reg256) {
+        const auto* tw = twiddle_table<float>(ctx_, 256, status);
         if (!tw) {
             return status;
         }
-        const float scale = axis == 2 ? static_cast<float>(1.0 / static_cast<double>(grid)) : 1.f;
-        if (fft_axis<float>(spectrum_, L_[0], L_[1], L_[2], axis, false, scale, tw, st) != cudaSuccess) {
+        env_row256_kernel<<<blocks, 256, 0, st>>>(spectrum_, E_[0], E_[1], E_[2], occ_, d2_, table_, tw, partial);
+        env_column256_kernel<<<16 * 256, 256, 0, st>>>(spectrum_, 256, 65536, 1.f, tw);  // y
+        env_column256_kernel<<<16 * 256, 256, 0, st>>>(spectrum_, 65536, 256,
+                                                       static_cast<float>(1.0 / static_cast<double>(grid)), tw);  // z
+        ctx_->launches += 3;
+        if (cudaGetLastError() != cudaSuccess) {
             return kCuda;
         }
+    }
+    else {
+        env_pack_kernel<<<blocks, 256, 0, st>>>(spectrum_, L_[0], L_[1], L_[2], E_[0], E_[1], E_[2], occ_, d2_, table_,
+                                                 partial);
         ctx_->launches++;
+        for (int axis = 0; axis != 3; ++axis) {
+            const auto* tw = twiddle_table<float>(ctx_, L_[axis], status);
+            if (!tw) {
+                return status;
+            }
+            const float scale = axis == 2 ? static_cast<float>(1.0 / static_cast<double>(grid)) : 1.f;
+            if (fft_axis<float>(spectrum_, L_[0], L_[1], L_[2], axis, false, scale, tw, st) != cudaSuccess) {
+                return kCuda;
+            }
+            ctx_->launches++;
+        }
     }
     std::vector<double> host(blocks);
     cudaMemcpyAsync(host.data(), partial, blocks * sizeof(double), cudaMemcpyDeviceToHost, st);

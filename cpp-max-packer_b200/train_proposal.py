@@ -57,12 +57,23 @@ def best_scores(session, orientations):
     return out
 
 
+LABEL = "linear"
+
+
 def labels_from(best, cap):
+    """Each orientation's gap to the layout's best score as a target in [0, 1].
+    'log': (log10(gap + 1e-5) + 5) / 5, so gaps of 1e-5 .. 1 spread evenly and
+    the near-best orientations, which decide the top k, stay apart; 'linear':
+    gap clipped to `cap`, over `cap`.  No admissible copy: 1."""
     top = best.min()
     if not np.isfinite(top):
         return None
     gap = np.where(np.isfinite(best), best - top, np.inf)
-    return np.where(np.isfinite(gap), np.minimum(gap, cap) / cap, 1.0).astype(np.float32)
+    if LABEL == "log":
+        y = np.clip((np.log10(np.where(np.isfinite(gap), gap, 1.0) + 1e-5) + 5.0) / 5.0, 0.0, 1.0)
+    else:
+        y = np.minimum(np.where(np.isfinite(gap), gap, cap), cap) / cap
+    return np.where(np.isfinite(gap), y, 1.0).astype(np.float32)
 
 
 def open_session(seed, orientations, context):
@@ -219,10 +230,14 @@ def main():
     ap.add_argument("--policy-stride", type=int, default=25)
     ap.add_argument("--policy-weights", default="", help="network whose fills give the policy layouts")
     ap.add_argument("--fill-seed", type=int, default=-1, help="held-out item for a full learned fill after training")
+    ap.add_argument("--fill-k", type=int, nargs="+", default=[32], help="proposal sizes of those fills")
+    ap.add_argument("--label", choices=["log", "linear"], default="linear")
     ap.add_argument("--out", default=os.path.join(HERE, "weights", "proposal_rounded256.npz"))
     ap.add_argument("--report", default="")
     args = ap.parse_args()
 
+    global LABEL
+    LABEL = args.label
     compute, proposal = pkg("compute"), pkg("proposal")
     ctx = compute.Context(0)
     t0 = time.time()
@@ -252,6 +267,7 @@ def main():
                                          if args.policy_weights else [], "policy_stride": args.policy_stride,
                                          "steps": args.steps, "dense": args.dense,
                                          "stride": args.stride, "orientations": args.orientations, "cap": args.cap,
+                                         "label": args.label,
                                          "batch": args.batch, "train_steps": args.train_steps, "lr": args.lr,
                                          "init_seed": args.init_seed, "layouts": len(data.crops),
                                          "samples": len(data.sample_label)}))
@@ -261,8 +277,13 @@ def main():
               "train_s": t_train, "loss_first": float(losses[:50].mean()), "loss_last": float(losses[-50:].mean()),
               "eval": ev, "k": args.k}
     if args.fill_seed >= 0:
-        copies, fallbacks = fill_copies(args.fill_seed, net, args.k, args.orientations, ctx)
-        report["fill"] = {"seed": args.fill_seed, "copies": copies, "fallback_steps": fallbacks}
+        report["fill"] = []
+        for k in args.fill_k:
+            t_fill = time.time()
+            copies, fallbacks = fill_copies(args.fill_seed, net, k, args.orientations, ctx)
+            report["fill"].append({"seed": args.fill_seed, "k": k, "copies": copies, "fallback_steps": fallbacks,
+                                   "seconds": round(time.time() - t_fill, 1)})
+            print(report["fill"][-1], flush=True)
     print(json.dumps(report), flush=True)
     if args.report:
         with open(args.report, "w") as f:
