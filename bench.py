@@ -169,6 +169,7 @@ def run_ours(args, rank, world, local_rank):
         session.greedy(args.warmup)
         session.stats(reset=True)
         launches0 = ctx.launches
+        exhaustive_offset = int(launches0)
         ex_ms, ex_placed = timed_steps(stream, lambda: session.greedy(args.steps), dist)
         ex_launches = ctx.launches - launches0
         page_stats = session.stats(reset=True)
@@ -200,6 +201,7 @@ def run_ours(args, rank, world, local_rank):
                               "gpu_launches": int(ln_launches if learned else ex_launches),
                               # library launches before the learned timed steps (an ncu -s skip count)
                               "launches_before_learned_steps": learned_offset,
+                              "launches_before_exhaustive_steps": exhaustive_offset,
                               "page_stats": page_stats}))
         session.close()
         ctx.close()
