@@ -479,6 +479,17 @@ __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ i
     }
 }
 
+// Pass B2 on 256^3 grids: 16 rows per block, 16 threads per row.
+//   mode 0: every key whose block cannot hold 64 smaller keys is emitted.
+//     The block's keys overwrite its staged rows in shared memory, a
+//     1024-bin histogram of their high 32 bits between the block's smallest
+//     and largest finds the first bin T by which 64 keys have accumulated,
+//     and keys in bins <= T that are also <= the request's pruning bound are
+//     appended; T's upper edge then lowers the bound.  A key in a bin above T
+//     has 64 smaller keys in its own block, so no key of the request's top 64
+//     is ever left out.
+//   mode 1: every candidate with approximate score <= threshold is appended
+//     and every candidate past the cursor floor is counted in *tau.
 __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
                                                          int legal_y, int legal_z,
                                                          const float2* __restrict__ twiddles,
@@ -489,10 +500,19 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
                                                          unsigned long long* __restrict__ tau,
                                                          unsigned long long* __restrict__ resid)
 {
+    constexpr int kBins = 1024;
     __shared__ float2 tw[256];
     __shared__ float2 lines[16 * kRegLine];
-    __shared__ unsigned long long pending[8][64];  // per warp: keys waiting to be merged
+    __shared__ unsigned int hist[kBins];
+    __shared__ unsigned int block_lo, block_hi, warp_sums[8];
+    __shared__ int cut_bin;
+    __shared__ unsigned long long emit_bound;
     tw[threadIdx.x] = twiddles[threadIdx.x];
+    if (threadIdx.x == 0) {
+        block_lo = 0xffffffffu;
+        block_hi = 0u;
+        cut_bin = kBins - 1;
+    }
     __syncthreads();
     const int t = threadIdx.x & 15;  // lane within the row (coalesced direction)
     const int j = threadIdx.x >> 4;  // row within the block
@@ -517,16 +537,14 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     for (int m2 = 0; m2 < 16; ++m2) {
         line[t + 16 * m2] = v[m2];
     }
+    // Keys replace the staged values slot for slot (mode 0).
+    auto* row_keys = reinterpret_cast<unsigned long long*>(line);
     const double t65z = valid ? t65[zz] : 0.0;
     const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
-    unsigned long long list_lo = kEmptyKey, list_hi = kEmptyKey;
-    unsigned long long worst = kEmptyKey;
-    int waiting = 0;  // warp-uniform count of staged keys
-    const int warp = threadIdx.x >> 5;
     float residual = 0.f;
-    // Keys above the request's pruning bound cannot enter the merged top-64:
-    // drop them before the warp sort (the bound only ever decreases).
-    unsigned long long bound = mode == 0 ? *reinterpret_cast<volatile unsigned long long*>(tau) : ~0ULL;
+    // Keys above the request's pruning bound cannot enter its top 64.
+    const unsigned long long bound = mode == 0 ? *reinterpret_cast<volatile unsigned long long*>(tau) : ~0ULL;
+    unsigned int lo = 0xffffffffu, hi = 0u;
 #pragma unroll 1
     for (int m2 = 0; m2 < 16; ++m2) {
         const int x = t + 16 * m2;
@@ -550,27 +568,11 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
             }
         }
         if (mode == 0) {
-            // Stage keys below the warp's current 64th; merge 32 at a time.
-            const bool qualifies = key < worst;
-            const unsigned mask = __ballot_sync(kFull, qualifies);
-            if (mask) {
-                if (qualifies) {
-                    pending[warp][waiting + __popc(mask & ((1u << lane) - 1u))] = key;
-                }
-                waiting += __popc(mask);
-                if (waiting >= 32) {
-                    __syncwarp();
-                    warp_merge32(list_lo, list_hi, pending[warp][lane], lane);
-                    const int rest = waiting - 32;
-                    const unsigned long long carry = lane < rest ? pending[warp][32 + lane] : kEmptyKey;
-                    __syncwarp();
-                    if (lane < rest) {
-                        pending[warp][lane] = carry;
-                    }
-                    __syncwarp();
-                    waiting = rest;
-                    worst = __shfl_sync(kFull, list_hi, 31);
-                }
+            row_keys[x] = key;
+            if (key != kEmptyKey) {
+                const unsigned int h = static_cast<unsigned int>(key >> 32);
+                lo = min(lo, h);
+                hi = max(hi, h);
             }
         }
         else {
@@ -594,66 +596,114 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     if (lane == 0 && residual > 0.f) {
         atomicMax(resid, static_cast<unsigned long long>(__float_as_uint(residual)));
     }
-    if (mode == 0 && waiting > 0) {
-        __syncwarp();
-        warp_merge32(list_lo, list_hi, lane < waiting ? pending[warp][lane] : kEmptyKey, lane);
+    if (mode != 0) {
+        return;
     }
-    if (mode == 0) {
-        // Block top-64: the eight sorted warp lists (odd warps stored in
-        // descending order, so neighbours form bitonic runs of 128) finish
-        // as one bitonic sort of 512 keys, one compare-exchange per thread
-        // per stage; only the block's 64 smallest are emitted, so an
-        // orientation emits at most 64 keys per block and its key range
-        // never overflows.
-        unsigned long long* merged = &pending[0][0];
-        __syncthreads();
-        const bool descending = warp & 1;
-        merged[warp * 64 + (descending ? 63 - lane : lane)] = list_lo;
-        merged[warp * 64 + (descending ? 31 - lane : 32 + lane)] = list_hi;
-        for (int k = 128; k <= 512; k <<= 1) {
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                __syncthreads();
-                const int t = threadIdx.x;
-                const int i = ((t & ~(j - 1)) << 1) | (t & (j - 1));
-                const int p = i | j;
-                const unsigned long long a = merged[i], b = merged[p];
-                if ((a > b) == ((i & k) == 0)) {
-                    merged[i] = b;
-                    merged[p] = a;
-                }
+    // Block range of the keys' high words, then the histogram over it.
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+    }
+    for (int b = threadIdx.x; b < kBins; b += 256) {
+        hist[b] = 0;
+    }
+    if (lane == 0 && lo <= hi) {
+        atomicMin(&block_lo, lo);
+        atomicMax(&block_hi, hi);
+    }
+    __syncthreads();
+    const unsigned int range_lo = block_lo;
+    if (range_lo > block_hi) {
+        return;  // no key in this block (uniform: every thread sees the same shared values)
+    }
+    int shift = 0;
+    while (shift < 32 && ((block_hi - range_lo) >> shift) >= static_cast<unsigned int>(kBins)) {
+        ++shift;
+    }
+#pragma unroll 1
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int x = t + 16 * m2;
+        if (valid && x < legal_x) {
+            const unsigned long long key = row_keys[x];
+            if (key != kEmptyKey) {
+                atomicAdd(&hist[(static_cast<unsigned int>(key >> 32) - range_lo) >> shift], 1u);
             }
         }
-        __syncthreads();
-        list_lo = merged[lane];
-        list_hi = merged[32 + lane];
-        if (warp == 0) {
-            const unsigned long long worst = __shfl_sync(kFull, list_hi, 31);
-            unsigned long long bound = 0;
-            if (lane == 0) {
-                if (worst != kEmptyKey) {
-                    const unsigned long long before = atomicMin(tau, worst);
-                    bound = before < worst ? before : worst;
-                }
-                else {
-                    bound = *reinterpret_cast<volatile unsigned long long*>(tau);
-                }
+    }
+    __syncthreads();
+    // First bin at which 64 keys have accumulated: each thread sums four
+    // consecutive bins, a block scan of those sums locates the crossing.
+    unsigned int mine = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        mine += hist[4 * threadIdx.x + q];
+    }
+    unsigned int inclusive = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int other = __shfl_up_sync(kFull, inclusive, o);
+        if (lane >= o) {
+            inclusive += other;
+        }
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane == 31) {
+        warp_sums[warp] = inclusive;
+    }
+    __syncthreads();
+    unsigned int before = 0, total = 0;
+    for (int w = 0; w < 8; ++w) {
+        before += w < warp ? warp_sums[w] : 0u;
+        total += warp_sums[w];
+    }
+    const unsigned int start = before + inclusive - mine;
+    constexpr unsigned int kNeed = kExactPerOrientation;
+    if (total >= kNeed && start < kNeed && start + mine >= kNeed) {
+        unsigned int running = start;
+        for (int q = 0; q < 4; ++q) {
+            running += hist[4 * threadIdx.x + q];
+            if (running >= kNeed) {
+                cut_bin = 4 * threadIdx.x + q;
+                break;
             }
-            bound = __shfl_sync(kFull, bound, 0);
-            for (int half = 0; half < 2; ++half) {
-                const unsigned long long kv = half ? list_hi : list_lo;
-                const bool take = kv != kEmptyKey && kv <= bound;
-                const unsigned mask = __ballot_sync(kFull, take);
-                if (mask) {
-                    unsigned int slot = 0;
-                    if (lane == 0) {
-                        slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
-                    }
-                    slot = __shfl_sync(kFull, slot, 0);
-                    const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
-                    if (take && slot + rank < cap) {
-                        keys[slot + rank] = kv;
-                    }
-                }
+        }
+    }
+    __syncthreads();
+    const int cut = cut_bin;
+    if (threadIdx.x == 0) {
+        unsigned long long b = *reinterpret_cast<volatile unsigned long long*>(tau);
+        const unsigned long long edge = static_cast<unsigned long long>(range_lo) +
+                                        (static_cast<unsigned long long>(cut + 1) << shift);
+        if (total >= kNeed && edge <= 0xffffffffULL) {
+            // Every key of bins <= cut is below (edge << 32): an upper bound of
+            // this block's 64th smallest key, hence of the request's.
+            const unsigned long long upper = (edge << 32) - 1;
+            const unsigned long long old = atomicMin(tau, upper);
+            b = old < upper ? old : upper;
+        }
+        emit_bound = b;
+    }
+    __syncthreads();
+    const unsigned long long limit = emit_bound;
+#pragma unroll 1
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int x = t + 16 * m2;
+        bool take = false;
+        unsigned long long key = kEmptyKey;
+        if (valid && x < legal_x) {
+            key = row_keys[x];
+            take = key != kEmptyKey && key <= limit &&
+                   static_cast<int>((static_cast<unsigned int>(key >> 32) - range_lo) >> shift) <= cut;
+        }
+        const unsigned mask = __ballot_sync(kFull, take);
+        if (mask) {
+            unsigned int slot = 0;
+            if (lane == 0) {
+                slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+            }
+            slot = __shfl_sync(kFull, slot, 0);
+            const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+            if (take && slot + rank < cap) {
+                keys[slot + rank] = key;
             }
         }
     }
@@ -1137,8 +1187,11 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
     cudaStream_t st = ctx_->stream;
     int status = kOk;
     const int per = kExactPerOrientation + 1;
-    // 256^3 grids emit at most 64 keys per pass-B2 block (4096 blocks at most),
-    // so their key range cannot overflow; other grids keep kKeyCapacity.
+    // 256^3 grids: each pass-B2 block emits the keys of its histogram bins up
+    // to the one where 64 accumulate (about 64), below the pruning bound, so
+    // 64 x 4096 keys cover a request; only heavy exact ties could exceed that,
+    // and an overflowing page is then left uncertified and widened.  Other
+    // grids keep kKeyCapacity.
     const bool large = L_[0] == 256 && L_[1] == 256 && L_[2] == 256;
     const unsigned int cap = large ? kLargeKeyChunks * kKeyCapacity : kKeyCapacity;
     auto* keys = static_cast<unsigned long long*>(
