@@ -175,99 +175,121 @@ __global__ void __launch_bounds__(256) edt_first_pass_kernel(const std::uint8_t*
     }
 }
 
-// The same 1D pass for lines of at most kSharedLineMax cells, with each
-// line's lower-envelope stack in shared memory: one warp handles 32 lines,
-// one per lane.  Lanes hold consecutive lines, so the loads and stores of the
-// y and z passes are coalesced across the warp.  A stack entry is the site q,
-// its value f and the first coordinate it wins from, clamped to
+// The same 1D pass for lines of at most kSharedLineMax cells, two lanes per
+// line.  Lane h of a pair builds the lower envelope of the sites in its half
+// of the line, [h * half, min(len, (h + 1) * half)), in shared memory (site q,
+// its value f, and the first coordinate it wins from, clamped to
 // [-1, length]: a site whose interval lies wholly outside [0, length) wins no
-// cell, so the clamp changes no output value.
+// cell, so the clamp changes no output).  Each lane then writes its half of
+// the outputs as the smaller of the two envelopes evaluated there: the lower
+// envelope of a union is the minimum of the envelopes.  One warp holds 16
+// lines; consecutive line pairs are consecutive lines, so the loads and
+// stores of the y and z passes are coalesced.
 constexpr int kSharedLineMax = 512;
+
+__device__ __forceinline__ long long envelope_value(const std::int32_t* sf, const std::int16_t* sq,
+                                                    const std::int16_t* ss, int count, int owner, int& site, int q)
+{
+    while (site + 1 < count && ss[(site + 1) * 32 + owner] <= q) {
+        ++site;
+    }
+    const long long delta = q - sq[site * 32 + owner];
+    return static_cast<long long>(sf[site * 32 + owner]) + delta * delta;
+}
 
 __global__ void __launch_bounds__(32) edt_pass_shared_kernel(std::int32_t* __restrict__ d2, int sx, int sy, int sz,
                                                              int axis)
 {
     extern __shared__ __align__(16) unsigned char stack_raw[];
     const int length = axis == 0 ? sx : axis == 1 ? sy : sz;
-    std::int32_t* sf = reinterpret_cast<std::int32_t*>(stack_raw);       // [length][32]
-    std::int16_t* sq = reinterpret_cast<std::int16_t*>(sf + length * 32);  // [length][32]
-    std::int16_t* ss = sq + length * 32;                                  // [length][32]
+    const int half = (length + 1) / 2;
+    std::int32_t* sf = reinterpret_cast<std::int32_t*>(stack_raw);     // [half][32]
+    std::int16_t* sq = reinterpret_cast<std::int16_t*>(sf + half * 32);  // [half][32]
+    std::int16_t* ss = sq + half * 32;                                  // [half][32]
     const int lane = threadIdx.x;
+    const int h = lane & 1;
     const long long lines = static_cast<long long>(sx) * sy * sz / length;
-    const long long line = static_cast<long long>(blockIdx.x) * 32 + lane;
-    if (line >= lines) {
+    const long long line = static_cast<long long>(blockIdx.x) * 16 + (lane >> 1);
+    const bool active = line < lines;  // both lanes of a pair agree
+    long long base = 0, stride = 1;
+    if (active) {
+        if (axis == 0) {
+            base = line * sx;
+        }
+        else if (axis == 1) {
+            const long long x = line % sx, z = line / sx;
+            base = x + z * static_cast<long long>(sx) * sy;
+            stride = sx;
+        }
+        else {
+            base = line;
+            stride = static_cast<long long>(sx) * sy;
+        }
+    }
+    const int q_begin = h * half, q_end = min(length, q_begin + half);
+    int count = 0;
+    if (active) {
+        for (int q0 = q_begin; q0 < q_end; q0 += 8) {
+            // Eight independent loads in flight before the envelope work.
+            std::int32_t fv[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                fv[i] = q0 + i < q_end ? d2[base + (q0 + i) * stride] : kInf;
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int q = q0 + i;
+                const std::int32_t f = fv[i];
+                if (f == kInf) {
+                    continue;
+                }
+                int start = -1;
+                while (count > 0) {
+                    const int top = (count - 1) * 32 + lane;
+                    const long long p = sq[top];
+                    const long long numerator = static_cast<long long>(f) - sf[top] + 1LL * q * q - p * p;
+                    const long long denominator = 2LL * (q - p);  // positive: q > p
+                    // The top site keeps cells before floor(n / d) + 1 when that
+                    // exceeds its own first cell S, i.e. when n >= S * d.
+                    if (numerator >= static_cast<long long>(ss[top]) * denominator) {
+                        long long quotient = numerator / denominator;
+                        if (numerator % denominator != 0 && numerator < 0) {
+                            --quotient;
+                        }
+                        const long long first = quotient + 1;
+                        start = first < -1 ? -1 : first > length ? length : static_cast<int>(first);
+                        break;
+                    }
+                    --count;
+                }
+                if (count == 0) {
+                    start = -1;
+                }
+                const int slot = count * 32 + lane;
+                sf[slot] = f;
+                sq[slot] = static_cast<std::int16_t>(q);
+                ss[slot] = static_cast<std::int16_t>(start);
+                ++count;
+            }
+        }
+    }
+    const int partner_count = __shfl_xor_sync(0xffffffffu, count, 1);
+    __syncwarp();
+    if (!active) {
         return;
     }
-    long long base, stride;
-    if (axis == 0) {
-        base = line * sx;
-        stride = 1;
-    }
-    else if (axis == 1) {
-        const long long x = line % sx, z = line / sx;
-        base = x + z * static_cast<long long>(sx) * sy;
-        stride = sx;
-    }
-    else {
-        base = line;
-        stride = static_cast<long long>(sx) * sy;
-    }
-    int count = 0;
-    for (int q0 = 0; q0 < length; q0 += 8) {
-        // Eight independent loads in flight before the envelope work.
-        std::int32_t fv[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            fv[i] = q0 + i < length ? d2[base + (q0 + i) * stride] : kInf;
+    const int partner = lane ^ 1;
+    int own_site = 0, partner_site = 0;
+    for (int q = q_begin; q < q_end; ++q) {
+        long long best = kInf;
+        if (count > 0) {
+            best = envelope_value(sf, sq, ss, count, lane, own_site, q);
         }
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const int q = q0 + i;
-            const std::int32_t f = fv[i];
-            if (f == kInf) {
-                continue;
-            }
-            int start = -1;
-            while (count > 0) {
-                const int top = (count - 1) * 32 + lane;
-                const long long p = sq[top];
-                const long long numerator = static_cast<long long>(f) - sf[top] + 1LL * q * q - p * p;
-                const long long denominator = 2LL * (q - p);  // positive: q > p
-                // The top site keeps cells before floor(n / d) + 1 when that
-                // exceeds its own first cell S, i.e. when n >= S * d.
-                if (numerator >= static_cast<long long>(ss[top]) * denominator) {
-                    long long quotient = numerator / denominator;
-                    if (numerator % denominator != 0 && numerator < 0) {
-                        --quotient;
-                    }
-                    const long long first = quotient + 1;
-                    start = first < -1 ? -1 : first > length ? length : static_cast<int>(first);
-                    break;
-                }
-                --count;
-            }
-            if (count == 0) {
-                start = -1;
-            }
-            const int slot = count * 32 + lane;
-            sf[slot] = f;
-            sq[slot] = static_cast<std::int16_t>(q);
-            ss[slot] = static_cast<std::int16_t>(start);
-            ++count;
+        if (partner_count > 0) {
+            const long long other = envelope_value(sf, sq, ss, partner_count, partner, partner_site, q);
+            best = other < best ? other : best;
         }
-    }
-    int site = 0;
-    for (int q = 0; q < length; ++q) {
-        const long long at = base + q * stride;
-        if (count == 0) {
-            d2[at] = kInf;
-            continue;
-        }
-        while (site + 1 < count && ss[(site + 1) * 32 + lane] <= q) {
-            ++site;
-        }
-        const long long delta = q - sq[site * 32 + lane];
-        d2[at] = static_cast<std::int32_t>(sf[site * 32 + lane] + delta * delta);
+        d2[base + q * stride] = best >= kInf ? kInf : static_cast<std::int32_t>(best);
     }
 }
 
@@ -357,12 +379,13 @@ int edt_squared(spk_context* ctx, const std::uint8_t* d_occupied, std::int32_t* 
     static std::once_flag attribute[64];
     once_per_device(attribute, [] {
         cudaFuncSetAttribute(edt_pass_shared_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kSharedLineMax * 32 * 8);
+                             (kSharedLineMax + 1) / 2 * 32 * 8);
     });
     for (int axis = first_fused ? 1 : 0; axis != 3; ++axis) {
         const long long lines = n / shape[axis];
         if (shape[axis] <= static_cast<std::uint32_t>(kSharedLineMax)) {
-            edt_pass_shared_kernel<<<static_cast<unsigned>((lines + 31) / 32), 32, shape[axis] * 32 * 8, stream>>>(
+            const unsigned stack_bytes = (shape[axis] + 1) / 2 * 32 * 8;
+            edt_pass_shared_kernel<<<static_cast<unsigned>((lines + 15) / 16), 32, stack_bytes, stream>>>(
                 d_d2, shape[0], shape[1], shape[2], axis);
         }
         else {
