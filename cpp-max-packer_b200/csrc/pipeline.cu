@@ -203,20 +203,6 @@ __device__ __forceinline__ void warp_insert(unsigned long long& lo, unsigned lon
     hi = warp_bitonic_finish(hi < rev ? hi : rev, lane);
 }
 
-// Merges 32 keys (one per lane, any order) into the warp's 64 smallest.
-__device__ __forceinline__ void warp_merge32(unsigned long long& lo, unsigned long long& hi, unsigned long long key,
-                                             int lane)
-{
-    key = warp_sort32(key, lane);
-    unsigned long long rev = __shfl_sync(kFull, key, 31 - lane);
-    const unsigned long long small = lo < rev ? lo : rev;
-    const unsigned long long large = lo < rev ? rev : lo;
-    lo = warp_bitonic_finish(small, lane);
-    const unsigned long long spill = warp_bitonic_finish(large, lane);
-    rev = __shfl_sync(kFull, spill, 31 - lane);
-    hi = warp_bitonic_finish(hi < rev ? hi : rev, lane);
-}
-
 // Pass B2: inverse FFT along x for 8 legal rows, then the fused epilogue.
 // mode 0: warp top-32 lists + pruning bound in *tau; mode 1: append every
 // candidate whose approximate score is <= threshold and count every candidate

@@ -87,18 +87,6 @@ __device__ __forceinline__ long long voxel_offset(const Vox& v, int iz, int iy, 
     return static_cast<long long>(cell) << lg_c;
 }
 
-__device__ __forceinline__ Vox decode(long long m, int s)
-{
-    Vox v;
-    v.x = static_cast<int>(m % s);
-    long long t = m / s;
-    v.y = static_cast<int>(t % s);
-    t /= s;
-    v.z = static_cast<int>(t % s);
-    v.n = static_cast<int>(t / s);
-    return v;
-}
-
 __device__ __forceinline__ uint4 load_channels(const bf16* voxel, int cin, int ci0)
 {
     if (cin >= 8) {
