@@ -33,30 +33,29 @@ int blocks_for(long long n, int threads)
     return static_cast<int>(std::min<long long>(std::max<long long>(want, 1), 148LL * 32));
 }
 
+// One thread per (face, cell) pair.  `offsets` is the exclusive prefix sum of
+// the faces' clipped cell-range sizes (outside faces count 0), so small faces
+// pack densely into warps instead of leaving most lanes of a per-face warp idle.
 __global__ void raster_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint,
-                              const geo::FaceRange* __restrict__ ranges, int faces, FieldWindow w,
-                              std::uint8_t* __restrict__ cells, int* __restrict__ error)
+                              const geo::FaceRange* __restrict__ ranges, const long long* __restrict__ offsets,
+                              int faces, long long total, FieldWindow w, std::uint8_t* __restrict__ cells,
+                              int* __restrict__ error)
 {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (warp >= faces) {
-        return;
-    }
-    const geo::FaceRange r = ranges[warp];
-    if (r.outside) {
-        return;
-    }
-    IVec3 tri[3];
-    for (int k = 0; k < 3; ++k) {
-        tri[k] = vint[tris[3 * warp + k]];
-    }
-    const long long nx = r.last[0] - r.first[0] + 1, ny = r.last[1] - r.first[1] + 1,
-                    nz = r.last[2] - r.first[2] + 1;
-    if (nx <= 0 || ny <= 0 || nz <= 0) {
-        return;
-    }
-    const long long n = nx * ny * nz;
-    for (long long c = lane; c < n; c += 32) {
+    for (long long item = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; item < total;
+         item += static_cast<long long>(gridDim.x) * blockDim.x) {
+        int lo = 0, hi = faces - 1;  // last face whose offset is <= item: the face that owns it
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (offsets[mid] <= item) {
+                lo = mid;
+            } else {
+                hi = mid - 1;
+            }
+        }
+        const int face = lo;
+        const geo::FaceRange r = ranges[face];
+        const long long nx = r.last[0] - r.first[0] + 1, ny = r.last[1] - r.first[1] + 1;
+        const long long c = item - offsets[face];
         std::int64_t index[3];
         index[0] = r.first[0] + c % nx;
         index[1] = r.first[1] + (c / nx) % ny;
@@ -71,6 +70,10 @@ __global__ void raster_kernel(const std::uint32_t* __restrict__ tris, const IVec
         if (!grid_cell_interval(w.origin, w.pitch, index, box)) {
             atomicOr(error, 1);
             continue;
+        }
+        IVec3 tri[3];
+        for (int k = 0; k < 3; ++k) {
+            tri[k] = vint[tris[3 * face + k]];
         }
         if (!triangle_box_disjoint(tri, box)) {
             cells[flat] = 2;
@@ -267,32 +270,46 @@ int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& 
         return kFieldIndexOverflow;
     }
     const std::size_t F = mesh.triangles.size(), V = mesh.vertices.size();
+    std::vector<long long> offsets(F + 1, 0);
+    for (std::size_t f = 0; f < F; ++f) {
+        const auto& r = ranges[f];
+        long long cells = 0;
+        if (!r.outside && r.last[0] >= r.first[0] && r.last[1] >= r.first[1] && r.last[2] >= r.first[2]) {
+            cells = (r.last[0] - r.first[0] + 1) * (r.last[1] - r.first[1] + 1) * (r.last[2] - r.first[2] + 1);
+        }
+        offsets[f + 1] = offsets[f] + cells;
+    }
+    const long long total = offsets[F];
     int status = kOk;
     auto* d_tris = static_cast<std::uint32_t*>(device_buffer(ctx, "field.tris", F * 12, status));
     auto* d_vint = static_cast<IVec3*>(device_buffer(ctx, "field.vint", V * sizeof(IVec3), status));
     auto* d_ranges = static_cast<geo::FaceRange*>(device_buffer(ctx, "field.ranges", F * sizeof(geo::FaceRange), status));
+    auto* d_offsets = static_cast<long long*>(device_buffer(ctx, "field.offsets", (F + 1) * sizeof(long long), status));
     auto* d_parent = static_cast<int*>(device_buffer(ctx, "field.parent", n * sizeof(int), status));
     auto* d_rootv = static_cast<std::uint8_t*>(device_buffer(ctx, "field.rootv", n, status));
     auto* d_misc = static_cast<int*>(device_buffer(ctx, "field.misc", 64, status));
     const unsigned int root_capacity = 1u << 20;
     auto* d_roots = static_cast<int*>(device_buffer(ctx, "field.roots", root_capacity * 4ULL, status));
-    if (!d_tris || !d_vint || !d_ranges || !d_parent || !d_rootv || !d_misc || !d_roots) {
+    if (!d_tris || !d_vint || !d_ranges || !d_offsets || !d_parent || !d_rootv || !d_misc || !d_roots) {
         return status;
     }
     cudaMemcpyAsync(d_tris, mesh.triangles.data(), F * 12, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_vint, placed.intervals.data(), V * sizeof(IVec3), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_ranges, ranges.data(), F * sizeof(geo::FaceRange), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_offsets, offsets.data(), (F + 1) * sizeof(long long), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_cells, 0, n, st);
     cudaMemsetAsync(d_misc, 0, 64, st);
     const int threads = 256;
-    raster_kernel<<<static_cast<unsigned>((F * 32 + threads - 1) / threads), threads, 0, st>>>(
-        d_tris, d_vint, d_ranges, static_cast<int>(F), w, d_cells, d_misc);
+    if (total > 0) {
+        raster_kernel<<<blocks_for(total, threads), threads, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets,
+                                                                      static_cast<int>(F), total, w, d_cells, d_misc);
+    }
     ccl_init_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, n);
     ccl_union_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, w.shape[0], w.shape[1],
                                                                    w.shape[2], d_misc);
     auto* d_root_count = reinterpret_cast<unsigned int*>(d_misc + 4);
     ccl_compress_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_parent, n, d_roots, d_root_count, root_capacity);
-    ctx->launches += 4;
+    ctx->launches += total > 0 ? 4 : 3;
     int h_misc[8];
     cudaMemcpyAsync(h_misc, d_misc, 32, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
