@@ -124,13 +124,16 @@ def timed_steps(stream, fn, dist):
 
 
 def max_over_ranks(ms, placed, world):
-    """(max ms over ranks, placements summed over ranks)."""
+    """(max ms over ranks, placements summed over ranks).  The exchanged pair
+    sits on the device the process group's backend serves: CUDA under NCCL,
+    the host under gloo."""
     if world == 1:
         return ms, float(placed)
     import torch
     import torch.distributed as tdist
 
-    t = torch.tensor([ms, float(placed)], device="cuda")
+    device = "cuda" if tdist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([ms, float(placed)], device=device)
     gathered = [torch.zeros_like(t) for _ in range(world)]
     tdist.all_gather(gathered, t)
     return max(float(g[0]) for g in gathered), sum(float(g[1]) for g in gathered)
