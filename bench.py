@@ -55,6 +55,41 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def step_model(fft_shape, env_shape, orientations, ms_per_step, hbm_gbs):
+    """Whole-step figures for one exhaustive placement step, beside the
+    pass-A kernel roofline.
+
+    Bytes: the floor of a fully fused design with FFT length L per axis,
+    P = L^3 and Ph = (L/2 + 1) L^2 complex-FP32 half spectra (8 B each).  Per
+    orientation it reads the kernel spectrum once (8 Ph) and makes one round
+    trip of an inverse-transform intermediate (16 Ph).  Per step it reads the
+    two environment spectra once (16 Ph), runs two forward environment
+    transforms (48 Ph), the EDT (24 B per window cell) and the stamp and
+    occupancy update (2 B per cell):
+        bytes_step = 24 Ph O + 64 Ph + 26 E^3.
+    FLOPs: 2.5 P log2 P per real transform; a step inverts a binary and a
+    proximity correlation per orientation and transforms both environment
+    fields forward: (2 O + 2) transforms.  The paged pipeline prunes to
+    legal translations, so it does less than this full-range count.
+    """
+    import math
+
+    L = [int(v) for v in fft_shape]
+    P = L[0] * L[1] * L[2]
+    Ph = (L[0] // 2 + 1) * L[1] * L[2]
+    E3 = int(env_shape[0]) * int(env_shape[1]) * int(env_shape[2])
+    O = int(orientations)
+    bytes_step = 24 * Ph * O + 64 * Ph + 26 * E3
+    flops_step = 2.5 * P * math.log2(P) * (2 * O + 2) if P > 1 else 0.0
+    seconds = ms_per_step / 1000.0
+    achieved = bytes_step / seconds / 1e9 if seconds > 0 else 0.0
+    return {"model_bytes_per_step": int(bytes_step), "achieved": round(achieved, 1), "peak": hbm_gbs,
+            "unit": "GB/s", "frac": round(achieved / hbm_gbs, 4) if hbm_gbs > 0 else None,
+            "floor_ms_per_step": round(bytes_step / (hbm_gbs * 1e9) * 1000.0, 3) if hbm_gbs > 0 else None,
+            "ms_per_step": round(ms_per_step, 4), "fft_flops_per_step": flops_step,
+            "fft_tflops": round(flops_step / seconds / 1e12, 3) if seconds > 0 else 0.0}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -291,7 +326,9 @@ def run_ours(args, rank, world, local_rank):
                        "session_open_s": round(open_s, 2), "parallelism": f"replicas x{world}",
                        "page_stats_exhaustive": page_stats},
             "exhaustive": {"value": round(ex_value, 4), "ms_per_step": round(ex_ms / max(args.steps, 1), 4),
-                           "gpu_launches": int(ex_launches)},
+                           "gpu_launches": int(ex_launches),
+                           "step_model": step_model(session.fft_shape, session.environment_shape, O,
+                                                    ex_ms / max(args.steps, 1), hbm)},
             "gpu_launches": int(ln_launches if learned else ex_launches),
             "roofline": {"bound": "hbm", "kernel": "pass_a256_kernel (spectral z pass)",
                          "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
