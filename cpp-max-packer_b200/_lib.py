@@ -90,6 +90,11 @@ def _declare(h):
         getattr(h, name).argtypes = [P, ctypes.POINTER(CorrelationSpec), P, P, ctypes.POINTER(CorrelationLimits),
                                      ctypes.POINTER(Control), ctypes.c_uint32, P, ctypes.c_uint64,
                                      ctypes.POINTER(CorrelationResultC)]
+    h.spk_correlate_binary_mask.argtypes = [P, ctypes.POINTER(CorrelationSpec), P, P,
+                                            ctypes.POINTER(CorrelationLimits), ctypes.POINTER(Control),
+                                            ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64),
+                                            ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint32, P, ctypes.c_uint64,
+                                            ctypes.POINTER(CorrelationResultC)]
     h.spk_build_proximity.argtypes = [P, P, P, P]
     h.spk_build_proximity_static.argtypes = [P, P, P, P]
 

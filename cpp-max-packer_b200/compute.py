@@ -24,6 +24,8 @@ from ._lib import SpkError, check, lib
 FP32 = 0
 FP64 = 1
 FP16 = 2  # FP32 transforms, joint spectrum stored in FP16 before the product
+MASK_ZERO = 0  # spk_correlate_binary_mask: mark translations with a zero overlap count
+MASK_NONZERO = 1  # ... or with a non-zero one
 
 _MESSAGES = {
     "CORRELATION_SHAPE_OVERFLOW": "Correlation extents must be positive and representable.",
@@ -79,6 +81,20 @@ class CorrelationResult:
     translation_first: tuple
     shape: tuple
     values: np.ndarray
+    numeric: NumericReport
+    stats: CorrelationStats
+    padded_shape: tuple = (0, 0, 0)
+
+
+@dataclasses.dataclass
+class MaskResult:
+    """spk_correlate_binary_mask's outcome: the correlation range and checks as
+    in CorrelationResult, and the u8 mask over the requested box (X fastest)."""
+    translation_first: tuple
+    shape: tuple
+    box_first: tuple
+    box_shape: tuple
+    mask: np.ndarray
     numeric: NumericReport
     stats: CorrelationStats
     padded_shape: tuple = (0, 0, 0)
@@ -212,6 +228,50 @@ def correlate_binary(spec: CorrelationSpec, environment, kernel, limits: Optiona
     """GPU compute::correlate_binary_cpu: full-range overlap counts (rounded, checked)."""
     return _correlate("spk_correlate_binary", spec, environment, kernel, limits, control, precision, context,
                       np.uint8)
+
+
+def correlate_binary_mask(spec: CorrelationSpec, environment, kernel, box_first: Sequence[int],
+                          box_shape: Sequence[int], select: int = MASK_ZERO,
+                          limits: Optional[CorrelationLimits] = None, control: Optional[OperationControl] = None,
+                          precision: int = FP32, context: Optional[Context] = None,
+                          capacity: Optional[int] = None) -> Union[MaskResult, CorrelationFailure]:
+    """The binary correlation thresholded on the device: one byte per
+    translation of the box instead of the full-range counts.  The gap-fill
+    free mask (gap_fill.cpp:404-420) is the legal box with MASK_ZERO; the
+    blocked offsets (gap_fill.cpp:443-446) and no-fit maps
+    (slab_lattice.cpp:688-691) are the full range with MASK_NONZERO."""
+    context = context or default_context()
+    limits = limits or CorrelationLimits()
+    es = [int(v) for v in spec.environment_shape]
+    ks = [int(v) for v in spec.kernel_shape]
+    env = np.ascontiguousarray(environment, dtype=np.uint8).reshape(-1)
+    ker = np.ascontiguousarray(kernel, dtype=np.uint8).reshape(-1)
+    if env.size != int(np.prod(es, dtype=np.int64)) or ker.size != int(np.prod(ks, dtype=np.int64)):
+        return CorrelationFailure("CORRELATION_INVALID_FIELD", _MESSAGES["CORRELATION_INVALID_FIELD"],
+                                  CorrelationStats())
+    bf = (ctypes.c_int64 * 3)(*[int(v) for v in box_first])
+    bs = (ctypes.c_uint32 * 3)(*[int(v) for v in box_shape])
+    count = int(np.prod([int(v) for v in box_shape], dtype=np.int64))
+    mask = np.zeros(max(count, 1), np.uint8)
+    cap = count if capacity is None else int(capacity)
+    res = _lib.CorrelationResultC()
+    lim = _lib.CorrelationLimits(limits.max_working_bytes, limits.reserved_bytes, limits.max_padded_cells,
+                                 limits.max_direct_terms)
+    ctl = control.as_c() if control is not None else None
+    status = lib().spk_correlate_binary_mask(
+        context.handle, ctypes.byref(_spec_c(spec)), env.ctypes.data_as(ctypes.c_void_p),
+        ker.ctypes.data_as(ctypes.c_void_p), ctypes.byref(lim), ctypes.byref(ctl) if ctl is not None else None,
+        precision, bf, bs, select, mask.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(res))
+    stats = CorrelationStats(res.padded_cells, res.working_bytes_peak, res.direct_terms)
+    if status:
+        code = _lib.status_code(status)
+        if code in ("CUDA_RUNTIME_ERROR", "SPK_INVALID_ARGUMENT"):
+            raise SpkError(status, code, "spk_correlate_binary_mask")
+        return CorrelationFailure(code, _MESSAGES.get(code, code), stats)
+    return MaskResult(tuple(res.translation_first), tuple(res.shape), tuple(int(v) for v in box_first),
+                      tuple(int(v) for v in box_shape), mask[:count],
+                      NumericReport(res.max_integer_residual, res.mass_residual, res.max_probe_error), stats,
+                      tuple(res.padded_shape))
 
 
 def correlate_proximity(spec: CorrelationSpec, environment, kernel, limits: Optional[CorrelationLimits] = None,

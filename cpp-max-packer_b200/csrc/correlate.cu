@@ -207,6 +207,42 @@ __global__ void extract_kernel(const cplx_t<T>* __restrict__ w, Grid g, int ox, 
     }
 }
 
+// Translation mask over a caller's box of absolute translations, from the
+// rounded full-range counts: inside the range, 1 where the count is zero
+// (want_zero) or non-zero (otherwise); outside the range, 0.  These are the
+// free and blocked rules of gap_fill.cpp:404-420 and :443-446.  dx..dz are the
+// box's first translation minus the range's first, clamped on the host so
+// that dx + x cannot overflow.
+__global__ void mask_kernel(const double* __restrict__ counts, long long ox, long long oy, long long oz, long long dx,
+                            long long dy, long long dz, long long bx, long long by, long long bz, int want_zero,
+                            std::uint8_t* __restrict__ mask)
+{
+    const long long n = bx * by * bz;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long x = dx + i % bx;
+        const long long r = i / bx;
+        const long long y = dy + r % by;
+        const long long z = dz + r / by;
+        std::uint8_t m = 0;
+        if (x >= 0 && y >= 0 && z >= 0 && x < ox && y < oy && z < oz) {
+            const bool zero = counts[x + ox * (y + oy * z)] == 0.0;
+            m = (zero == (want_zero != 0)) ? 1 : 0;
+        }
+        mask[i] = m;
+    }
+}
+
+// A request to threshold on the device: the mask is written to host memory
+// and the FP64 counts stay on the device.
+struct MaskRequest {
+    std::int64_t first[3];
+    std::uint32_t shape[3];
+    bool want_zero;
+    std::uint8_t* mask;
+    std::uint64_t capacity;
+};
+
 struct Compensated {
     double value {}, correction {};
     void add(double v)
@@ -304,7 +340,8 @@ int grid_blocks(long long n, int threads)
 template <typename T, typename E>
 int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* environment, const std::uint8_t* kernel,
               const spk_correlation_limits* limits_ptr, const spk_control* control, double* out_values,
-              std::uint64_t out_capacity, spk_correlation_result* result, bool half_spectra = false)
+              std::uint64_t out_capacity, spk_correlation_result* result, bool half_spectra = false,
+              const MaskRequest* mask_request = nullptr)
 {
     constexpr bool binary = std::is_same_v<E, std::uint8_t>;
     if (!ctx || !spec_ptr || !environment || !kernel || !result) {
@@ -403,13 +440,24 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     const int extract_threads = 256;
     const int extract_blocks = grid_blocks(static_cast<long long>(padded_count), extract_threads);
     const std::uint64_t half_bytes = half_spectra ? static_cast<std::uint64_t>(g.n()) * 4 : 0;
+    std::uint64_t mask_count = 0;
+    if (mask_request) {
+        mask_count = 1;
+        for (int a = 0; a != 3; ++a) {
+            if (!checked_mul(mask_count, mask_request->shape[a], mask_count)) {
+                return kShapeOverflow;
+            }
+        }
+    }
     const std::uint64_t working = limits.reserved_bytes + 2 * grid_bytes + half_bytes + out_bytes +
-                                  env_count * sizeof(E) + ker_count + extract_blocks * sizeof(ExtractStats) + 64;
+                                  env_count * sizeof(E) + ker_count + extract_blocks * sizeof(ExtractStats) + 64 +
+                                  mask_count;
     if (working > limits.max_working_bytes) {
         return kMemoryLimit;
     }
     result->working_bytes_peak = working;
-    if (out_capacity < padded_count || !out_values) {
+    if (mask_request ? (mask_request->capacity < mask_count || (mask_count && !mask_request->mask))
+                     : (out_capacity < padded_count || !out_values)) {
         return kInvalidArgument;
     }
     int status = kOk;
@@ -478,9 +526,33 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         binary ? 1 : 0, maximum_output, imag_tolerance, proximity_tolerance, d_out, d_stats, d_flags,
         reinterpret_cast<int*>(d_flags + 1));
     ctx->launches++;
+    if (mask_request && mask_count) {
+        // Box offset from the range's first translation, per axis.  A box
+        // more than 2^33 away lies wholly outside the < 2^32-wide range, so
+        // the offset is clamped there and dx + x stays far from overflow.
+        long long delta[3];
+        for (int a = 0; a != 3; ++a) {
+            long long d;
+            if (__builtin_sub_overflow(mask_request->first[a], result->translation_first[a], &d)) {
+                d = mask_request->first[a] < 0 ? -(1LL << 33) : (1LL << 33);
+            }
+            delta[a] = std::max(-(1LL << 33), std::min(1LL << 33, d));
+        }
+        auto* d_mask = static_cast<std::uint8_t*>(device_buffer(ctx, "corr.mask", mask_count, status));
+        if (!d_mask) {
+            return status;
+        }
+        mask_kernel<<<grid_blocks(static_cast<long long>(mask_count), threads), threads, 0, st>>>(
+            d_out, padded[0], padded[1], padded[2], delta[0], delta[1], delta[2], mask_request->shape[0],
+            mask_request->shape[1], mask_request->shape[2], mask_request->want_zero ? 1 : 0, d_mask);
+        ctx->launches++;
+        cudaMemcpyAsync(mask_request->mask, d_mask, mask_count, cudaMemcpyDeviceToHost, st);
+    }
     std::vector<ExtractStats> stats(extract_blocks);
     unsigned long long flags[2] {};
-    cudaMemcpyAsync(out_values, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
+    if (!mask_request) {
+        cudaMemcpyAsync(out_values, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
+    }
     cudaMemcpyAsync(stats.data(), d_stats, extract_blocks * sizeof(ExtractStats), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(flags, d_flags, 16, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
@@ -529,6 +601,17 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     add_probe(count / 3);
     add_probe((count / 3) * 2);
     add_probe((count / 4) * 3);
+    // With a mask request the counts stay on the device: fetch the probed ones.
+    double probe_values[8] {};
+    if (mask_request) {
+        for (std::size_t p = 0; p != probe_count; ++p) {
+            cudaMemcpyAsync(&probe_values[p], d_out + probes[p], sizeof(double), cudaMemcpyDeviceToHost, st);
+        }
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            cudaGetLastError();
+            return kCuda;
+        }
+    }
     double max_probe_error = 0;
     std::uint64_t terms = 0;
     for (std::size_t p = 0; p != probe_count; ++p) {
@@ -540,7 +623,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
             }
             return kDirectTermLimit;
         }
-        const double error = std::fabs(out_values[probes[p]] - expected);
+        const double error = std::fabs((mask_request ? probe_values[p] : out_values[probes[p]]) - expected);
         max_probe_error = std::max(max_probe_error, error);
         // FP64 keeps the reference's per-probe relative tolerance; FP32 and
         // FP16 state their bounds relative to the output scale.
@@ -607,6 +690,37 @@ int spk_correlate_binary(spk_context* ctx, const spk_correlation_spec* spec, con
                                      : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
                                                                       out_values, out_capacity, result,
                                                                       precision == SPK_FP16);
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_correlate_binary_mask(spk_context* ctx, const spk_correlation_spec* spec, const uint8_t* environment,
+                              const uint8_t* kernel, const spk_correlation_limits* limits, const spk_control* control,
+                              uint32_t precision, const int64_t box_first[3], const uint32_t box_shape[3],
+                              uint32_t select, uint8_t* mask, uint64_t mask_capacity, spk_correlation_result* result)
+{
+    try {
+        if (ctx && cudaSetDevice(ctx->device) != cudaSuccess) {
+            return kCuda;
+        }
+        if (precision > SPK_FP16 || select > SPK_MASK_NONZERO || !box_first || !box_shape) {
+            return kInvalidArgument;
+        }
+        MaskRequest request {};
+        for (int a = 0; a != 3; ++a) {
+            request.first[a] = box_first[a];
+            request.shape[a] = box_shape[a];
+        }
+        request.want_zero = select == SPK_MASK_ZERO;
+        request.mask = mask;
+        request.capacity = mask_capacity;
+        return precision == SPK_FP64 ? correlate<double, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
+                                                                       nullptr, 0, result, false, &request)
+                                     : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
+                                                                      nullptr, 0, result, precision == SPK_FP16,
+                                                                      &request);
     }
     catch (...) {
         return kAllocation;

@@ -32,6 +32,12 @@ typedef struct spk_context spk_context;
  * the output scale). */
 enum { SPK_FP32 = 0, SPK_FP64 = 1, SPK_FP16 = 2 };
 
+/* Which translations spk_correlate_binary_mask marks: SPK_MASK_ZERO, those
+ * with a zero overlap count (gap_fill.cpp:404-420, free translations);
+ * SPK_MASK_NONZERO, those with a non-zero count (gap_fill.cpp:443-446,
+ * blocked offsets; slab_lattice.cpp:675-691, no-fit maps). */
+enum { SPK_MASK_ZERO = 0, SPK_MASK_NONZERO = 1 };
+
 /* Reference: compute::CorrelationSpec, correlation.hpp:22-27. */
 typedef struct spk_correlation_spec {
     uint32_t environment_shape[3];
@@ -116,6 +122,26 @@ int spk_correlate_binary(spk_context* context, const spk_correlation_spec* spec,
                          const spk_correlation_limits* limits, const spk_control* control,
                          uint32_t precision, double* out_values, uint64_t out_capacity,
                          spk_correlation_result* result);
+
+/* The binary correlation thresholded on the device, for the solver's mask
+ * callers: gap_fill.cpp:392 (free translations over the legal box, read back
+ * at :404-420), gap_fill.cpp:432 (blocked offsets, :443-446) and
+ * slab_lattice.cpp:675 (no-fit map).  Each of them calls
+ * compute::correlate_binary_cpu and rounds the values on the host.  This
+ * runs the same correlation with the same checks and status codes as
+ * spk_correlate_binary.  Instead of the (E+K-1)^3 doubles it writes one byte
+ * per translation of the caller's box: box_first is the absolute translation
+ * of mask[0], box_shape its extent, X fastest.  mask[t] is 1 when t lies in
+ * the correlation range and its rounded count is zero (SPK_MASK_ZERO) or
+ * non-zero (SPK_MASK_NONZERO); otherwise it is 0.  result is filled as by
+ * spk_correlate_binary, and mask_capacity must hold the box.  Host pointers;
+ * on a non-zero status the mask's contents are unspecified. */
+int spk_correlate_binary_mask(spk_context* context, const spk_correlation_spec* spec,
+                              const uint8_t* environment, const uint8_t* kernel,
+                              const spk_correlation_limits* limits, const spk_control* control,
+                              uint32_t precision, const int64_t box_first[3], const uint32_t box_shape[3],
+                              uint32_t select, uint8_t* mask, uint64_t mask_capacity,
+                              spk_correlation_result* result);
 
 /* Replaces compute::correlate_proximity_cpu (correlation.hpp:113-117,
  * correlation.cpp:650-655): f64 environment in [0,1], binary kernel. */
