@@ -736,13 +736,18 @@ int spk_cube_catalog(double out[96])
     if (!out) {
         return kInvalidArgument;
     }
-    const auto cube = geo::cube_catalog();
-    for (int i = 0; i < 24; ++i) {
-        for (int k = 0; k < 4; ++k) {
-            out[4 * i + k] = cube[i][k];
+    try {
+        const auto cube = geo::cube_catalog();
+        for (int i = 0; i < 24; ++i) {
+            for (int k = 0; k < 4; ++k) {
+                out[4 * i + k] = cube[i][k];
+            }
         }
+        return kOk;
     }
-    return kOk;
+    catch (...) {
+        return kAllocation;
+    }
 }
 
 int spk_custom_catalog(const double* in, uint64_t count, double* out, uint64_t* out_count)
@@ -750,25 +755,30 @@ int spk_custom_catalog(const double* in, uint64_t count, double* out, uint64_t* 
     if (!in || !out || !out_count || count == 0) {
         return kCatalog;
     }
-    std::vector<geo::Quat> result;
-    for (std::uint64_t i = 0; i < count; ++i) {
-        const geo::Quat q { in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3] };
-        const double n = std::hypot(std::hypot(q[0], q[1]), std::hypot(q[2], q[3]));
-        if (!std::isfinite(n) || !(n > 0)) {
-            return kCatalog;
+    try {
+        std::vector<geo::Quat> result;
+        for (std::uint64_t i = 0; i < count; ++i) {
+            const geo::Quat q { in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3] };
+            const double n = std::hypot(std::hypot(q[0], q[1]), std::hypot(q[2], q[3]));
+            if (!std::isfinite(n) || !(n > 0)) {
+                return kCatalog;
+            }
+            const auto c = geo::canonical(q);
+            if (std::find(result.begin(), result.end(), c) == result.end()) {
+                result.push_back(c);
+            }
         }
-        const auto c = geo::canonical(q);
-        if (std::find(result.begin(), result.end(), c) == result.end()) {
-            result.push_back(c);
+        for (std::size_t i = 0; i < result.size(); ++i) {
+            for (int k = 0; k < 4; ++k) {
+                out[4 * i + k] = result[i][k];
+            }
         }
+        *out_count = result.size();
+        return kOk;
     }
-    for (std::size_t i = 0; i < result.size(); ++i) {
-        for (int k = 0; k < 4; ++k) {
-            out[4 * i + k] = result[i][k];
-        }
+    catch (...) {
+        return kAllocation;
     }
-    *out_count = result.size();
-    return kOk;
 }
 
 int spk_session_open(spk_context* ctx, const spk_session_desc* d, spk_session_info* info)
