@@ -86,12 +86,17 @@ typedef struct spk_control {
 
 /* ---- context ---------------------------------------------------------- */
 
-/* Opens a context on `device` with a device-memory cap (0 = no cap). */
+/* Opens a context on `device` with a device-memory cap (0 = no cap).  It
+ * holds what the reference's FftExecution holds (make_fft_execution,
+ * correlation.hpp:80-98): execution resources reused across calls, which one
+ * coordinator serialises (correlation.hpp:78-79). */
 int spk_context_create(int device, uint64_t max_device_bytes, spk_context** out);
 void spk_context_destroy(spk_context* context);
-/* Static string for a status (e.g. "CORRELATION_NUMERIC"); never NULL. */
+/* Static string for a status (e.g. "CORRELATION_NUMERIC"); never NULL.  The
+ * reference's static code strings (correlation.hpp:52-56, ADR 0015). */
 const char* spk_status_code(int status);
-/* Number of kernels this library launched on the context (all entry points). */
+/* Measurement only, no counterpart in the reference: the number of kernels
+ * this library launched on the context (all entry points). */
 uint64_t spk_context_launches(const spk_context* context);
 /* The CUDA stream (cudaStream_t) every launch of this context is queued on,
  * so a caller can record timing events on it. */
@@ -323,22 +328,30 @@ int spk_session_open(spk_context* context, const spk_session_desc* desc, spk_ses
 int spk_session_close(spk_context* context);
 int spk_session_info_get(spk_context* context, spk_session_info* info);
 /* Stamps a copy at lattice translation t with catalog orientation o
- * (BlockedField::add of voxelize_placed at pose origin + pitch * t). */
+ * (BlockedField::add, conservative_fields.hpp:134-138,
+ * conservative_fields.cpp:1695-1808, of voxelize_placed at pose
+ * origin + pitch * t). */
 int spk_session_place(spk_context* context, uint64_t orientation, const int64_t translation[3]);
-/* Unstamps the most recent copy (BlockedField::remove). */
+/* Unstamps the most recent copy (BlockedField::remove,
+ * conservative_fields.hpp:140-143, conservative_fields.cpp:1810-1885). */
 int spk_session_remove_last(spk_context* context);
-/* Pages for n queries over the current layout; pages holds n x 32 entries. */
+/* Pages for n queries over the current layout, as build_spectral_pipeline's
+ * page scan and recount (spectral_pipeline.cpp:1706-1857) make them; pages
+ * holds n x 32 entries. */
 int spk_session_pages(spk_context* context, uint64_t n, const spk_page_query* queries, spk_candidate* pages,
                       uint32_t* counts, spk_page_report* reports);
 /* Greedy fill (spectral.cpp:1460-1591 page merge, direct-zero recount gate;
  * native validation is the caller's): up to max_steps copies are placed. */
 int spk_session_greedy(spk_context* context, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
                        int64_t* translations, double* scores);
-/* Work counters of the session's page pipeline since open or the last reset:
+/* Measurement only, no counterpart in the reference.  Work counters of the
+ * session's page pipeline since open or the last reset:
  * out[0] first-pass pages, [1] threshold passes, [2] exactly rescored
  * candidates, [3] pages certified by the first pass. */
 int spk_session_stats(spk_context* context, uint64_t out[4], int reset);
-/* Field readback: kind 0 container blocker, 1 occupancy, 2 kernel of
+/* The session's fields, which the reference keeps as host CellFields
+ * (conservative_fields.hpp:71-126).  Readback: kind 0 container blocker,
+ * 1 occupancy, 2 kernel of
  * `orientation` (window in first/shape), 3 proximity (f64). */
 int spk_session_field(spk_context* context, int kind, uint64_t orientation, int64_t first[3], uint32_t shape[3],
                       void* out, uint64_t capacity_bytes);
