@@ -1,7 +1,6 @@
 """The C-ABI library loads and exports every entry point include/*.h declares
 (no compute calls: CPU only)."""
 
-import ctypes
 import glob
 import os
 import re
