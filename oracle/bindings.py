@@ -17,6 +17,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libspk_ref.so")
+# Where the reference checkout lies when it is present (build recipes only).
+REFERENCE_ROOT = "/root/reference"
 
 _c = ctypes
 _P = ctypes.c_void_p
@@ -34,7 +36,7 @@ def build_oracle() -> str:
     return ORACLE_SO
 
 
-def build_reference(reference_root: str = "/root/reference") -> str | None:
+def build_reference(reference_root: str = REFERENCE_ROOT) -> str | None:
     """Compiles the reference's hot-path sources in place (oracle/ref/Makefile)."""
     if not os.path.isdir(reference_root):
         return REF_SO if os.path.exists(REF_SO) else None
