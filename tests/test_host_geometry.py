@@ -51,3 +51,22 @@ def test_environment_window_halo():
     geometry = package("geometry")
     assert geometry.environment_window((0, 0, 0, 64, 64, 64), (0, 0, 0), 1.0) == ((-1, -1, -1), (66, 66, 66))
     assert geometry.environment_window((0, 0, 0, 63, 63, 63), (0, 0, 0), 0.5) == ((-1, -1, -1), (128, 128, 128))
+
+
+def test_custom_catalog_matches_the_reference_build(oracle_ref):
+    # The reference's make_orientation_catalog in catalog mode
+    # (orientations.cpp:104-172): unit length, the w > 0 sign rule, and
+    # first-seen de-duplication, on seeded quaternions with scaled copies,
+    # sign flips and w = 0 entries mixed in.
+    geometry = package("geometry")
+    rng = np.random.default_rng(12)
+    q = rng.standard_normal((40, 4))
+    q[5] = -q[3]
+    q[9] = 3.5 * q[1]
+    q[12] = [0.0, 0.6, -0.8, 0.0]
+    q[13] = [0.0, -0.6, 0.8, 0.0]
+    q[20] = [1e-3, 0.0, 0.0, 0.0]
+    got = geometry.custom_catalog(q)
+    want = oracle_ref.catalog(4, q)
+    assert got.shape == want.shape
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
