@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
+import time
 from typing import Optional, Sequence, Union
 
 import numpy as np
@@ -130,6 +131,14 @@ class OperationControl:
     def as_c(self) -> _lib.Control:
         return _lib.Control(ctypes.pointer(self._word), self.deadline_ns)
 
+    def poll(self) -> Optional[str]:
+        """The stop cause as the reference's code, or None (OperationControl::poll)."""
+        if self._word.value:
+            return "OPERATION_CANCELLED"
+        if self.deadline_ns and time.monotonic_ns() >= self.deadline_ns:
+            return "DEADLINE_EXCEEDED"
+        return None
+
 
 class Context:
     """A device context: stream, memory arena and the launch counter."""
@@ -191,16 +200,32 @@ def estimate_correlation(spec: CorrelationSpec, precision: int = FP64) -> Union[
     return CorrelationEstimate(tuple(out.padded_shape), out.padded_cells, out.working_bytes)
 
 
+def _field_failure(es, ks, env, ker, control=None) -> Optional[CorrelationFailure]:
+    """The reference's first checks, in its order (correlation.cpp:263-312):
+    interruption, extents, then cell counts.  The library cannot see the cell
+    counts, so a bad field fails here, before any device work; an
+    interruption still wins over it, as in the reference.  Valid fields go to
+    the library, which polls the control itself."""
+    for code, bad in (("CORRELATION_SHAPE_OVERFLOW", min(es + ks) <= 0),
+                      ("CORRELATION_INVALID_FIELD", env.size != int(np.prod(es, dtype=np.int64)) or
+                       ker.size != int(np.prod(ks, dtype=np.int64)))):
+        if bad:
+            cause = control.poll() if control is not None else None
+            code = cause or code
+            return CorrelationFailure(code, _MESSAGES[code], CorrelationStats())
+    return None
+
+
 def _correlate(name, spec, environment, kernel, limits, control, precision, context, env_dtype):
-    context = context or default_context()
     limits = limits or CorrelationLimits()
     es = [int(v) for v in spec.environment_shape]
     ks = [int(v) for v in spec.kernel_shape]
     env = np.ascontiguousarray(environment, dtype=env_dtype).reshape(-1)
     ker = np.ascontiguousarray(kernel, dtype=np.uint8).reshape(-1)
-    if env.size != int(np.prod(es, dtype=np.int64)) or ker.size != int(np.prod(ks, dtype=np.int64)):
-        return CorrelationFailure("CORRELATION_INVALID_FIELD", _MESSAGES["CORRELATION_INVALID_FIELD"],
-                                  CorrelationStats())
+    bad = _field_failure(es, ks, env, ker, control)
+    if bad is not None:
+        return bad
+    context = context or default_context()
     count = int(np.prod([e + k - 1 for e, k in zip(es, ks)], dtype=np.int64))
     out = np.empty(max(count, 1), np.float64)
     res = _lib.CorrelationResultC()
@@ -240,15 +265,15 @@ def correlate_binary_mask(spec: CorrelationSpec, environment, kernel, box_first:
     free mask (gap_fill.cpp:404-420) is the legal box with MASK_ZERO; the
     blocked offsets (gap_fill.cpp:443-446) and no-fit maps
     (slab_lattice.cpp:688-691) are the full range with MASK_NONZERO."""
-    context = context or default_context()
     limits = limits or CorrelationLimits()
     es = [int(v) for v in spec.environment_shape]
     ks = [int(v) for v in spec.kernel_shape]
     env = np.ascontiguousarray(environment, dtype=np.uint8).reshape(-1)
     ker = np.ascontiguousarray(kernel, dtype=np.uint8).reshape(-1)
-    if env.size != int(np.prod(es, dtype=np.int64)) or ker.size != int(np.prod(ks, dtype=np.int64)):
-        return CorrelationFailure("CORRELATION_INVALID_FIELD", _MESSAGES["CORRELATION_INVALID_FIELD"],
-                                  CorrelationStats())
+    bad = _field_failure(es, ks, env, ker, control)
+    if bad is not None:
+        return bad
+    context = context or default_context()
     bf = (ctypes.c_int64 * 3)(*[int(v) for v in box_first])
     bs = (ctypes.c_uint32 * 3)(*[int(v) for v in box_shape])
     count = int(np.prod([int(v) for v in box_shape], dtype=np.int64))
