@@ -1,6 +1,9 @@
-"""The host mirror's own checks, which come before any device work and so run
-without a GPU: extents, then cell counts, with the reference's codes and in
-its order (correlation.cpp:276-312)."""
+"""Host-side logic that runs without a GPU.  It covers two things:
+- the mirror's own checks, which come before any device work: extents, then
+  cell counts, with the reference's codes and in its order
+  (correlation.cpp:263-312);
+- the proposal trainer's label definition, layout schedule and dataset merge.
+"""
 
 import numpy as np
 
@@ -35,3 +38,33 @@ def test_an_interruption_wins_over_a_bad_field():
     r = compute.correlate_binary(spec, np.zeros(23, np.uint8), np.ones(8, np.uint8),
                                  control=compute.OperationControl(deadline_ns=1))
     assert r.code == "DEADLINE_EXCEEDED"
+
+
+def test_proposal_labels_and_layout_schedule():
+    # Labels: each orientation's gap to the layout's best exact score, clipped
+    # at the cap and scaled to [0, 1]; no admissible copy labels 1; a layout
+    # where nothing is admissible gives no labels.
+    train = package("train_proposal")
+    best = np.array([-0.30, -0.29, np.inf, 0.10, -0.30])
+    y = train.labels_from(best, 0.25)
+    assert y.dtype == np.float32
+    assert np.allclose(y, [0.0, 0.04, 1.0, 1.0, 0.0], atol=1e-6)
+    assert train.labels_from(np.full(3, np.inf), 0.25) is None
+    # Every step up to `dense`, then every `stride`-th.
+    assert train.labelled_steps(3, 10, 35) == [0, 1, 2, 3, 13, 23, 33]
+
+
+def test_policy_layouts_merge_with_reindexed_crops():
+    # Policy layouts index their crops from 0; their items already start at
+    # the base dataset's item count (generate_policy's item_base_count).
+    train, proposal = package("train_proposal"), package("proposal")
+    base = proposal.ProposalDataset(np.zeros((2, 4)), np.zeros((3, 4)), np.array([0, 1], np.uint32),
+                                    np.array([2, 0], np.uint32), np.array([0.1, 0.2], np.float32))
+    extra = ([np.ones(4)], [np.ones((2, 4))], [np.full(2, 0, np.uint32)], [3 + np.arange(2, dtype=np.uint32)],
+             [np.array([0.3, 0.4], np.float32)])
+    merged = train.merge_datasets(base, *extra)
+    assert merged.crops.shape == (3, 4) and merged.items.shape == (5, 4)
+    assert merged.sample_crop.tolist() == [0, 1, 2, 2]
+    assert merged.sample_item.tolist() == [2, 0, 3, 4]
+    assert np.allclose(merged.sample_label, [0.1, 0.2, 0.3, 0.4])
+    assert train.merge_datasets(base, [], [], [], [], []) is base
