@@ -223,8 +223,10 @@ constexpr double kSlopes[12][2] = { { 0.137, 0.271 }, { 0.223, 0.419 }, { 0.347,
 
 // Ray parity against a triangle list; `prefilter` skips triangles whose
 // bounding box is strictly disjoint from the segment's (local variant only).
+// `bounds`, when given, holds each triangle's coordinate bounds: the values
+// the prefilter would otherwise recompute per ray.
 Decision ray_parity(const Vec3& point, const Bounds& reach, const std::vector<std::array<Vec3, 3>>& triangles,
-                    bool prefilter)
+                    bool prefilter, const std::vector<Bounds>* bounds = nullptr)
 {
     const double span = std::max({ reach.max[0] - reach.min[0], reach.max[1] - reach.min[1],
                                    reach.max[2] - reach.min[2], 1.0 });
@@ -233,12 +235,13 @@ Decision ray_parity(const Vec3& point, const Bounds& reach, const std::vector<st
                               point[2] + slope[1] * span };
         std::uint64_t crossings = 0;
         bool retry = false;
-        for (const auto& tri : triangles) {
+        for (std::size_t i = 0; i < triangles.size(); ++i) {
+            const auto& tri = triangles[i];
             if (prefilter) {
                 bool disjoint = false;
                 for (int a = 0; a < 3; ++a) {
-                    const double low = std::min({ tri[0][a], tri[1][a], tri[2][a] });
-                    const double high = std::max({ tri[0][a], tri[1][a], tri[2][a] });
+                    const double low = bounds ? (*bounds)[i].min[a] : std::min({ tri[0][a], tri[1][a], tri[2][a] });
+                    const double high = bounds ? (*bounds)[i].max[a] : std::max({ tri[0][a], tri[1][a], tri[2][a] });
                     disjoint = disjoint || std::max(point[a], endpoint[a]) < low ||
                                std::min(point[a], endpoint[a]) > high;
                 }
@@ -314,10 +317,21 @@ Decision local_interval_point_in_material(const Placed& solid, const Bounds& wi)
         }
     }
     const auto& mesh = *solid.prepared->mesh;
-    for (const auto& face : mesh.triangles) {
+    const auto& triangles = solid.prepared->triangles;
+    const auto& bounds = solid.prepared->triangle_bounds;
+    for (std::size_t i = 0; i < triangles.size(); ++i) {
+        // The first three axes of triangle_box_disjoint, from the kept bounds:
+        // a triangle they separate is disjoint, and the full test is skipped.
+        bool separated = false;
+        for (int a = 0; a < 3; ++a) {
+            separated = separated || bounds[i].max[a] < local.v[a].low || local.v[a].high < bounds[i].min[a];
+        }
+        if (separated) {
+            continue;
+        }
         IVec3 tri[3];
         for (int k = 0; k < 3; ++k) {
-            const Vec3& v = mesh.vertices[face[k]];
+            const Vec3& v = triangles[i][k];
             tri[k] = { { point_interval(v[0]), point_interval(v[1]), point_interval(v[2]) } };
         }
         if (!triangle_box_disjoint(tri, local)) {
@@ -331,13 +345,7 @@ Decision local_interval_point_in_material(const Placed& solid, const Bounds& wi)
             return Decision::indeterminate;
         }
     }
-    std::vector<std::array<Vec3, 3>> triangles(mesh.triangles.size());
-    for (std::size_t i = 0; i < mesh.triangles.size(); ++i) {
-        for (int k = 0; k < 3; ++k) {
-            triangles[i][k] = mesh.vertices[mesh.triangles[i][k]];
-        }
-    }
-    return ray_parity(witness, mesh.bounds, triangles, true);
+    return ray_parity(witness, mesh.bounds, triangles, true, &bounds);
 }
 
 }  // namespace
@@ -346,6 +354,18 @@ Prepared prepare(const Mesh& mesh)
 {
     Prepared p;
     p.mesh = &mesh;
+    p.triangles.resize(mesh.triangles.size());
+    p.triangle_bounds.resize(mesh.triangles.size());
+    for (std::size_t i = 0; i < mesh.triangles.size(); ++i) {
+        auto& tri = p.triangles[i];
+        for (int k = 0; k < 3; ++k) {
+            tri[k] = mesh.vertices[mesh.triangles[i][k]];
+        }
+        for (int a = 0; a < 3; ++a) {
+            p.triangle_bounds[i].min[a] = std::min({ tri[0][a], tri[1][a], tri[2][a] });
+            p.triangle_bounds[i].max[a] = std::max({ tri[0][a], tri[1][a], tri[2][a] });
+        }
+    }
     // certify_cuboid (:384-447)
     const auto& vs = mesh.vertices;
     if (vs.size() != 8 || mesh.triangles.size() != 12) {

@@ -31,10 +31,14 @@ struct Mesh {
 };
 
 // prepare(): cuboid certificate (validation_kernel.cpp:384-447, 805-827).
+// Also keeps each triangle's local vertices and their bounds, which every
+// interval witness test reads (local_interval_point_in_material).
 struct Prepared {
     const Mesh* mesh {};
     bool is_cuboid {};
     Bounds cuboid {};
+    std::vector<std::array<Vec3, 3>> triangles;
+    std::vector<Bounds> triangle_bounds;
 };
 Prepared prepare(const Mesh& mesh);
 
