@@ -736,6 +736,39 @@ PlanKind plan_placed_window(const Placed& placed, const Window& whole, const dou
     return same ? PlanKind::full_window : PlanKind::cropped_window;
 }
 
+namespace {
+
+// floor((v - origin) / pitch) with the quotient in long double, as
+// rasterize_boundary forms it (validation_kernel.cpp:3282-3330).  The binary64
+// quotient is within 2^-52 of the exact one, relative, and the long double
+// quotient within 2^-62.  When the binary64 quotient lies farther than 2^-48
+// (relative) from every integer, all three have the same floor, so the long
+// double division is needed only near integers and for huge or non-finite
+// quotients.  `lower` selects the reference's range check for a lower or an
+// upper bound; false when it fails.
+bool quotient_floor(double v, double origin, double pitch, bool lower, std::int64_t& out)
+{
+    const double q = (v - origin) / pitch;
+    if (std::isfinite(q) && std::fabs(q) < 0x1p50) {
+        const double f = std::floor(q);
+        const double margin = std::fabs(q) * 0x1p-48 + 0x1p-60;
+        if (q - f > margin && (f + 1.0) - q > margin) {
+            out = static_cast<std::int64_t>(f);
+            return true;
+        }
+    }
+    const long double ratio = (static_cast<long double>(v) - origin) / pitch;
+    if (!std::isfinite(ratio) ||
+        (lower ? ratio <= static_cast<long double>(std::numeric_limits<std::int64_t>::min() + 1)
+               : ratio >= static_cast<long double>(std::numeric_limits<std::int64_t>::max()))) {
+        return false;
+    }
+    out = static_cast<std::int64_t>(std::floor(ratio));
+    return true;
+}
+
+}  // namespace
+
 bool face_ranges(const Placed& placed, const Window& window, const double* origin, double pitch,
                  std::vector<FaceRange>& out)
 {
@@ -756,15 +789,12 @@ bool face_ranges(const Placed& placed, const Window& window, const double* origi
                 low = std::min(low, placed.intervals[face[k]].v[a].low);
                 high = std::max(high, placed.intervals[face[k]].v[a].high);
             }
-            const long double lo = (static_cast<long double>(low) - origin[a]) / pitch;
-            const long double hi = (static_cast<long double>(high) - origin[a]) / pitch;
-            if (!std::isfinite(lo) || !std::isfinite(hi) ||
-                lo <= static_cast<long double>(std::numeric_limits<std::int64_t>::min() + 1) ||
-                hi >= static_cast<long double>(std::numeric_limits<std::int64_t>::max())) {
+            std::int64_t lo, hi;
+            if (!quotient_floor(low, origin[a], pitch, true, lo) || !quotient_floor(high, origin[a], pitch, false, hi)) {
                 return false;
             }
-            r.first[a] = static_cast<std::int64_t>(std::floor(lo)) - 1;
-            r.last[a] = static_cast<std::int64_t>(std::floor(hi)) + 1;
+            r.first[a] = lo - 1;
+            r.last[a] = hi + 1;
             if (r.last[a] < window.first[a] || r.first[a] > window_last[a]) {
                 r.outside = 1;
             }
