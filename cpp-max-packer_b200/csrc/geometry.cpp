@@ -95,11 +95,29 @@ bool cardinal_rotation(const Quat& quaternion, int* source_axis, int* sign)
     return true;
 }
 
+// multiply_interval(a, point_interval(p)).  With a point operand the four
+// products are two, each computed twice, and the first-minimum / first-maximum
+// scan picks the same values from the pair, so the result is identical.
+Interval multiply_by_point(const Interval& a, double p)
+{
+    if (!a.valid || !f_finite(p)) {
+        return { 0, 0, false };
+    }
+    const double v0 = f_mul(a.low, p), v2 = f_mul(a.high, p);
+    if (!f_finite(v0) || !f_finite(v2)) {
+        return { 0, 0, false };
+    }
+    double lo = v0, hi = v0;
+    if (v2 < lo) lo = v2;
+    if (hi < v2) hi = v2;
+    return widened(lo, hi);
+}
+
 Interval transformed_interval(const Vec3& point, const Vec3& translation, const Interval rotation[3][3], int row)
 {
     Interval value = point_interval(translation[row]);
     for (int column = 0; column < 3; ++column) {
-        value = add_interval(value, multiply_interval(rotation[row][column], point_interval(point[column])));
+        value = add_interval(value, multiply_by_point(rotation[row][column], point[column]));
     }
     return value;
 }
