@@ -6,7 +6,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <limits>
+#include <mutex>
+#include <thread>
+#include <vector>
 
 #include "exact.hpp"
 
@@ -531,6 +535,70 @@ void rotation_intervals(const Quat& q, Interval h[3][3])
     }
 }
 
+namespace {
+
+// One chunk of place()'s general branch: its vertices' world points and
+// intervals, whether all intervals are valid and all cardinal world points
+// exact, and the bounds of its intervals.
+struct VertexChunk {
+    bool valid { true };
+    bool world_exact { true };
+    bool any { false };
+    Bounds conservative {};
+};
+
+VertexChunk place_vertices(const Mesh& mesh, const Vec3& translation, const RotationTransform& transform,
+                           const Interval rotation[3][3], Placed& out, std::size_t begin, std::size_t end)
+{
+    VertexChunk c;
+    for (std::size_t i = begin; i < end; ++i) {
+        for (int a = 0; a < 3; ++a) {
+            double w = translation[a];
+            for (int s = 0; s < 3; ++s) {
+                w += transform.matrix[a][s] * mesh.vertices[i][s];
+            }
+            out.world[i][a] = w;
+            const Interval iv = transformed_interval(mesh.vertices[i], translation, rotation, a);
+            out.intervals[i].v[a] = iv;
+            if (!iv.valid) {
+                c.valid = false;
+                return c;
+            }
+            if (out.is_cardinal) {
+                const int source = out.source_axis[a];
+                const double ta = translation[a];
+                const double b = out.sign[a] * mesh.vertices[i][source];
+                const double sum = ta + b;
+                out.world[i][a] = sum;
+                c.world_exact = c.world_exact && compare_coordinates({ ta, mesh.vertices[i][source], out.sign[a] },
+                                                                     { 0.0, sum, 1 }) == exact::Sign::zero;
+            }
+            if (!c.any) {
+                c.conservative.min[a] = iv.low;
+                c.conservative.max[a] = iv.high;
+            }
+            else {
+                c.conservative.min[a] = std::min(c.conservative.min[a], iv.low);
+                c.conservative.max[a] = std::max(c.conservative.max[a], iv.high);
+            }
+        }
+        c.any = true;
+    }
+    return c;
+}
+
+// Chunks for n vertices: one below 2048, else up to four of at least 1024.
+std::size_t vertex_parts(std::size_t n)
+{
+    if (n < 2048) {
+        return 1;
+    }
+    const std::size_t cores = std::max(1U, std::thread::hardware_concurrency());
+    return std::min({ std::size_t { 4 }, cores, n / 1024 });
+}
+
+}  // namespace
+
 bool place(const Prepared& prepared, const Vec3& translation, const Quat& q, Placed& out)
 {
     if (!finite_pose(translation, q)) {
@@ -584,36 +652,68 @@ bool place(const Prepared& prepared, const Vec3& translation, const Quat& q, Pla
     }
     Interval rotation[3][3];
     rotation_intervals(q, rotation);
+    // Vertices are independent: contiguous chunks run on up to four host
+    // threads, and their bounds combine in vertex order.  std::min / std::max
+    // keep the earlier of equal values, so the combined bounds are the ones a
+    // single pass over all vertices gives.
+    const std::size_t parts = vertex_parts(nv);
+    std::vector<VertexChunk> chunks(parts);
+    std::exception_ptr failure;
+    std::mutex failure_lock;
+    const auto run = [&](std::size_t p) noexcept {
+        try {
+            chunks[p] = place_vertices(mesh, translation, *transform, rotation, out, nv * p / parts,
+                                       nv * (p + 1) / parts);
+        }
+        catch (...) {
+            const std::lock_guard<std::mutex> hold(failure_lock);
+            failure = std::current_exception();
+        }
+    };
+    {
+        std::vector<std::thread> workers;
+        struct JoinAll {
+            std::vector<std::thread>& threads;
+            ~JoinAll()
+            {
+                for (auto& t : threads) {
+                    if (t.joinable()) {
+                        t.join();
+                    }
+                }
+            }
+        } join { workers };
+        for (std::size_t p = 1; p < parts; ++p) {
+            try {
+                workers.emplace_back(run, p);
+            }
+            catch (...) {
+                run(p);  // no thread to be had: this one does the chunk
+            }
+        }
+        run(0);
+    }
+    if (failure) {
+        std::rethrow_exception(failure);
+    }
     out.world_exact = out.is_cardinal;
     bool first = true;
-    for (std::size_t i = 0; i < nv; ++i) {
+    for (const auto& c : chunks) {
+        if (!c.valid) {
+            return false;
+        }
+        out.world_exact = out.world_exact && c.world_exact;
+        if (!c.any) {
+            continue;
+        }
         for (int a = 0; a < 3; ++a) {
-            double w = translation[a];
-            for (int s = 0; s < 3; ++s) {
-                w += transform->matrix[a][s] * mesh.vertices[i][s];
-            }
-            out.world[i][a] = w;
-            const Interval iv = transformed_interval(mesh.vertices[i], translation, rotation, a);
-            out.intervals[i].v[a] = iv;
-            if (!iv.valid) {
-                return false;
-            }
-            if (out.is_cardinal) {
-                const int source = out.source_axis[a];
-                const double ta = translation[a];
-                const double b = out.sign[a] * mesh.vertices[i][source];
-                const double sum = ta + b;
-                out.world[i][a] = sum;
-                out.world_exact = out.world_exact && compare_coordinates({ ta, mesh.vertices[i][source], out.sign[a] },
-                                                                         { 0.0, sum, 1 }) == exact::Sign::zero;
-            }
             if (first) {
-                out.conservative.min[a] = iv.low;
-                out.conservative.max[a] = iv.high;
+                out.conservative.min[a] = c.conservative.min[a];
+                out.conservative.max[a] = c.conservative.max[a];
             }
             else {
-                out.conservative.min[a] = std::min(out.conservative.min[a], iv.low);
-                out.conservative.max[a] = std::max(out.conservative.max[a], iv.high);
+                out.conservative.min[a] = std::min(out.conservative.min[a], c.conservative.min[a]);
+                out.conservative.max[a] = std::max(out.conservative.max[a], c.conservative.max[a]);
             }
         }
         first = false;
