@@ -587,14 +587,63 @@ VertexChunk place_vertices(const Mesh& mesh, const Vec3& translation, const Rota
     return c;
 }
 
-// Chunks for n vertices: one below 2048, else up to four of at least 1024.
-std::size_t vertex_parts(std::size_t n)
+// Chunks for n independent items: one below 2048, else up to four of at
+// least 1024.
+std::size_t chunk_count(std::size_t n)
 {
     if (n < 2048) {
         return 1;
     }
     const std::size_t cores = std::max(1U, std::thread::hardware_concurrency());
     return std::min({ std::size_t { 4 }, cores, n / 1024 });
+}
+
+// Runs body(p, begin, end) on the `parts` contiguous chunks of [0, n): chunk 0
+// on the calling thread, each other one on a thread of its own, or on the
+// calling thread when no thread can be had.  Returns after every chunk is
+// done, rethrowing the first exception a chunk raised.
+template <class Body>
+void run_chunks(std::size_t n, std::size_t parts, const Body& body)
+{
+    std::exception_ptr failure;
+    std::mutex failure_lock;
+    const auto run = [&](std::size_t p) noexcept {
+        try {
+            body(p, n * p / parts, n * (p + 1) / parts);
+        }
+        catch (...) {
+            const std::lock_guard<std::mutex> hold(failure_lock);
+            if (!failure) {
+                failure = std::current_exception();
+            }
+        }
+    };
+    {
+        std::vector<std::thread> workers;
+        struct JoinAll {
+            std::vector<std::thread>& threads;
+            ~JoinAll()
+            {
+                for (auto& t : threads) {
+                    if (t.joinable()) {
+                        t.join();
+                    }
+                }
+            }
+        } join { workers };
+        for (std::size_t p = 1; p < parts; ++p) {
+            try {
+                workers.emplace_back(run, p);
+            }
+            catch (...) {
+                run(p);
+            }
+        }
+        run(0);
+    }
+    if (failure) {
+        std::rethrow_exception(failure);
+    }
 }
 
 }  // namespace
@@ -656,46 +705,11 @@ bool place(const Prepared& prepared, const Vec3& translation, const Quat& q, Pla
     // threads, and their bounds combine in vertex order.  std::min / std::max
     // keep the earlier of equal values, so the combined bounds are the ones a
     // single pass over all vertices gives.
-    const std::size_t parts = vertex_parts(nv);
+    const std::size_t parts = chunk_count(nv);
     std::vector<VertexChunk> chunks(parts);
-    std::exception_ptr failure;
-    std::mutex failure_lock;
-    const auto run = [&](std::size_t p) noexcept {
-        try {
-            chunks[p] = place_vertices(mesh, translation, *transform, rotation, out, nv * p / parts,
-                                       nv * (p + 1) / parts);
-        }
-        catch (...) {
-            const std::lock_guard<std::mutex> hold(failure_lock);
-            failure = std::current_exception();
-        }
-    };
-    {
-        std::vector<std::thread> workers;
-        struct JoinAll {
-            std::vector<std::thread>& threads;
-            ~JoinAll()
-            {
-                for (auto& t : threads) {
-                    if (t.joinable()) {
-                        t.join();
-                    }
-                }
-            }
-        } join { workers };
-        for (std::size_t p = 1; p < parts; ++p) {
-            try {
-                workers.emplace_back(run, p);
-            }
-            catch (...) {
-                run(p);  // no thread to be had: this one does the chunk
-            }
-        }
-        run(0);
-    }
-    if (failure) {
-        std::rethrow_exception(failure);
-    }
+    run_chunks(nv, parts, [&](std::size_t p, std::size_t begin, std::size_t end) {
+        chunks[p] = place_vertices(mesh, translation, *transform, rotation, out, begin, end);
+    });
     out.world_exact = out.is_cardinal;
     bool first = true;
     for (const auto& c : chunks) {
@@ -896,31 +910,39 @@ bool face_ranges(const Placed& placed, const Window& window, const double* origi
     for (int a = 0; a < 3; ++a) {
         window_last[a] = window.first[a] + static_cast<std::int64_t>(window.shape[a] - 1);
     }
-    for (std::size_t f = 0; f < mesh.triangles.size(); ++f) {
-        const auto& face = mesh.triangles[f];
-        auto& r = out[f];
-        r.outside = 0;
-        r.pad = 0;
-        for (int a = 0; a < 3; ++a) {
-            double low = placed.intervals[face[0]].v[a].low, high = placed.intervals[face[0]].v[a].high;
-            for (int k = 1; k < 3; ++k) {
-                low = std::min(low, placed.intervals[face[k]].v[a].low);
-                high = std::max(high, placed.intervals[face[k]].v[a].high);
+    // Faces are independent: contiguous chunks on up to four host threads.
+    const std::size_t faces = mesh.triangles.size();
+    const std::size_t parts = chunk_count(faces);
+    std::vector<char> ok(parts, 1);
+    run_chunks(faces, parts, [&](std::size_t p, std::size_t begin, std::size_t end) {
+        for (std::size_t f = begin; f < end; ++f) {
+            const auto& face = mesh.triangles[f];
+            auto& r = out[f];
+            r.outside = 0;
+            r.pad = 0;
+            for (int a = 0; a < 3; ++a) {
+                double low = placed.intervals[face[0]].v[a].low, high = placed.intervals[face[0]].v[a].high;
+                for (int k = 1; k < 3; ++k) {
+                    low = std::min(low, placed.intervals[face[k]].v[a].low);
+                    high = std::max(high, placed.intervals[face[k]].v[a].high);
+                }
+                std::int64_t lo, hi;
+                if (!quotient_floor(low, origin[a], pitch, true, lo) ||
+                    !quotient_floor(high, origin[a], pitch, false, hi)) {
+                    ok[p] = 0;
+                    return;
+                }
+                r.first[a] = lo - 1;
+                r.last[a] = hi + 1;
+                if (r.last[a] < window.first[a] || r.first[a] > window_last[a]) {
+                    r.outside = 1;
+                }
+                r.first[a] = std::max(r.first[a], window.first[a]);
+                r.last[a] = std::min(r.last[a], window_last[a]);
             }
-            std::int64_t lo, hi;
-            if (!quotient_floor(low, origin[a], pitch, true, lo) || !quotient_floor(high, origin[a], pitch, false, hi)) {
-                return false;
-            }
-            r.first[a] = lo - 1;
-            r.last[a] = hi + 1;
-            if (r.last[a] < window.first[a] || r.first[a] > window_last[a]) {
-                r.outside = 1;
-            }
-            r.first[a] = std::max(r.first[a], window.first[a]);
-            r.last[a] = std::min(r.last[a], window_last[a]);
         }
-    }
-    return true;
+    });
+    return std::all_of(ok.begin(), ok.end(), [](char v) { return v != 0; });
 }
 
 Decision classify_material_witness(const Placed& solid, const Bounds& wi)
