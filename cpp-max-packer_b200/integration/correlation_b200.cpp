@@ -17,6 +17,7 @@
 #include <atomic>
 #include <chrono>
 #include <limits>
+#include <new>
 #include <stop_token>
 #include <string_view>
 #include <vector>
@@ -26,38 +27,24 @@
 namespace spectrapack::compute {
 namespace {
 
-// Messages of the reference's failures (correlation.cpp), by code.
-std::string_view message_of(std::string_view code) noexcept
+// The reference's metadata admission (correlation.cpp:67-72,255-259): the
+// call's own outcome, values vector and control, before anything else.
+constexpr std::uint64_t kMetadataBytes =
+    2 * sizeof(CorrelationOutcome) + sizeof(std::vector<double>) + sizeof(runtime::OperationControl);
+
+CorrelationFailure failure(std::string_view code, std::string_view message, CorrelationStats stats = {}) noexcept
 {
-    struct Entry {
-        std::string_view code, message;
-    };
-    static constexpr Entry table[] = {
-        { "CORRELATION_SHAPE_OVERFLOW", "Correlation extents must be positive and representable." },
-        { "CORRELATION_INDEX_OVERFLOW", "The first output translation is not representable." },
-        { "CORRELATION_INVALID_FIELD", "Shape does not match supplied cells." },
-        { "CORRELATION_INVALID_ENVIRONMENT", "Environment cells must be finite values in [0,1]." },
-        { "CORRELATION_INVALID_KERNEL", "Kernel cells must be binary." },
-        { "CORRELATION_NUMERIC_RANGE", "Correlation mass is not exactly representable." },
-        { "CORRELATION_PADDED_CELL_LIMIT", "Padded field exceeds its cell limit." },
-        { "CORRELATION_MEMORY_LIMIT", "Correlation buffers exceed their memory limit." },
-        { "CORRELATION_NUMERIC", "FFT output failed a numeric check." },
-        { "CORRELATION_DIRECT_TERM_LIMIT", "Deterministic direct checks exhausted their work limit." },
-        { "CORRELATION_ALLOCATION", "Correlation allocation failed." },
-        { "OPERATION_CANCELLED", "Correlation interrupted." },
-        { "DEADLINE_EXCEEDED", "Correlation interrupted." },
-    };
-    for (const auto& e : table) {
-        if (e.code == code) {
-            return e.message;
-        }
-    }
-    return code;
+    return CorrelationFailure { code, message, stats };
 }
 
-CorrelationFailure failure(std::string_view code, CorrelationStats stats = {}) noexcept
+std::optional<CorrelationFailure> metadata_limit(const CorrelationLimits& limits) noexcept
 {
-    return CorrelationFailure { code, message_of(code), stats };
+    std::uint64_t metadata {};
+    if (__builtin_add_overflow(limits.reserved_bytes, kMetadataBytes, &metadata) ||
+        metadata > limits.max_working_bytes) {
+        return failure("CORRELATION_MEMORY_LIMIT", "Correlation metadata exceeds its memory limit.");
+    }
+    return std::nullopt;
 }
 
 // One context per process on device 0, created on first use.  Calls are
@@ -115,41 +102,58 @@ std::optional<CorrelationFailure> interrupted(const runtime::OperationControl& c
 {
     switch (control.poll()) {
     case runtime::StopCause::user_stopped:
-        return failure("OPERATION_CANCELLED");
+        return failure("OPERATION_CANCELLED", "Correlation interrupted.");
     case runtime::StopCause::deadline:
-        return failure("DEADLINE_EXCEEDED");
+        return failure("DEADLINE_EXCEEDED", "Correlation interrupted.");
     default:
         return std::nullopt;
     }
 }
 
-// The reference's spec and field checks, in its order (correlation.cpp:
-// 276-312): extents, translation range, then the supplied cell counts.  The
-// library repeats the first two; the cell counts only the caller's spans hold.
+// The reference's spec and field checks, in its order and with its message
+// per site (correlation.cpp:276-314): per axis the extents, the padded
+// length, the first and the last translation; then the storage size and the
+// supplied cell counts.  The library repeats the axis checks; the cell counts
+// only the caller's spans hold.
 std::optional<CorrelationFailure> check_fields(const CorrelationSpec& spec, std::size_t environment_size,
                                                std::size_t kernel_size, std::uint64_t& output_count) noexcept
 {
     std::uint64_t env_cells = 1, ker_cells = 1, count = 1;
     for (int a = 0; a < 3; ++a) {
         const std::uint64_t e = spec.environment_shape[a], k = spec.kernel_shape[a];
-        const std::uint64_t length = e + k - 1;
         if (!e || !k || __builtin_mul_overflow(env_cells, e, &env_cells) ||
-            __builtin_mul_overflow(ker_cells, k, &ker_cells) || length > std::numeric_limits<std::uint32_t>::max() ||
-            __builtin_mul_overflow(count, length, &count)) {
-            return failure("CORRELATION_SHAPE_OVERFLOW");
+            __builtin_mul_overflow(ker_cells, k, &ker_cells)) {
+            return failure("CORRELATION_SHAPE_OVERFLOW", "Correlation extents must be positive and representable.");
+        }
+        const std::uint64_t length = e + k - 1;
+        if (length > std::numeric_limits<std::uint32_t>::max() || __builtin_mul_overflow(count, length, &count)) {
+            return failure("CORRELATION_SHAPE_OVERFLOW", "Padded correlation shape overflowed.");
         }
         std::int64_t difference {}, first {}, last {};
         if (__builtin_sub_overflow(spec.environment_first[a], spec.kernel_first[a], &difference) ||
-            __builtin_sub_overflow(difference, static_cast<std::int64_t>(k) - 1, &first) ||
-            __builtin_add_overflow(first, static_cast<std::int64_t>(length) - 1, &last)) {
-            return failure("CORRELATION_INDEX_OVERFLOW");
+            __builtin_sub_overflow(difference, static_cast<std::int64_t>(k) - 1, &first)) {
+            return failure("CORRELATION_INDEX_OVERFLOW", "The first output translation is not representable.");
+        }
+        if (__builtin_add_overflow(first, static_cast<std::int64_t>(length) - 1, &last)) {
+            return failure("CORRELATION_INDEX_OVERFLOW", "The last output translation is not representable.");
         }
     }
+    if (env_cells > std::numeric_limits<std::size_t>::max() || ker_cells > std::numeric_limits<std::size_t>::max() ||
+        count > std::numeric_limits<std::size_t>::max()) {
+        return failure("CORRELATION_SHAPE_OVERFLOW", "Correlation storage size is not representable.");
+    }
     if (environment_size != env_cells || kernel_size != ker_cells) {
-        return failure("CORRELATION_INVALID_FIELD");
+        return failure("CORRELATION_INVALID_FIELD", "Shape does not match supplied cells.");
     }
     output_count = count;
     return std::nullopt;
+}
+
+// A library failure as the reference's value: its code, and the message the
+// library recorded for the failing site.
+CorrelationFailure library_failure(spk_context* context, int status, CorrelationStats stats) noexcept
+{
+    return failure(spk_status_code(status), spk_context_message(context), stats);
 }
 
 spk_correlation_spec to_spk(const CorrelationSpec& s) noexcept
@@ -180,6 +184,9 @@ CorrelationOutcome run(const CorrelationSpec& spec, std::span<const Env> environ
                        const runtime::OperationControl& control, Call call) noexcept
 {
     try {
+        if (auto limit = metadata_limit(limits)) {
+            return *limit;
+        }
         if (auto stop = interrupted(control)) {
             return *stop;
         }
@@ -189,7 +196,7 @@ CorrelationOutcome run(const CorrelationSpec& spec, std::span<const Env> environ
         }
         spk_context* context = device_context();
         if (!context) {
-            return failure("CORRELATION_ALLOCATION");
+            return failure("CORRELATION_ALLOCATION", "Correlation allocation failed.");
         }
         std::vector<double> values(count);
         const spk_correlation_spec s = to_spk(spec);
@@ -199,7 +206,7 @@ CorrelationOutcome run(const CorrelationSpec& spec, std::span<const Env> environ
         const int status = call(context, &s, environment.data(), kernel.data(), &l, bridge.get(), SPK_FP64,
                                 values.data(), count, &r);
         if (status != 0) {
-            return failure(spk_status_code(status), stats_of(r));
+            return library_failure(context, status, stats_of(r));
         }
         return CorrelationResult { { r.translation_first[0], r.translation_first[1], r.translation_first[2] },
                                    { r.shape[0], r.shape[1], r.shape[2] },
@@ -207,8 +214,11 @@ CorrelationOutcome run(const CorrelationSpec& spec, std::span<const Env> environ
                                    { r.max_integer_residual, r.mass_residual, r.max_probe_error },
                                    stats_of(r) };
     }
+    catch (const std::bad_alloc&) {
+        return failure("CORRELATION_ALLOCATION", "Correlation allocation failed.");
+    }
     catch (...) {
-        return failure("CORRELATION_ALLOCATION");
+        return failure("CORRELATION_OPERATION", "Correlation operation failed.");
     }
 }
 
@@ -237,6 +247,9 @@ std::optional<CorrelationFailure> correlate_binary_mask_b200(const CorrelationSp
                                                              const runtime::OperationControl& control) noexcept
 {
     try {
+        if (auto limit = metadata_limit(limits)) {
+            return limit;
+        }
         if (auto stop = interrupted(control)) {
             return stop;
         }
@@ -246,7 +259,7 @@ std::optional<CorrelationFailure> correlate_binary_mask_b200(const CorrelationSp
         }
         spk_context* context = device_context();
         if (!context) {
-            return failure("CORRELATION_ALLOCATION");
+            return failure("CORRELATION_ALLOCATION", "Correlation allocation failed.");
         }
         const spk_correlation_spec s = to_spk(spec);
         const spk_correlation_limits l = to_spk(limits);
@@ -257,12 +270,15 @@ std::optional<CorrelationFailure> correlate_binary_mask_b200(const CorrelationSp
             box.shape.data(), rule == MaskRule::zero_count ? SPK_MASK_ZERO : SPK_MASK_NONZERO, mask.data(),
             mask.size(), &r);
         if (status != 0) {
-            return failure(spk_status_code(status), stats_of(r));
+            return library_failure(context, status, stats_of(r));
         }
         return std::nullopt;
     }
+    catch (const std::bad_alloc&) {
+        return failure("CORRELATION_ALLOCATION", "Correlation allocation failed.");
+    }
     catch (...) {
-        return failure("CORRELATION_ALLOCATION");
+        return failure("CORRELATION_OPERATION", "Correlation operation failed.");
     }
 }
 

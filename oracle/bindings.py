@@ -17,8 +17,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libspk_ref.so")
-# Where the reference checkout lies when it is present (build recipes only).
-REFERENCE_ROOT = "/root/reference"
+# The reference checkout, when present, is found by oracle/ref/Makefile
+# (SPK_REFERENCE_ROOT, or the recipe's default); without it the prebuilt
+# oracle/_ref library is used as it is.
 
 _c = ctypes
 _P = ctypes.c_void_p
@@ -36,12 +37,12 @@ def build_oracle() -> str:
     return ORACLE_SO
 
 
-def build_reference(reference_root: str = REFERENCE_ROOT) -> str | None:
-    """Compiles the reference's hot-path sources in place (oracle/ref/Makefile)."""
-    if not os.path.isdir(reference_root):
-        return REF_SO if os.path.exists(REF_SO) else None
-    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), f"REF={reference_root}"], check=True)
-    return REF_SO
+def build_reference(reference_root: str | None = None) -> str | None:
+    """Compiles the reference's hot-path sources in place (oracle/ref/Makefile;
+    a no-op where the sources are absent)."""
+    extra = [f"REF={reference_root}"] if reference_root else []
+    subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "ref"), *extra], check=True)
+    return REF_SO if os.path.exists(REF_SO) else None
 
 
 class C:

@@ -60,7 +60,11 @@ void compare(const char* name, const compute::CorrelationOutcome& ours, const co
         return;
     }
     if (a != "OK") {
-        report(name, true, a);
+        // Same code: the message must be the reference's for the same site.
+        const auto& fa = std::get<compute::CorrelationFailure>(ours);
+        const auto& fb = std::get<compute::CorrelationFailure>(ref);
+        report(name, fa.message == fb.message,
+               a + " '" + std::string(fa.message) + "' vs '" + std::string(fb.message) + "'");
         return;
     }
     const auto& x = std::get<compute::CorrelationResult>(ours);
@@ -134,6 +138,29 @@ int main()
     const compute::CorrelationSpec far { { 7, 5, 4 }, { 3, 2, 2 }, { INT64_MIN + 1, 0, 0 }, { 5, 0, 0 } };
     compare("index_overflow", compute::correlate_binary_b200(far, env, ker),
             compute::correlate_binary_cpu(far, env, ker), false);
+
+    // A stopped control with no working bytes at all: the metadata limit is
+    // checked before the stop (correlation.cpp:255-275).
+    compute::CorrelationLimits none;
+    none.max_working_bytes = 0;
+    compare("stopped_no_memory", compute::correlate_binary_b200(spec, env, ker, none, stopped),
+            compute::correlate_binary_cpu(spec, env, ker, none, stopped), false);
+
+    // The first translation fits, the last does not.
+    const compute::CorrelationSpec edge { { 7, 5, 4 }, { 3, 2, 2 }, { INT64_MAX - 4, 0, 0 }, { 0, 0, 0 } };
+    compare("last_translation", compute::correlate_binary_b200(edge, env, ker),
+            compute::correlate_binary_cpu(edge, env, ker), false);
+
+    std::vector<double> bad_prox = prox;
+    bad_prox[3] = 1.5;
+    compare("invalid_environment", compute::correlate_proximity_b200(spec, bad_prox, ker),
+            compute::correlate_proximity_cpu(spec, bad_prox, ker), true);
+
+    // Padded cells over the caller's limit, reached in the library.
+    compute::CorrelationLimits few;
+    few.max_padded_cells = 10;
+    compare("padded_limit", compute::correlate_binary_b200(spec, env, ker, few),
+            compute::correlate_binary_cpu(spec, env, ker, few), false);
 
     std::vector<std::uint8_t> bad_kernel = ker;
     bad_kernel[1] = 2;
