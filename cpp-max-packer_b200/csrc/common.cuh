@@ -40,6 +40,7 @@ enum Status : int {
     kKernelWait = 24,          // SPK_DEVICE_WAIT_LIMIT (bounded device wait expired)
     kScratchLimit = 25,        // SPK_SCRATCH_LIMIT
     kNotReady = 26,            // SPK_CONTEXT_STATE
+    kValidationAborted = 27,   // SPECTRAL_VALIDATION_ABORTED
 };
 
 template <typename T>

@@ -103,6 +103,11 @@ int spk_context_pass_times(const spk_context* ctx, uint64_t* launches, double* t
     return spk::kOk;
 }
 
+const char* spk_context_message(const spk_context* ctx)
+{
+    return ctx && ctx->message ? ctx->message : "";
+}
+
 const char* spk_status_code(int status)
 {
     switch (status) {
@@ -133,6 +138,7 @@ const char* spk_status_code(int status)
     case spk::kKernelWait: return "SPK_DEVICE_WAIT_LIMIT";
     case spk::kScratchLimit: return "SPK_SCRATCH_LIMIT";
     case spk::kNotReady: return "SPK_CONTEXT_STATE";
+    case spk::kValidationAborted: return "SPECTRAL_VALIDATION_ABORTED";
     default: return "SPK_UNKNOWN_STATUS";
     }
 }

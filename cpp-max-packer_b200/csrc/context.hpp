@@ -36,6 +36,7 @@ struct spk_context {
     double pass_ms[4] {};
     double pass_bytes[4] {};  // algorithmic bytes of the profiled launches
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;  // (pass, events)
+    const char* message { "" };  // static text of the last correlation failure on this context
 };
 
 namespace spk {
@@ -129,6 +130,31 @@ const cplx_t<T>* twiddle_table(spk_context* ctx, int L, int& status)
 }
 
 std::int64_t monotonic_ns();
+
+// Records the reference's message for a failure site and returns its status.
+inline int fail(spk_context* ctx, int status, const char* message)
+{
+    ctx->message = message;
+    return status;
+}
+
+// A failing status whose site left no message gets the reference's wording
+// for its code (correlation.cpp:268-270,587) or the library's own.
+inline int finish(spk_context* ctx, int status)
+{
+    if (status && ctx && !*ctx->message) {
+        switch (status) {
+        case kCancelled:
+        case kDeadline: ctx->message = "Correlation interrupted."; break;
+        case kAllocation: ctx->message = "Correlation allocation failed."; break;
+        case kMemoryLimit: ctx->message = "Correlation buffers and FFT workspace exceed their memory limit."; break;
+        case kCuda: ctx->message = "CUDA runtime call failed."; break;
+        case kInvalidArgument: ctx->message = "Invalid argument."; break;
+        default: break;
+        }
+    }
+    return status;
+}
 
 // The reference polls stop first, then the deadline (operation_control.hpp:33-42).
 inline int poll(const spk_control* control)

@@ -135,7 +135,8 @@ template <typename T>
 __global__ void extract_kernel(const cplx_t<T>* __restrict__ w, Grid g, int ox, int oy, int oz, int kx, int ky,
                                int kz, int binary, double maximum_output, double imag_tolerance,
                                double range_tolerance, double* __restrict__ out, ExtractStats* __restrict__ stats,
-                               unsigned long long* __restrict__ max_residual_bits, int* __restrict__ failed)
+                               unsigned long long* __restrict__ max_residual_bits,
+                               unsigned long long* __restrict__ first_failure)
 {
     __shared__ double s_mass[256];
     __shared__ double s_abs[256];
@@ -143,7 +144,10 @@ __global__ void extract_kernel(const cplx_t<T>* __restrict__ w, Grid g, int ox, 
     const long long n = static_cast<long long>(ox) * oy * oz;
     double mass = 0.0, best = -1.0, residual_max = 0.0;
     long long best_i = 0;
-    bool bad = false;
+    // Lowest failing output index per kind: [0] non-finite or non-real,
+    // [1] integer or range.  The reference scans outputs in index order and
+    // reports the first cell that fails, checking non-real before range.
+    unsigned long long bad_real = ~0ULL, bad_range = ~0ULL;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
         const int x = static_cast<int>(i % ox);
@@ -157,7 +161,7 @@ __global__ void extract_kernel(const cplx_t<T>* __restrict__ w, Grid g, int ox, 
         const double value = static_cast<double>(v.x);
         const double imag = static_cast<double>(v.y);
         if (!isfinite(value) || !isfinite(imag) || fabs(imag) >= imag_tolerance) {
-            bad = true;
+            bad_real = min(bad_real, static_cast<unsigned long long>(i));
         }
         mass += value;
         if (fabs(value) > best) {
@@ -169,19 +173,22 @@ __global__ void extract_kernel(const cplx_t<T>* __restrict__ w, Grid g, int ox, 
             const double residual = fabs(value - rounded);
             residual_max = fmax(residual_max, residual);
             if (residual >= 0.25 || rounded < 0.0 || rounded > maximum_output) {
-                bad = true;
+                bad_range = min(bad_range, static_cast<unsigned long long>(i));
             }
             out[i] = rounded;
         }
         else {
             if (value < -range_tolerance || value > maximum_output + range_tolerance) {
-                bad = true;
+                bad_range = min(bad_range, static_cast<unsigned long long>(i));
             }
             out[i] = value;
         }
     }
-    if (bad) {
-        atomicOr(failed, 1);
+    if (bad_real != ~0ULL) {
+        atomicMin(&first_failure[0], bad_real);
+    }
+    if (bad_range != ~0ULL) {
+        atomicMin(&first_failure[1], bad_range);
     }
     if (binary) {
         atomicMax(max_residual_bits, static_cast<unsigned long long>(__double_as_longlong(residual_max)));
@@ -353,8 +360,15 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         limits = *limits_ptr;
     }
     std::memset(result, 0, sizeof(*result));
+    ctx->message = "";
+    // The reference admits its own call metadata before anything else
+    // (correlation.cpp:255-259); here that is the result record.
+    if (limits.reserved_bytes > limits.max_working_bytes ||
+        limits.max_working_bytes - limits.reserved_bytes < sizeof(spk_correlation_result)) {
+        return fail(ctx, kMemoryLimit, "Correlation metadata exceeds its memory limit.");
+    }
     if (int s = poll(control)) {
-        return s;
+        return fail(ctx, s, "Correlation interrupted.");
     }
     std::uint64_t env_count = 1, ker_count = 1, padded_count = 1;
     std::uint32_t padded[3];
@@ -362,25 +376,25 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         if (spec.environment_shape[a] == 0 || spec.kernel_shape[a] == 0 ||
             !checked_mul(env_count, spec.environment_shape[a], env_count) ||
             !checked_mul(ker_count, spec.kernel_shape[a], ker_count)) {
-            return kShapeOverflow;
+            return fail(ctx, kShapeOverflow, "Correlation extents must be positive and representable.");
         }
         const std::uint64_t length = std::uint64_t { spec.environment_shape[a] } + spec.kernel_shape[a] - 1;
         if (length > UINT32_MAX || !checked_mul(padded_count, length, padded_count)) {
-            return kShapeOverflow;
+            return fail(ctx, kShapeOverflow, "Padded correlation shape overflowed.");
         }
         padded[a] = static_cast<std::uint32_t>(length);
         const std::int64_t ef = spec.environment_first[a], kf = spec.kernel_first[a];
         if ((kf > 0 && ef < INT64_MIN + kf) || (kf < 0 && ef > INT64_MAX + kf)) {
-            return kIndexOverflow;
+            return fail(ctx, kIndexOverflow, "The first output translation is not representable.");
         }
         const std::int64_t diff = ef - kf;
         const std::int64_t k1 = static_cast<std::int64_t>(spec.kernel_shape[a]) - 1;
         if (diff < INT64_MIN + k1) {
-            return kIndexOverflow;
+            return fail(ctx, kIndexOverflow, "The first output translation is not representable.");
         }
         result->translation_first[a] = diff - k1;
         if (result->translation_first[a] > INT64_MAX - static_cast<std::int64_t>(length - 1)) {
-            return kIndexOverflow;
+            return fail(ctx, kIndexOverflow, "The last output translation is not representable.");
         }
         result->shape[a] = padded[a];
     }
@@ -390,7 +404,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     for (std::uint64_t i = 0; i != env_count; ++i) {
         const double value = static_cast<double>(environment[i]);
         if (!std::isfinite(value) || value < 0.0 || value > 1.0) {
-            return kInvalidEnvironment;
+            return fail(ctx, kInvalidEnvironment, "Environment cells must be finite values in [0,1].");
         }
         if constexpr (binary) {
             env_ones += environment[i];
@@ -401,7 +415,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     }
     for (std::uint64_t i = 0; i != ker_count; ++i) {
         if (kernel[i] > 1) {
-            return kInvalidKernel;
+            return fail(ctx, kInvalidKernel, "Kernel cells must be binary.");
         }
         ker_ones += kernel[i];
     }
@@ -409,7 +423,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     if constexpr (binary) {
         std::uint64_t product;
         if (!checked_mul(env_ones, ker_ones, product) || product > kExactInteger) {
-            return kNumericRange;
+            return fail(ctx, kNumericRange, "Binary correlation mass is not exactly representable.");
         }
         environment_mass = static_cast<double>(env_ones);
         expected_mass = static_cast<double>(product);
@@ -418,18 +432,18 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         environment_mass = env_mass_sum.value;
         expected_mass = environment_mass * static_cast<double>(ker_ones);
         if (!std::isfinite(environment_mass) || !std::isfinite(expected_mass)) {
-            return kNumericRange;
+            return fail(ctx, kNumericRange, "Proximity correlation mass is not representable.");
         }
     }
     result->padded_cells = padded_count;
     if (padded_count > limits.max_padded_cells) {
-        return kPaddedCellLimit;
+        return fail(ctx, kPaddedCellLimit, "Padded field exceeds its cell limit.");
     }
     Grid g;
     for (int a = 0; a != 3; ++a) {
         const std::uint32_t L = next_pow2(padded[a]);
         if (L > static_cast<std::uint32_t>(kMaxFftLength)) {
-            return kUnsupportedLength;
+            return fail(ctx, kUnsupportedLength, "Padded extent exceeds the device FFT's longest axis.");
         }
         g.L[a] = static_cast<int>(L);
         result->padded_shape[a] = L;
@@ -445,7 +459,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         mask_count = 1;
         for (int a = 0; a != 3; ++a) {
             if (!checked_mul(mask_count, mask_request->shape[a], mask_count)) {
-                return kShapeOverflow;
+                return fail(ctx, kShapeOverflow, "Mask box size is not representable.");
             }
         }
     }
@@ -453,7 +467,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
                                   env_count * sizeof(E) + ker_count + extract_blocks * sizeof(ExtractStats) + 64 +
                                   mask_count;
     if (working > limits.max_working_bytes) {
-        return kMemoryLimit;
+        return fail(ctx, kMemoryLimit, "Correlation buffers and FFT workspace exceed their memory limit.");
     }
     result->working_bytes_peak = working;
     if (mask_request ? (mask_request->capacity < mask_count || (mask_count && !mask_request->mask))
@@ -467,7 +481,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     auto* d_ker = static_cast<std::uint8_t*>(device_buffer(ctx, "corr.ker", ker_count, status));
     auto* d_out = static_cast<double*>(device_buffer(ctx, "corr.out", out_bytes, status));
     auto* d_stats = static_cast<ExtractStats*>(
-        device_buffer(ctx, "corr.stats", extract_blocks * sizeof(ExtractStats) + 16, status));
+        device_buffer(ctx, "corr.stats", extract_blocks * sizeof(ExtractStats) + 32, status));
     if (!z || !w || !d_env || !d_ker || !d_out || !d_stats) {
         return status;
     }
@@ -477,6 +491,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     cudaMemcpyAsync(d_env, environment, env_count * sizeof(E), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_ker, kernel, ker_count, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_flags, 0, 16, st);
+    cudaMemsetAsync(d_flags + 2, 0xff, 16, st);
     const int threads = 256;
     pack_kernel<T, E><<<grid_blocks(g.n(), threads), threads, 0, st>>>(
         z, g, d_env, spec.environment_shape[0], spec.environment_shape[1], spec.environment_shape[2], d_ker,
@@ -523,8 +538,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     const double imag_tolerance = binary ? 0.25 : proximity_tolerance;
     extract_kernel<T><<<extract_blocks, extract_threads, 0, st>>>(
         w, g, padded[0], padded[1], padded[2], spec.kernel_shape[0], spec.kernel_shape[1], spec.kernel_shape[2],
-        binary ? 1 : 0, maximum_output, imag_tolerance, proximity_tolerance, d_out, d_stats, d_flags,
-        reinterpret_cast<int*>(d_flags + 1));
+        binary ? 1 : 0, maximum_output, imag_tolerance, proximity_tolerance, d_out, d_stats, d_flags, d_flags + 2);
     ctx->launches++;
     if (mask_request && mask_count) {
         // Box offset from the range's first translation, per axis.  A box
@@ -549,18 +563,22 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         cudaMemcpyAsync(mask_request->mask, d_mask, mask_count, cudaMemcpyDeviceToHost, st);
     }
     std::vector<ExtractStats> stats(extract_blocks);
-    unsigned long long flags[2] {};
+    unsigned long long flags[4] {};
     if (!mask_request) {
         cudaMemcpyAsync(out_values, d_out, out_bytes, cudaMemcpyDeviceToHost, st);
     }
     cudaMemcpyAsync(stats.data(), d_stats, extract_blocks * sizeof(ExtractStats), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(flags, d_flags, 16, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(flags, d_flags, 32, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         cudaGetLastError();
         return kCuda;
     }
-    if (flags[1]) {
-        return kNumeric;
+    if (flags[2] != ~0ULL || flags[3] != ~0ULL) {
+        if (flags[2] <= flags[3]) {
+            return fail(ctx, kNumeric, "FFT produced a nonfinite or non-real value.");
+        }
+        return fail(ctx, kNumeric, binary ? "Binary FFT output failed its integer or range check."
+                                          : "Proximity FFT output failed its range check.");
     }
     double max_residual = 0;
     std::memcpy(&max_residual, &flags[0], 8);
@@ -577,7 +595,7 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     const double mass_residual = std::fabs(output_mass.value - expected_mass);
     const double mass_tolerance = binary ? 0.25 : rel * std::max(1.0, std::fabs(expected_mass));
     if (!std::isfinite(mass_residual) || (binary ? mass_residual >= mass_tolerance : mass_residual > mass_tolerance)) {
-        return kNumeric;
+        return fail(ctx, kNumeric, "FFT output failed its total-mass check.");
     }
     // Deterministic direct checks (correlation.cpp:549-577).
     std::uint64_t probes[8];
@@ -619,9 +637,9 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
         if (!direct_probe(spec, environment, kernel, padded, probes[p], limits.max_direct_terms, terms, expected)) {
             result->direct_terms = terms;
             if (int s = poll(control)) {
-                return s;
+                return fail(ctx, s, "Correlation interrupted.");
             }
-            return kDirectTermLimit;
+            return fail(ctx, kDirectTermLimit, "Deterministic direct checks exhausted their work limit.");
         }
         const double error = std::fabs((mask_request ? probe_values[p] : out_values[probes[p]]) - expected);
         max_probe_error = std::max(max_probe_error, error);
@@ -631,14 +649,17 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
             binary ? 0.25 : rel * std::max(1.0, sizeof(T) == 8 ? std::fabs(expected) : maximum_output);
         if (!std::isfinite(error) || (binary ? error >= tolerance : error > tolerance)) {
             result->direct_terms = terms;
-            return kNumeric;
+            return fail(ctx, kNumeric, "FFT output failed a deterministic direct check.");
         }
     }
     result->direct_terms = terms;
     result->max_integer_residual = max_residual;
     result->mass_residual = mass_residual;
     result->max_probe_error = max_probe_error;
-    return poll(control);
+    if (int s = poll(control)) {
+        return fail(ctx, s, "Correlation interrupted.");
+    }
+    return kOk;
 }
 
 }  // namespace
@@ -679,20 +700,24 @@ int spk_correlate_binary(spk_context* ctx, const spk_correlation_spec* spec, con
                          uint32_t precision, double* out_values, uint64_t out_capacity, spk_correlation_result* result)
 {
     try {
+        if (ctx) {
+            ctx->message = "";
+        }
         if (ctx && cudaSetDevice(ctx->device) != cudaSuccess) {
-            return kCuda;
+            return finish(ctx, kCuda);
         }
         if (precision > SPK_FP16) {
-            return kInvalidArgument;
+            return finish(ctx, kInvalidArgument);
         }
-        return precision == SPK_FP64 ? correlate<double, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
-                                                                       out_values, out_capacity, result)
-                                     : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
-                                                                      out_values, out_capacity, result,
-                                                                      precision == SPK_FP16);
+        return finish(ctx, precision == SPK_FP64
+                               ? correlate<double, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
+                                                                 out_values, out_capacity, result)
+                               : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
+                                                                out_values, out_capacity, result,
+                                                                precision == SPK_FP16));
     }
     catch (...) {
-        return kAllocation;
+        return ctx ? fail(ctx, kAllocation, "Correlation allocation failed.") : kAllocation;
     }
 }
 
@@ -702,11 +727,14 @@ int spk_correlate_binary_mask(spk_context* ctx, const spk_correlation_spec* spec
                               uint32_t select, uint8_t* mask, uint64_t mask_capacity, spk_correlation_result* result)
 {
     try {
+        if (ctx) {
+            ctx->message = "";
+        }
         if (ctx && cudaSetDevice(ctx->device) != cudaSuccess) {
-            return kCuda;
+            return finish(ctx, kCuda);
         }
         if (precision > SPK_FP16 || select > SPK_MASK_NONZERO || !box_first || !box_shape) {
-            return kInvalidArgument;
+            return finish(ctx, kInvalidArgument);
         }
         MaskRequest request {};
         for (int a = 0; a != 3; ++a) {
@@ -716,14 +744,15 @@ int spk_correlate_binary_mask(spk_context* ctx, const spk_correlation_spec* spec
         request.want_zero = select == SPK_MASK_ZERO;
         request.mask = mask;
         request.capacity = mask_capacity;
-        return precision == SPK_FP64 ? correlate<double, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
-                                                                       nullptr, 0, result, false, &request)
-                                     : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
-                                                                      nullptr, 0, result, precision == SPK_FP16,
-                                                                      &request);
+        return finish(ctx, precision == SPK_FP64
+                               ? correlate<double, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
+                                                                 nullptr, 0, result, false, &request)
+                               : correlate<float, std::uint8_t>(ctx, spec, environment, kernel, limits, control,
+                                                                nullptr, 0, result, precision == SPK_FP16,
+                                                                &request));
     }
     catch (...) {
-        return kAllocation;
+        return ctx ? fail(ctx, kAllocation, "Correlation allocation failed.") : kAllocation;
     }
 }
 
@@ -733,20 +762,23 @@ int spk_correlate_proximity(spk_context* ctx, const spk_correlation_spec* spec, 
                             spk_correlation_result* result)
 {
     try {
+        if (ctx) {
+            ctx->message = "";
+        }
         if (ctx && cudaSetDevice(ctx->device) != cudaSuccess) {
-            return kCuda;
+            return finish(ctx, kCuda);
         }
         if (precision > SPK_FP16) {
-            return kInvalidArgument;
+            return finish(ctx, kInvalidArgument);
         }
-        return precision == SPK_FP64 ? correlate<double, double>(ctx, spec, environment, kernel, limits, control,
-                                                                 out_values, out_capacity, result)
-                                     : correlate<float, double>(ctx, spec, environment, kernel, limits, control,
-                                                                out_values, out_capacity, result,
-                                                                precision == SPK_FP16);
+        return finish(ctx, precision == SPK_FP64
+                               ? correlate<double, double>(ctx, spec, environment, kernel, limits, control,
+                                                           out_values, out_capacity, result)
+                               : correlate<float, double>(ctx, spec, environment, kernel, limits, control, out_values,
+                                                          out_capacity, result, precision == SPK_FP16));
     }
     catch (...) {
-        return kAllocation;
+        return ctx ? fail(ctx, kAllocation, "Correlation allocation failed.") : kAllocation;
     }
 }
 

@@ -211,6 +211,9 @@ struct Session {
     __nv_bfloat16* items {};  // every orientation's kernel pooled to 32^3 (proposal input)
     bool items_ready {};
     std::uint64_t items_tag {};  // unique per session: names the pooled items for the network's cache
+    spk_validate_fn validator {};  // the caller's native validation of a chosen pose (may be null)
+    void* validator_user {};
+    std::uint64_t validated {}, rejected {};
 };
 
 Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
@@ -439,6 +442,25 @@ int greedy_step(spk_context* ctx, Session& s, const std::vector<std::size_t>& su
         cursors[*best] = c;
         if (!c.direct_zero) {
             continue;
+        }
+        // The reference's try_pose: the pose goes to native validation before
+        // it joins the layout; a rejected pose leaves the layout unchanged and
+        // the merge moves on to the next candidate (spectral.cpp:1289-1430,
+        // called at :1571-1591).
+        if (s.validator) {
+            const double pose[3] = { s.origin[0] + s.pitch * static_cast<double>(c.t[0]),
+                                     s.origin[1] + s.pitch * static_cast<double>(c.t[1]),
+                                     s.origin[2] + s.pitch * static_cast<double>(c.t[2]) };
+            const geo::Quat& q = s.catalog[c.orientation];
+            const int verdict = s.validator(s.validator_user, c.orientation, c.t, pose, q.data());
+            ++s.validated;
+            if (verdict == SPK_POSE_REJECTED) {
+                ++s.rejected;
+                continue;
+            }
+            if (verdict != SPK_POSE_ACCEPTED) {
+                return kValidationAborted;
+            }
         }
         int status = session_place(ctx, s, c.orientation, c.t);
         if (status) {
@@ -1028,6 +1050,30 @@ int spk_session_greedy(spk_context* ctx, uint64_t max_steps, uint64_t* placed, u
     catch (...) {
         return kAllocation;
     }
+}
+
+int spk_session_set_validator(spk_context* ctx, spk_validate_fn validator, void* user)
+{
+    if (!ctx || !session_of(ctx)) {
+        return kNotReady;
+    }
+    auto& s = *session_of(ctx);
+    s.validator = validator;
+    s.validator_user = user;
+    return kOk;
+}
+
+int spk_session_validation_counts(spk_context* ctx, uint64_t* validated, uint64_t* rejected)
+{
+    if (!ctx || !session_of(ctx)) {
+        return kNotReady;
+    }
+    if (!validated || !rejected) {
+        return kInvalidArgument;
+    }
+    *validated = session_of(ctx)->validated;
+    *rejected = session_of(ctx)->rejected;
+    return kOk;
 }
 
 int spk_session_features(spk_context* ctx, float* crop, float* items)

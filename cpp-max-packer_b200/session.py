@@ -4,7 +4,9 @@ reference's SpectralWorkspace plus its greedy placement loop.
 Reference: engine/pack_solver/src/spectral_pipeline.hpp:67-99 (workspace and
 build_spectral_pipeline pages) and engine/pack_solver/src/spectral.cpp:
 1460-1591 (run_trial: page merge by rank_less, direct-zero gate, place at
-origin + pitch * t).  Native validation stays with the caller.
+origin + pitch * t).  Native validation stays with the caller, who can hand
+it to the greedy loops as a validator (the reference's try_pose gate,
+spectral.cpp:1289-1430).
 """
 
 from __future__ import annotations
@@ -22,6 +24,10 @@ from .geometry import MeshC, _lib_ready
 from .pipeline import PAGE_SIZE, CandidateC, PageQueryC, PageReportC, RankedCandidate
 
 P = ctypes.c_void_p
+POSE_ACCEPTED, POSE_REJECTED = 0, 1
+# int (*)(void* user, uint64 orientation, const int64 t[3], const double pose_mm[3], const double q[4])
+VALIDATE_FN = ctypes.CFUNCTYPE(ctypes.c_int, P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int64),
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double))
 
 
 class SessionDescC(ctypes.Structure):
@@ -51,6 +57,8 @@ def _declare(lib):
     lib.spk_session_greedy.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64), P, P, P]
     lib.spk_session_field.argtypes = [P, ctypes.c_int, ctypes.c_uint64, P, P, P, ctypes.c_uint64]
     lib.spk_session_stats.argtypes = [P, P, ctypes.c_int]
+    lib.spk_session_set_validator.argtypes = [P, VALIDATE_FN, P]
+    lib.spk_session_validation_counts.argtypes = [P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     lib._session_declared = True
 
 
@@ -151,6 +159,36 @@ class Session:
         out = [Placement(int(ori[i]), tuple(int(v) for v in t[i]), float(scores[i])) for i in range(placed.value)]
         self.placements += out
         return out
+
+    def set_validator(self, validate) -> None:
+        """`validate(orientation, translation, pose_mm, quaternion_xyzw)`
+        returns True to accept a chosen pose, False to reject it (the greedy
+        moves on to the next candidate); an exception stops the fill with
+        SPECTRAL_VALIDATION_ABORTED.  None removes the validator."""
+        if validate is None:
+            self._validator = None
+            _lib.check(self.lib.spk_session_set_validator(self.context.handle, VALIDATE_FN(), None),
+                       "spk_session_set_validator")
+            return
+
+        def call(_user, orientation, t, pose, q):
+            try:
+                ok = validate(int(orientation), tuple(t[a] for a in range(3)), tuple(pose[a] for a in range(3)),
+                              tuple(q[a] for a in range(4)))
+            except Exception:  # noqa: BLE001 - reported to the library as an abort
+                return 2
+            return POSE_ACCEPTED if ok else POSE_REJECTED
+
+        self._validator = VALIDATE_FN(call)
+        _lib.check(self.lib.spk_session_set_validator(self.context.handle, self._validator, None),
+                   "spk_session_set_validator")
+
+    def validation_counts(self) -> tuple:
+        """(poses validated, poses rejected) since the session opened."""
+        v, r = ctypes.c_uint64(), ctypes.c_uint64()
+        _lib.check(self.lib.spk_session_validation_counts(self.context.handle, ctypes.byref(v), ctypes.byref(r)),
+                   "spk_session_validation_counts")
+        return int(v.value), int(r.value)
 
     def stats(self, reset: bool = False) -> dict:
         out = np.zeros(4, np.uint64)

@@ -95,6 +95,12 @@ void spk_context_destroy(spk_context* context);
 /* Static string for a status (e.g. "CORRELATION_NUMERIC"); never NULL.  The
  * reference's static code strings (correlation.hpp:52-56, ADR 0015). */
 const char* spk_status_code(int status);
+/* The failure message of the last correlation call on `context` (static
+ * text, "" after a success), worded as the reference words the same failure
+ * site: CorrelationFailure::message, correlation.cpp:255-590.  Sites with no
+ * counterpart there (device FFT length, CUDA errors) carry the library's own
+ * text.  Never NULL. */
+const char* spk_context_message(const spk_context* context);
 /* Measurement only, no counterpart in the reference: the number of kernels
  * this library launched on the context (all entry points). */
 uint64_t spk_context_launches(const spk_context* context);
@@ -340,10 +346,31 @@ int spk_session_remove_last(spk_context* context);
  * holds n x 32 entries. */
 int spk_session_pages(spk_context* context, uint64_t n, const spk_page_query* queries, spk_candidate* pages,
                       uint32_t* counts, spk_page_report* reports);
-/* Greedy fill (spectral.cpp:1460-1591 page merge, direct-zero recount gate;
- * native validation is the caller's): up to max_steps copies are placed. */
+/* Greedy fill (spectral.cpp:1460-1591 page merge, direct-zero recount gate,
+ * then the session's validator when one is set): up to max_steps copies are
+ * placed. */
 int spk_session_greedy(spk_context* context, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
                        int64_t* translations, double* scores);
+
+/* The caller's native validation of a chosen pose, the reference's try_pose
+ * -> geometry::validate_incremental gate (spectral.cpp:1289-1430, called at
+ * :1571-1591).  The greedy loops (spk_session_greedy,
+ * spk_session_greedy_proposed, spk_jobs_greedy) call it for each candidate
+ * with a zero exact overlap, in rank order, before placing it: pose_mm is
+ * origin + pitch * translation, exactly as the reference forms the
+ * CopyPose; quaternion_xyzw is the catalog entry.  Return
+ * SPK_POSE_ACCEPTED to place the copy, SPK_POSE_REJECTED to leave the layout
+ * unchanged and go on to the next candidate (the reference counts an
+ * invalid candidate and continues), anything else to stop the fill with
+ * SPECTRAL_VALIDATION_ABORTED.  Called on the thread that drives the
+ * context. */
+enum { SPK_POSE_ACCEPTED = 0, SPK_POSE_REJECTED = 1 };
+typedef int (*spk_validate_fn)(void* user, uint64_t orientation, const int64_t translation[3],
+                               const double pose_mm[3], const double quaternion_xyzw[4]);
+/* Sets (or, with NULL, clears) the session's validator. */
+int spk_session_set_validator(spk_context* context, spk_validate_fn validator, void* user);
+/* Poses the validator has seen and rejected since the session opened. */
+int spk_session_validation_counts(spk_context* context, uint64_t* validated, uint64_t* rejected);
 /* Measurement only, no counterpart in the reference.  Work counters of the
  * session's page pipeline since open or the last reset:
  * out[0] first-pass pages, [1] threshold passes, [2] exactly rescored
