@@ -159,6 +159,37 @@ __device__ __forceinline__ unsigned long long make_key(double score, unsigned in
     return (static_cast<unsigned long long>(k) << 32) | index;
 }
 
+// The FP32 score in a key's high half (the inverse of make_key's mapping).
+__device__ __forceinline__ float key_score_f32(unsigned long long key)
+{
+    const unsigned int k = static_cast<unsigned int>(key >> 32);
+    return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Prefilter of the epilogue, per legal z: the proximity sum below which a
+// cell's key is certainly above `bound`, so the cell needs no FP64 score.
+// The score t65z - 0.35 p / occ falls as p grows; a key exceeds the bound
+// when its score, rounded down to FP32, exceeds the bound's FP32 score S,
+// which holds once the score reaches the next float above S.  The returned
+// value lies below the exact crossing by a margin far wider than the FP64
+// rounding of the score, and is itself rounded down to FP32, so every p
+// below it gives a key above the bound.  No bound yet: -inf (no cell skips).
+__device__ __forceinline__ float skip_below(unsigned long long bound, double t65z, double inv_occ)
+{
+    if (bound == kEmptyKey) {
+        return -INFINITY;
+    }
+    const float s = key_score_f32(bound);
+    if (!isfinite(s)) {
+        return -INFINITY;
+    }
+    const double next = static_cast<double>(nextafterf(s, INFINITY));
+    const double scale = 0.35 * inv_occ;
+    const double crossing = (t65z - next) / scale;
+    const double margin = 1e-9 * (fabs(t65z) + fabs(next)) / scale;
+    return __double2float_rd(crossing - margin);
+}
+
 __device__ __forceinline__ unsigned long long warp_sort32(unsigned long long v, int lane)
 {
     for (int k = 2; k <= 32; k <<= 1) {
@@ -247,6 +278,8 @@ __global__ void pass_b2_kernel(const float2* __restrict__ inter, int L0, int L1,
     const int y = static_cast<int>(row % legal_y);
     const int zz = static_cast<int>(row / legal_y);
     const double t65z = t65[zz];
+    const float skip = mode == 0 ? skip_below(*reinterpret_cast<volatile unsigned long long*>(tau), t65z, inv_occ)
+                                 : -INFINITY;
     unsigned long long list_lo = kEmptyKey, list_hi = kEmptyKey;
     float residual = 0.f;
     const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
@@ -257,7 +290,7 @@ __global__ void pass_b2_kernel(const float2* __restrict__ inter, int L0, int L1,
         if (x < legal_x) {
             const float2 v = res[warp * pitch + x];
             residual = fmaxf(residual, fabsf(v.x - rintf(v.x)));
-            if (fabsf(v.x) < 0.5f) {
+            if (fabsf(v.x) < 0.5f && !(v.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(v.y) * inv_occ);
                 if (score >= cursor_floor) {
                     key = make_key(score, row_index + x);
@@ -359,6 +392,72 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
         const int z = t + 16 * m2;
         if (z < legal_z) {
             inter[col + plane * z] = v[m2];
+        }
+    }
+}
+
+// Pass A over a batch of orientations on 256^3 grids: the environment
+// spectrum column is read once per block and kept in registers while each
+// orientation of the batch finishes its kernel column, multiplies and
+// inverts along z.  The spectrum (134 MB at 256^3) then crosses HBM once per
+// batch instead of once per orientation.  The next orientation's kernel
+// planes are fetched before the current one's transforms.
+__global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
+                                                             const PassABatch batch,
+                                                             const float2* __restrict__ twiddles)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int j = threadIdx.x & 15;  // column within the group (coalesced direction)
+    const int t = threadIdx.x >> 4;  // lane within the line
+    const int ky = blockIdx.x >> 4;
+    const long long col = ((blockIdx.x & 15) << 4) + j + 256LL * ky;
+    const long long plane = 65536;
+    float2 sp[16];
+#pragma unroll
+    for (int k2 = 0; k2 < 16; ++k2) {
+        sp[k2] = __ldcs(spectrum + col + plane * (t + 16 * k2));
+    }
+    float2* line = lines + j * kRegLine;
+    // Kernel planes z = t and z = 16 + t of the next orientation (almost
+    // every kernel has K2 <= 32; deeper planes are read in the loop).
+    float2 next0 = make_float2(0.f, 0.f), next1 = make_float2(0.f, 0.f);
+    if (batch.count > 0) {
+        const PassASlot& s0 = batch.slot[0];
+        next0 = t < s0.K2 ? s0.partial[col + plane * t] : next0;
+        next1 = 16 + t < s0.K2 ? s0.partial[col + plane * (16 + t)] : next1;
+    }
+#pragma unroll 1
+    for (int g = 0; g < batch.count; ++g) {
+        const PassASlot s = batch.slot[g];
+        float2 v[16];
+        v[0] = next0;
+        v[1] = next1;
+#pragma unroll
+        for (int n1 = 2; n1 < 16; ++n1) {
+            const int z = 16 * n1 + t;
+            v[n1] = z < s.K2 ? s.partial[col + plane * z] : make_float2(0.f, 0.f);
+        }
+        if (g + 1 < batch.count) {
+            const PassASlot& sn = batch.slot[g + 1];
+            next0 = t < sn.K2 ? sn.partial[col + plane * t] : make_float2(0.f, 0.f);
+            next1 = 16 + t < sn.K2 ? sn.partial[col + plane * (16 + t)] : make_float2(0.f, 0.f);
+        }
+        fft256<false>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
+#pragma unroll
+        for (int k2 = 0; k2 < 16; ++k2) {
+            const float2 sv = sp[k2];
+            v[k2] = make_float2(sv.x * v[k2].x + sv.y * v[k2].y, sv.y * v[k2].x - sv.x * v[k2].y);
+        }
+        fft256<true>(v, line, t, tw);  // v[m2] = w(z = t + 16 m2)
+#pragma unroll
+        for (int m2 = 0; m2 < 16; ++m2) {
+            const int z = t + 16 * m2;
+            if (z < s.legal_z) {
+                s.inter[col + plane * z] = v[m2];
+            }
         }
     }
 }
@@ -530,6 +629,7 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     float residual = 0.f;
     // Keys above the request's pruning bound cannot enter its top 64.
     const unsigned long long bound = mode == 0 ? *reinterpret_cast<volatile unsigned long long*>(tau) : ~0ULL;
+    const float skip = mode == 0 && valid ? skip_below(bound, t65z, inv_occ) : -INFINITY;
     unsigned int lo = 0xffffffffu, hi = 0u;
 #pragma unroll 1
     for (int m2 = 0; m2 < 16; ++m2) {
@@ -539,7 +639,7 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
         if (valid && x < legal_x) {
             const float2 w = line[x];
             residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
-            if (fabsf(w.x) < 0.5f) {
+            if (fabsf(w.x) < 0.5f && !(w.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
                 if (score >= cursor_floor) {
                     key = make_key(score, row_index + x);
@@ -904,7 +1004,10 @@ int Pipeline::set_geometry(const std::int64_t* env_first, const std::uint32_t* e
     occ_ = static_cast<std::uint8_t*>(device_buffer(ctx_, "pipe.occ", cells, status));
     d2_ = static_cast<std::int32_t*>(device_buffer(ctx_, "pipe.d2", cells * sizeof(std::int32_t), status));
     spectrum_ = static_cast<float2*>(device_buffer(ctx_, "pipe.spectrum", grid * sizeof(float2), status));
-    if (!occ_ || !d2_ || !spectrum_) {
+    const long long tiles = static_cast<long long>((E_[0] + kEdtTile - 1) / kEdtTile) *
+                            ((E_[1] + kEdtTile - 1) / kEdtTile) * ((E_[2] + kEdtTile - 1) / kEdtTile);
+    tile_max_ = static_cast<std::int32_t*>(device_buffer(ctx_, "pipe.tile_max", tiles * sizeof(std::int32_t), status));
+    if (!occ_ || !d2_ || !spectrum_ || !tile_max_) {
         return status;
     }
     const std::uint32_t shape[3] = { env_shape[0], env_shape[1], env_shape[2] };
@@ -925,9 +1028,32 @@ int Pipeline::set_occupancy(const std::uint8_t* d_occupancy)
     const std::uint32_t shape[3] = { static_cast<std::uint32_t>(E_[0]), static_cast<std::uint32_t>(E_[1]),
                                      static_cast<std::uint32_t>(E_[2]) };
     int status = edt_squared(ctx_, occ_, d2_, shape, st);
+    if (status || (status = edt_tile_max(ctx_, d2_, shape, tile_max_, st))) {
+        return status;
+    }
+    return update_spectrum();
+}
+
+int Pipeline::add_occupied(const std::uint8_t* d_occupancy, const std::uint8_t* d_sites, const EdtBox& sites)
+{
+    cudaStream_t st = ctx_->stream;
+    const long long cells = static_cast<long long>(E_[0]) * E_[1] * E_[2];
+    if (d_occupancy != occ_) {
+        cudaMemcpyAsync(occ_, d_occupancy, cells, cudaMemcpyDeviceToDevice, st);
+    }
+    const std::uint32_t shape[3] = { static_cast<std::uint32_t>(E_[0]), static_cast<std::uint32_t>(E_[1]),
+                                     static_cast<std::uint32_t>(E_[2]) };
+    int status = edt_add_sites(ctx_, d_sites, sites, d2_, tile_max_, shape, st);
     if (status) {
         return status;
     }
+    return update_spectrum();
+}
+
+int Pipeline::update_spectrum()
+{
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
     const long long grid = static_cast<long long>(L_[0]) * L_[1] * L_[2];
     const bool reg256 = L_[0] == 256 && L_[1] == 256 && L_[2] == 256;
     const int blocks = reg256 ? 256 * 256 / 16 : launch_blocks(grid, 256);
@@ -1139,6 +1265,28 @@ double Pipeline::pass_a_bytes(const KernelSlot& s) const
     return plane * L_[2] + plane * (s.K[2] + s.legal[2]);
 }
 
+int Pipeline::run_a256_batch(const KernelSlot* const* slots, int count, float2* const* inter)
+{
+    int status = kOk;
+    const auto* tw2 = twiddle_table<float>(ctx_, L_[2], status);
+    if (!tw2) {
+        return status;
+    }
+    PassABatch batch {};
+    batch.count = count;
+    const double spectrum_bytes = static_cast<double>(L_[0]) * L_[1] * L_[2] * sizeof(float2);
+    double bytes = spectrum_bytes;
+    for (int i = 0; i < count; ++i) {
+        batch.slot[i] = { slots[i]->partial, inter[i], slots[i]->K[2], slots[i]->legal[2] };
+        bytes += pass_a_bytes(*slots[i]) - spectrum_bytes;
+    }
+    auto ev = pass_begin(ctx_);
+    pass_a256_batch_kernel<<<16 * 256, 256, 0, ctx_->stream>>>(spectrum_, batch, tw2);
+    pass_end(ctx_, 0, ev, bytes);
+    ctx_->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
 int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double threshold, double cursor_floor,
                        unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
                        unsigned long long* resid)
@@ -1150,15 +1298,18 @@ int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double thre
     if (!tw0 || !tw1) {
         return status;
     }
+    // Algorithmic bytes: B1 reads the legal-z planes and writes their legal
+    // rows; B2 reads those rows (its keys are a few KB).
+    const double legal_rows = static_cast<double>(s.legal[1]) * s.legal[2];
     auto ev = pass_begin(ctx_);
     pass_b1_256_kernel<<<16 * s.legal[2], 256, 0, st>>>(inter, s.legal[1], tw1);
-    pass_end(ctx_, 1, ev);
+    pass_end(ctx_, 1, ev, 8.0 * L_[0] * L_[1] * s.legal[2] + 8.0 * L_[0] * legal_rows);
     const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
     ev = pass_begin(ctx_);
     pass_b2_256_kernel<<<static_cast<unsigned>((rows + 15) / 16), 256, 0, st>>>(
         inter, s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied), mode, threshold,
         cursor_floor, keys, count, cap, tau, resid);
-    pass_end(ctx_, 2, ev);
+    pass_end(ctx_, 2, ev, 8.0 * L_[0] * legal_rows);
     ctx_->launches += 2;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
@@ -1220,12 +1371,44 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         floor[r] = requests[r].has_cursor ? requests[r].cursor.score - eps_s[r] : -INFINITY;
         runnable.push_back(r);
     }
-    for (std::size_t i = 0; i < runnable.size(); ++i) {
-        const int r = runnable[i];
-        const auto& s = slots_[requests[r].slot];
-        if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap, count + r, cap,
-                                      tau + r, resid + r))) {
+    if (large) {
+        // Pass A in batches of kPassABatch orientations, each batch followed by
+        // the batch's B passes.
+        const std::size_t stride = static_cast<std::size_t>(L_[0]) * L_[1] * L_[2];
+        const std::size_t batch_size = std::min<std::size_t>(kPassABatch, runnable.size());
+        auto* inter = static_cast<float2*>(
+            device_buffer(ctx_, "pipe.inter_batch", batch_size * stride * sizeof(float2), status));
+        if (!inter) {
             return status;
+        }
+        for (std::size_t i0 = 0; i0 < runnable.size(); i0 += kPassABatch) {
+            const int n = static_cast<int>(std::min<std::size_t>(kPassABatch, runnable.size() - i0));
+            const KernelSlot* group[kPassABatch];
+            float2* outs[kPassABatch];
+            for (int g = 0; g < n; ++g) {
+                group[g] = &slots_[requests[runnable[i0 + g]].slot];
+                outs[g] = inter + g * stride;
+            }
+            if ((status = run_a256_batch(group, n, outs))) {
+                return status;
+            }
+            for (int g = 0; g < n; ++g) {
+                const int r = runnable[i0 + g];
+                if ((status = run_b256(*group[g], outs[g], 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap,
+                                       count + r, cap, tau + r, resid + r))) {
+                    return status;
+                }
+            }
+        }
+    }
+    else {
+        for (std::size_t i = 0; i < runnable.size(); ++i) {
+            const int r = runnable[i];
+            const auto& s = slots_[requests[r].slot];
+            if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap, count + r,
+                                          cap, tau + r, resid + r))) {
+                return status;
+            }
         }
     }
     cudaMemcpyAsync(jobs, host_jobs.data(), R * sizeof(ExactJob), cudaMemcpyHostToDevice, st);

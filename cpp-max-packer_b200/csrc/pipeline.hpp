@@ -19,6 +19,7 @@
 
 #include "../../include/spk_b200.h"
 #include "common.cuh"
+#include "edt.cuh"
 
 struct spk_context;
 
@@ -52,6 +53,19 @@ struct KernelSlot {
     std::vector<std::uint8_t> host_cells;
 };
 
+// One orientation of a batched pass A (256^3 grids).
+constexpr int kPassABatch = 16;
+struct PassASlot {
+    const float2* partial;
+    float2* inter;
+    int K2;
+    int legal_z;
+};
+struct PassABatch {
+    PassASlot slot[kPassABatch];
+    int count;
+};
+
 struct PageRequest {
     std::uint64_t slot {};
     bool has_cursor {};
@@ -82,6 +96,10 @@ public:
                      double pitch, double container_min_z, double container_height);
     // Device occupancy (u8, E^3): runs the exact EDT and the environment spectrum.
     int set_occupancy(const std::uint8_t* d_occupancy);
+    // The same after the only change since the last call is that the cells
+    // d_sites != 0 (all inside `sites`, window coordinates) became occupied:
+    // the EDT is updated in place over the region they can affect.
+    int add_occupied(const std::uint8_t* d_occupancy, const std::uint8_t* d_sites, const EdtBox& sites);
     // Adds an oriented kernel field (host cells, X-fastest); returns the slot.
     int add_kernel(std::uint64_t orientation, const std::int64_t* first, const std::uint32_t* shape,
                    const std::uint8_t* cells, double max_z, std::uint64_t& slot);
@@ -105,6 +123,10 @@ private:
                  unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
                  unsigned long long* resid);
     double pass_a_bytes(const KernelSlot& s) const;
+    int update_spectrum();
+    // Pass A for up to kPassABatch orientations in one launch (256^3 grids);
+    // orientation i's legal-z intermediate goes to inter[i].
+    int run_a256_batch(const KernelSlot* const* slots, int count, float2* const* inter);
     double score(const KernelSlot& s, const std::int64_t* t, double p) const;
     double approx_epsilon(const KernelSlot& s) const;
 
@@ -118,6 +140,7 @@ private:
     double height_ {};
     std::uint8_t* occ_ {};
     std::int32_t* d2_ {};
+    std::int32_t* tile_max_ {};  // largest d2 per kEdtTile^3 tile (incremental EDT)
     float2* spectrum_ {};
     float2* inter_ {};
     std::size_t inter_bytes_ {};
