@@ -309,7 +309,268 @@ int blocks_for(long long n, int threads)
     return static_cast<int>(want < 1 ? 1 : (want > 148LL * 32 ? 148LL * 32 : want));
 }
 
+// ---- incremental update after new occupied cells ------------------------
+
+// Largest d2 of each kEdtTile^3 tile: one block of 64 threads per tile,
+// thread i scanning the tile's x-run at (y, z) = (i % 8, i / 8).  With a
+// region, tiles that do not meet it are left as they are.
+__global__ void __launch_bounds__(64) edt_tile_max_kernel(const std::int32_t* __restrict__ d2, int sx, int sy,
+                                                         int sz, int tx, int ty, std::int32_t* __restrict__ tile_max,
+                                                         const EdtBox* __restrict__ region)
+{
+    const int t = blockIdx.x;
+    const int x0 = (t % tx) * kEdtTile, y0 = ((t / tx) % ty) * kEdtTile, z0 = (t / (tx * ty)) * kEdtTile;
+    if (region) {
+        const EdtBox r = *region;
+        if (x0 >= r.hi[0] || x0 + kEdtTile <= r.lo[0] || y0 >= r.hi[1] || y0 + kEdtTile <= r.lo[1] ||
+            z0 >= r.hi[2] || z0 + kEdtTile <= r.lo[2]) {
+            return;  // the whole block
+        }
+    }
+    const int y = y0 + (threadIdx.x & 7), z = z0 + (threadIdx.x >> 3);
+    std::int32_t m = 0;
+    if (y < sy && z < sz) {
+        const std::int32_t* row = d2 + x0 + static_cast<long long>(sx) * (y + static_cast<long long>(sy) * z);
+        for (int i = 0; i < kEdtTile && x0 + i < sx; ++i) {
+            m = max(m, row[i]);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    }
+    __shared__ std::int32_t warp_max[2];
+    if ((threadIdx.x & 31) == 0) {
+        warp_max[threadIdx.x >> 5] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        tile_max[t] = max(warp_max[0], warp_max[1]);
+    }
+}
+
+__global__ void edt_region_init_kernel(EdtBox sites, EdtBox* __restrict__ region)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *region = sites;
+    }
+}
+
+// Grows `region` (initialised to the sites' box) by every tile that a new
+// site could bring nearer: one whose squared distance to the sites' box is
+// below its largest d2.  Every cell of any other tile is at least that far
+// from each new site, and already that near an old one.
+__global__ void edt_region_kernel(const std::int32_t* __restrict__ tile_max, int sx, int sy, int sz, int tx, int ty,
+                                  int tz, EdtBox sites, EdtBox* __restrict__ region)
+{
+    const long long tiles = static_cast<long long>(tx) * ty * tz;
+    int lo[3] = { INT32_MAX, INT32_MAX, INT32_MAX }, hi[3] = { INT32_MIN, INT32_MIN, INT32_MIN };
+    const int extent[3] = { sx, sy, sz };
+    for (long long t = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; t < tiles;
+         t += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int c[3] = { static_cast<int>(t % tx), static_cast<int>((t / tx) % ty),
+                           static_cast<int>(t / (1LL * tx * ty)) };
+        int a0[3], a1[3];
+        long long dist = 0;
+        for (int a = 0; a < 3; ++a) {
+            a0[a] = c[a] * kEdtTile;
+            a1[a] = min(a0[a] + kEdtTile, extent[a]);
+            const long long gap = max(0, max(sites.lo[a] - (a1[a] - 1), a0[a] - (sites.hi[a] - 1)));
+            dist += gap * gap;
+        }
+        if (dist < static_cast<long long>(tile_max[t])) {
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = min(lo[a], a0[a]);
+                hi[a] = max(hi[a], a1[a]);
+            }
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && lo[0] != INT32_MAX) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&region->lo[a], lo[a]);
+            atomicMax(&region->hi[a], hi[a]);
+        }
+    }
+}
+
+// First pass of the new sites' EDT over the region: along x, the squared
+// distance to the nearest site on the same line (a left and a right sweep).
+__global__ void edt_region_x_kernel(const std::uint8_t* __restrict__ sites, std::int32_t* __restrict__ tmp, int sx,
+                                    int sy, const EdtBox* __restrict__ region)
+{
+    const EdtBox r = *region;
+    const int ny = r.hi[1] - r.lo[1], nz = r.hi[2] - r.lo[2];
+    const long long line = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+    if (line >= static_cast<long long>(ny) * nz) {
+        return;
+    }
+    const int y = r.lo[1] + static_cast<int>(line % ny), z = r.lo[2] + static_cast<int>(line / ny);
+    const long long base = static_cast<long long>(sx) * (y + static_cast<long long>(sy) * z);
+    constexpr int kFar = 1 << 24;
+    int last = -kFar;
+    for (int x = r.lo[0]; x < r.hi[0]; ++x) {
+        if (sites[base + x]) {
+            last = x;
+        }
+        tmp[base + x] = x - last;
+    }
+    int next = kFar;
+    for (int x = r.hi[0] - 1; x >= r.lo[0]; --x) {
+        if (sites[base + x]) {
+            next = x;
+        }
+        const int d = min(tmp[base + x], next - x);
+        tmp[base + x] = d >= kFar / 2 ? kInf : d * d;
+    }
+}
+
+// Later passes over the region, along `axis` (1: y, 2: z): one thread per
+// line builds the lower envelope of the line's parabolas in shared memory
+// (f, site, first cell it wins: the integer rule of the full passes above)
+// and evaluates it; the last pass takes min with the old d2.
+__global__ void __launch_bounds__(32) edt_region_envelope_kernel(std::int32_t* __restrict__ tmp,
+                                                                std::int32_t* __restrict__ d2, int sx, int sy,
+                                                                int axis, int last, int max_length,
+                                                                const EdtBox* __restrict__ region)
+{
+    extern __shared__ __align__(16) unsigned char stack_raw[];
+    std::int32_t* sf = reinterpret_cast<std::int32_t*>(stack_raw);            // [max_length][32]
+    std::int16_t* sq = reinterpret_cast<std::int16_t*>(sf + max_length * 32);  // [max_length][32]
+    std::int16_t* ss = sq + max_length * 32;                                   // [max_length][32]
+    const EdtBox r = *region;
+    const int lane = threadIdx.x;
+    const int length = r.hi[axis] - r.lo[axis];
+    const int other = axis == 1 ? 2 : 1;  // the second line coordinate; x is the first
+    const int n0 = r.hi[0] - r.lo[0], n1 = r.hi[other] - r.lo[other];
+    const long long line = static_cast<long long>(blockIdx.x) * 32 + lane;
+    if (line >= static_cast<long long>(n0) * n1) {
+        return;
+    }
+    const int x = r.lo[0] + static_cast<int>(line % n0);
+    const int w = r.lo[other] + static_cast<int>(line / n0);
+    const long long plane = static_cast<long long>(sx) * sy;
+    const long long stride = axis == 1 ? sx : plane;
+    const long long base = x + (axis == 1 ? plane * w : static_cast<long long>(sx) * w) + stride * r.lo[axis];
+    int count = 0;
+    for (int q = 0; q < length; ++q) {
+        const std::int32_t f = tmp[base + q * stride];
+        if (f == kInf) {
+            continue;
+        }
+        int start = -1;
+        while (count > 0) {
+            const int top = (count - 1) * 32 + lane;
+            const long long p = sq[top];
+            const long long numerator = static_cast<long long>(f) - sf[top] + 1LL * q * q - p * p;
+            const long long denominator = 2LL * (q - p);
+            if (numerator >= static_cast<long long>(ss[top]) * denominator) {
+                long long quotient = numerator / denominator;
+                if (numerator % denominator != 0 && numerator < 0) {
+                    --quotient;
+                }
+                const long long first = quotient + 1;
+                start = first < -1 ? -1 : first > length ? length : static_cast<int>(first);
+                break;
+            }
+            --count;
+        }
+        if (count == 0) {
+            start = -1;
+        }
+        const int slot = count * 32 + lane;
+        sf[slot] = f;
+        sq[slot] = static_cast<std::int16_t>(q);
+        ss[slot] = static_cast<std::int16_t>(start);
+        ++count;
+    }
+    int site = 0;
+    for (int q = 0; q < length; ++q) {
+        long long value = kInf;
+        if (count > 0) {
+            while (site + 1 < count && ss[(site + 1) * 32 + lane] <= q) {
+                ++site;
+            }
+            const long long delta = q - sq[site * 32 + lane];
+            value = static_cast<long long>(sf[site * 32 + lane]) + delta * delta;
+        }
+        const long long at = base + q * stride;
+        const std::int32_t v = value >= kInf ? kInf : static_cast<std::int32_t>(value);
+        if (last) {
+            d2[at] = min(d2[at], v);
+        }
+        else {
+            tmp[at] = v;
+        }
+    }
+}
+
 }  // namespace
+
+int edt_tile_max(spk_context* ctx, const std::int32_t* d_d2, const std::uint32_t* shape, std::int32_t* d_tile_max,
+                 cudaStream_t stream)
+{
+    const int tx = (static_cast<int>(shape[0]) + kEdtTile - 1) / kEdtTile;
+    const int ty = (static_cast<int>(shape[1]) + kEdtTile - 1) / kEdtTile;
+    const int tz = (static_cast<int>(shape[2]) + kEdtTile - 1) / kEdtTile;
+    edt_tile_max_kernel<<<tx * ty * tz, 64, 0, stream>>>(d_d2, shape[0], shape[1], shape[2], tx, ty, d_tile_max,
+                                                         nullptr);
+    ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int edt_add_sites(spk_context* ctx, const std::uint8_t* d_sites, const EdtBox& sites, std::int32_t* d_d2,
+                  std::int32_t* d_tile_max, const std::uint32_t* shape, cudaStream_t stream)
+{
+    EdtBox box = sites;
+    for (int a = 0; a < 3; ++a) {
+        box.lo[a] = std::max(box.lo[a], 0);
+        box.hi[a] = std::min(box.hi[a], static_cast<int>(shape[a]));
+        if (box.lo[a] >= box.hi[a]) {
+            return kOk;  // no new site inside the window
+        }
+    }
+    const int sx = static_cast<int>(shape[0]), sy = static_cast<int>(shape[1]), sz = static_cast<int>(shape[2]);
+    if (sx > 32767 || sy > 32767 || sz > 32767) {
+        return kInvalidArgument;  // sites are held as 16-bit coordinates
+    }
+    const long long n = static_cast<long long>(sx) * sy * sz;
+    int status = kOk;
+    auto* region = static_cast<EdtBox*>(device_buffer(ctx, "edt.region", sizeof(EdtBox), status));
+    auto* tmp = static_cast<std::int32_t*>(device_buffer(ctx, "edt.tmp", n * sizeof(std::int32_t), status));
+    if (!region || !tmp) {
+        return status;
+    }
+    const int tx = (sx + kEdtTile - 1) / kEdtTile, ty = (sy + kEdtTile - 1) / kEdtTile,
+              tz = (sz + kEdtTile - 1) / kEdtTile;
+    const long long tiles = static_cast<long long>(tx) * ty * tz;
+    const int longest = std::max(sy, sz);
+    if (static_cast<long long>(longest) * 32 * 8 > 227LL * 1024) {
+        return kInvalidArgument;
+    }
+    static std::once_flag attribute[64];
+    once_per_device(attribute, [] {
+        cudaFuncSetAttribute(edt_region_envelope_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    });
+    edt_region_init_kernel<<<1, 32, 0, stream>>>(box, region);
+    edt_region_kernel<<<blocks_for(tiles, 256), 256, 0, stream>>>(d_tile_max, sx, sy, sz, tx, ty, tz, box, region);
+    edt_region_x_kernel<<<static_cast<unsigned>((static_cast<long long>(sy) * sz + 127) / 128), 128, 0, stream>>>(
+        d_sites, tmp, sx, sy, region);
+    edt_region_envelope_kernel<<<static_cast<unsigned>((static_cast<long long>(sx) * sz + 31) / 32), 32,
+                                 static_cast<std::size_t>(sy) * 32 * 8, stream>>>(tmp, d_d2, sx, sy, 1, 0, sy,
+                                                                                  region);
+    edt_region_envelope_kernel<<<static_cast<unsigned>((static_cast<long long>(sx) * sy + 31) / 32), 32,
+                                 static_cast<std::size_t>(sz) * 32 * 8, stream>>>(tmp, d_d2, sx, sy, 2, 1, sz,
+                                                                                  region);
+    edt_tile_max_kernel<<<static_cast<unsigned>(tiles), 64, 0, stream>>>(d_d2, sx, sy, sz, tx, ty, d_tile_max,
+                                                                          region);
+    ctx->launches += 6;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
 
 bool proximity_shape_supported(const std::uint32_t* shape)
 {

@@ -113,10 +113,12 @@ int object_field(spk_context* ctx, const geo::Prepared& prepared, const double* 
     return cudaStreamSynchronize(ctx->stream) == cudaSuccess ? kOk : kCuda;
 }
 
-// voxelize_placed into d_out over `requested` (device).
+// voxelize_placed into d_out over `requested` (device).  `support`, when
+// given, receives a box (cells of `requested`, possibly reaching past its
+// edges) outside which every output cell is zero.
 int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Window& requested, const double* origin,
                  double pitch, const geo::Vec3& translation, const geo::Quat& q, double clearance,
-                 std::uint8_t* d_out)
+                 std::uint8_t* d_out, EdtBox* support = nullptr)
 {
     if (!geo::canonical_unit(q)) {
         return kFieldInput;
@@ -135,7 +137,22 @@ int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Win
     const std::uint64_t n = cells_of(requested);
     if (kind == geo::PlanKind::certified_empty) {
         cudaMemsetAsync(d_out, 0, n, ctx->stream);
+        if (support) {
+            *support = {};
+        }
         return kOk;
+    }
+    if (support) {
+        // The raster writes only inside `plan`; the clearance dilation reaches
+        // `halo` cells further.
+        for (int a = 0; a < 3; ++a) {
+            const long long h = static_cast<long long>(halo);
+            const long long lo = plan.first[a] - h - requested.first[a];
+            const long long hi = plan.first[a] + static_cast<long long>(plan.shape[a]) + h - requested.first[a];
+            const long long top = static_cast<long long>(requested.shape[a]);
+            support->lo[a] = static_cast<int>(std::min(std::max(lo, -1LL), top + 1));
+            support->hi[a] = static_cast<int>(std::min(std::max(hi, -1LL), top + 1));
+        }
     }
     int status = kOk;
     auto* raw = static_cast<std::uint8_t*>(device_buffer(ctx, "placed.raw", cells_of(plan), status));
@@ -214,6 +231,11 @@ struct Session {
     spk_validate_fn validator {};  // the caller's native validation of a chosen pose (may be null)
     void* validator_user {};
     std::uint64_t validated {}, rejected {};
+    // Set when the only change since the last refresh is one placed copy,
+    // whose field is in "session.placed" with its support box: the EDT is
+    // then updated in place rather than rebuilt.
+    bool one_added {};
+    EdtBox added_support {};
 };
 
 Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
@@ -228,10 +250,17 @@ int refresh(spk_context* ctx, Session& s)
     if (status) {
         return status;
     }
-    if ((status = s.pipe->set_occupancy(s.occ))) {
+    if (s.one_added) {
+        auto* placed = static_cast<std::uint8_t*>(device_buffer(ctx, "session.placed", cells_of(s.env), status));
+        if (!placed || (status = s.pipe->add_occupied(s.occ, placed, s.added_support))) {
+            return status ? status : kAllocation;
+        }
+    }
+    else if ((status = s.pipe->set_occupancy(s.occ))) {
         return status;
     }
     s.dirty = false;
+    s.one_added = false;
     return kOk;
 }
 
@@ -280,14 +309,18 @@ int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const
     if (!placed) {
         return status;
     }
+    EdtBox support {};
     if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[orientation], s.pair,
-                               placed))) {
+                               placed, &support))) {
         return status;
     }
     if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), 1))) {
         return status;
     }
     s.copies.push_back({ orientation, { t[0], t[1], t[2] } });
+    // One copy added to an up-to-date layout: its EDT can be updated in place.
+    s.one_added = !s.dirty;
+    s.added_support = support;
     s.dirty = true;
     return kOk;
 }
@@ -960,6 +993,7 @@ int spk_session_remove_last(spk_context* ctx)
         }
         s.copies.pop_back();
         s.dirty = true;
+        s.one_added = false;  // distances can grow: rebuild
         return kOk;
     }
     catch (...) {
