@@ -156,11 +156,15 @@ def custom_catalog(quaternions) -> np.ndarray:
     return out[: count.value].copy()
 
 
-def hopf_catalog(count: int, seed: int) -> np.ndarray:
-    """Seeded uniform SO(3) sample (unit quaternions via Shoemake's subgroup
-    algorithm), made canonical and de-duplicated like a custom catalog."""
+def hopf_quaternions(count: int, seed: int) -> np.ndarray:
+    """Seeded uniform SO(3) sample: unit XYZW quaternions by Shoemake's
+    subgroup algorithm, before canonicalisation (numpy only)."""
     rng = np.random.default_rng(seed)
     u1, u2, u3 = rng.random(count), rng.random(count), rng.random(count)
-    q = np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
-                  np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], axis=1)
-    return custom_catalog(q)
+    return np.stack([np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+                     np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)], axis=1)
+
+
+def hopf_catalog(count: int, seed: int) -> np.ndarray:
+    """hopf_quaternions made canonical and de-duplicated like a custom catalog."""
+    return custom_catalog(hopf_quaternions(count, seed))
