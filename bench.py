@@ -34,10 +34,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 METRIC = "placements/s at 256^3 grid x512 orients: learned-proposal vs exhaustive GPU"
 UNIT = "placements/s"
-# dram__bytes_read.sum + dram__bytes_write.sum of one pass_a256_kernel launch,
-# mean of the four launches captured in profiles/step_kernels_rounded256_o16.md
-# (211,964,672 / 211,798,016 / 211,456,000 / 211,373,312 bytes).
-PASS_A256_DRAM_BYTES = 211648000
+# The page pipeline's passes as the library's per-pass timing reports them.
+PASSES = [
+    ("pass_a256_batch_kernel", "spectral z: environment spectrum read once per batch of orientations, kernel z "
+                               "finish, conjugate product, inverse z"),
+    ("pass_b1_256_kernel", "inverse y over the legal z planes"),
+    ("pass_b2_256_kernel", "inverse x with the fused threshold / score / top-k epilogue"),
+    ("merge_kernel + exact_kernel", "key merge and exact recount"),
+]
+# dram__bytes_read.sum + dram__bytes_write.sum per launch of each kernel on
+# the 256^3 workload, from the ncu captures summarised in profiles/ (the file
+# named beside each figure); absent where no capture of the current kernel
+# exists yet.
+NCU_DRAM_BYTES = {}
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp-max-packer_b200", "weights",
                                "proposal_rounded256.npz")
 
@@ -158,6 +167,28 @@ def timed_steps(stream, fn, dist):
     return start.elapsed_time(end), out
 
 
+class profiler_region:
+    """cudaProfilerStart/Stop around one timed arm, so that a profiler started
+    with --profile-from-start off records only that arm's launches."""
+
+    def __init__(self, active: bool):
+        self.active = active
+
+    def __enter__(self):
+        if self.active:
+            import torch
+
+            torch.cuda.profiler.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.active:
+            import torch
+
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+
+
 def max_over_ranks(ms, placed, world):
     """(max ms over ranks, placements summed over ranks).  The exchanged pair
     sits on the device the process group's backend serves: CUDA under NCCL,
@@ -203,12 +234,16 @@ def run_ours(args, rank, world, local_rank):
     k = min(args.k, O)
 
     with ClockSampler(local_rank) as clocks:
-        # Exhaustive arm: every orientation paged at every step.
-        session.greedy(args.warmup)
+        # Exhaustive arm: every orientation paged at every step (a profiling
+        # run of the learned arm alone may skip it).
+        skip_exhaustive = args.no_extras and args.profile_region == "learned"
+        session.greedy(0 if skip_exhaustive else args.warmup)
         session.stats(reset=True)
         launches0 = ctx.launches
         exhaustive_offset = int(launches0)
-        ex_ms, ex_placed = timed_steps(stream, lambda: session.greedy(args.steps), dist)
+        with profiler_region(args.profile_region == "exhaustive"):
+            ex_ms, ex_placed = timed_steps(stream, lambda: session.greedy(0 if skip_exhaustive else args.steps),
+                                           dist)
         ex_launches = ctx.launches - launches0
         page_stats = session.stats(reset=True)
         ex_ms, ex_total = max_over_ranks(ex_ms, len(ex_placed), world)
@@ -224,8 +259,9 @@ def run_ours(args, rank, world, local_rank):
             proposal.greedy_proposed(session, net, k, args.warmup)
             launches0 = ctx.launches
             learned_offset = int(launches0)
-            ln_ms, (ln_placed, fallbacks) = timed_steps(
-                stream, lambda: proposal.greedy_proposed(session, net, k, args.steps), dist)
+            with profiler_region(args.profile_region == "learned"):
+                ln_ms, (ln_placed, fallbacks) = timed_steps(
+                    stream, lambda: proposal.greedy_proposed(session, net, k, args.steps), dist)
             ln_launches = ctx.launches - launches0
             ln_ms, ln_total = max_over_ranks(ln_ms, len(ln_placed), world)
             ln_value = ln_total / (ln_ms / 1000.0) if ln_ms > 0 else 0.0
@@ -245,8 +281,9 @@ def run_ours(args, rank, world, local_rank):
         ctx.close()
         return
 
-    # Roofline of pass A (the dominant spectral pass), timed with events on the
-    # context stream around each launch during two further exhaustive steps.
+    # Roofline of the page passes, timed with events on the context stream
+    # around each launch during two further exhaustive steps; the bench line's
+    # roofline is the pass with the largest share of that time.
     lib.spk_context_set_profiling(ctx.handle, 1)
     session.greedy(2)
     launches_arr = np.zeros(4, np.uint64)
@@ -256,12 +293,20 @@ def run_ours(args, rank, world, local_rank):
     lib.spk_context_pass_bytes(ctx.handle, pass_bytes.ctypes.data, 4)
     lib.spk_context_set_profiling(ctx.handle, 0)
     hbm, peak_kind = peaks()
-    launches_a = max(int(launches_arr[0]), 1)
-    bytes_a = pass_bytes[0] / launches_a  # algorithmic bytes per pass-A launch (one orientation)
-    avg_a_ms = total_ms[0] / launches_a
-    achieved = bytes_a / (avg_a_ms / 1000.0) / 1e9 if avg_a_ms > 0 else 0.0
-    pass_share = {name: round(float(total_ms[i] / max(total_ms.sum(), 1e-9)), 3)
-                  for i, name in enumerate(["spectral_z", "inverse_y", "inverse_x_epilogue", "merge_exact"])}
+    full256 = tuple(session.fft_shape) == (256, 256, 256)
+    passes = []
+    for i, (kernel, what) in enumerate(PASSES):
+        n = max(int(launches_arr[i]), 1)
+        avg_ms = total_ms[i] / n
+        per_launch = pass_bytes[i] / n
+        achieved_i = per_launch / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 and per_launch > 0 else None
+        passes.append({"kernel": kernel, "work": what, "launches": int(launches_arr[i]),
+                       "share": round(float(total_ms[i] / max(total_ms.sum(), 1e-9)), 3),
+                       "avg_launch_ms": round(avg_ms, 5), "algorithmic_bytes_per_launch": int(per_launch),
+                       "achieved_gbs": round(achieved_i, 1) if achieved_i else None,
+                       "frac": round(achieved_i / hbm, 4) if achieved_i else None,
+                       "traffic": NCU_DRAM_BYTES.get(kernel) if full256 else None})
+    dominant = max(passes[:3], key=lambda p: p["share"])
 
     # End to end through the public API with host buffers: the proposal
     # (predictions out), page queries in, pages out, the chosen copy placed.
@@ -301,9 +346,11 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(wl, O)
+        cpu = cpu_baseline(args.workload, O)
 
     if rank == 0:
+        config = reference_config(args.workload, world)
+        config["orientations"] = O
         value = ln_value if learned else ex_value
         ms = ln_ms if learned else ex_ms
         same = 0
@@ -317,27 +364,21 @@ def run_ours(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32 spectra, fp64 exact scores, u8 fields, bf16 proposal network",
             "data": "synthetic (seeded rounded-box STL container, spherical-harmonic blob item, seeded SO(3) catalog)",
-            "config": {"workload": wl.name, "grid": list(session.environment_shape), "fft": list(session.fft_shape),
-                       "orientations": O, "object_triangles": int(len(wl.obj.triangles)),
-                       "container_triangles": int(len(wl.container.triangles)) if hasattr(wl.container, "triangles")
-                       else 0,
-                       "mode": f"learned proposal (top {k} of {O}, exhaustive fallback)" if learned else "exhaustive",
-                       "l2": "working set above L2 (all orientations' kernel spectra stay in HBM)",
-                       "session_open_s": round(open_s, 2), "parallelism": f"replicas x{world}",
-                       "page_stats_exhaustive": page_stats},
+            "config": config,
+            "mode": f"learned proposal (top {k} of {O}, exhaustive fallback)" if learned else "exhaustive",
+            "fft": list(session.fft_shape), "session_open_s": round(open_s, 2), "page_stats_exhaustive": page_stats,
             "exhaustive": {"value": round(ex_value, 4), "ms_per_step": round(ex_ms / max(args.steps, 1), 4),
                            "gpu_launches": int(ex_launches),
                            "step_model": step_model(session.fft_shape, session.environment_shape, O,
                                                     ex_ms / max(args.steps, 1), hbm)},
             "gpu_launches": int(ln_launches if learned else ex_launches),
-            "roofline": {"bound": "hbm", "kernel": "pass_a256_kernel (spectral z pass)",
-                         "achieved": round(achieved, 1), "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4),
-                         # DRAM read + write bytes of one pass_a256 launch (one orientation), cold-cache ncu
-                         # capture of the same kernel on this workload's 256^3 window; see profiles/.
-                         "traffic": PASS_A256_DRAM_BYTES if tuple(session.fft_shape) == (256, 256, 256) else None,
-                         "algorithmic_bytes_per_launch": int(bytes_a), "avg_launch_ms": round(avg_a_ms, 5),
-                         "pass_share": pass_share},
+            "roofline": {"bound": "hbm", "kernel": f"{dominant['kernel']} ({dominant['work']})",
+                         "achieved": dominant["achieved_gbs"], "peak": hbm,
+                         "peak_kind": f"{peak_kind} (burst copy bandwidth; each launch is timed alone)",
+                         "unit": "GB/s", "frac": dominant["frac"], "traffic": dominant["traffic"],
+                         "algorithmic_bytes_per_launch": dominant["algorithmic_bytes_per_launch"],
+                         "avg_launch_ms": dominant["avg_launch_ms"], "share": dominant["share"],
+                         "passes": passes},
             "e2e": e2e,
             "clocks": clocks.summary(),
         }
@@ -355,54 +396,39 @@ def run_ours(args, rank, world, local_rank):
     ctx.close()
 
 
-def reference_sample(wl, z_planes: int = 16, orientation: int = 0, barrier=None):
-    """The reference's own correlate_binary_cpu + correlate_proximity_cpu
-    (compiled from its sources; FP64 FFT with a Bluestein stand-in for
-    pocketfft) for one orientation's kernel against the lowest `z_planes`
-    planes of the workload's environment window (the empty layout's container
-    blocker and proximity).  Preparation runs before `barrier`; only the two
-    correlations are timed.  Returns (seconds, sampled padded cells, full
-    padded cells, kernel shape, window shape)."""
-    from oracle.bindings import Ref, ref_voxelize_container
-
-    geometry = pkg("geometry")
-    ref = Ref()
-    obj = ref.asset(wl.object_stl)
-    kfirst, kshape, kernel = obj.voxelize_object(wl.origin, wl.pitch, wl.catalog[orientation])
-    if wl.container_stl:
-        container = ref.asset(wl.container_stl, container=True)
-        v, t, b = container.mesh()
-        bounds = list(b)
-    else:
-        container = tuple(wl.container)
-        bounds = [0, 0, 0, *wl.container]
-    first, shape = geometry.environment_window(bounds, wl.origin, wl.pitch)
-    sub_shape = (shape[0], shape[1], min(z_planes, shape[2]))
-    mask = ref_voxelize_container(ref, container, wl.origin, wl.pitch, first, sub_shape, wl.wall_clearance)
-    prox = ref.build_proximity(sub_shape, mask)
-    if barrier is not None:
-        barrier.wait()
-    t0 = time.perf_counter()
-    b = ref.correlate(False, sub_shape, kshape, first, kfirst, mask, kernel)
-    p = ref.correlate(True, sub_shape, kshape, first, kfirst, prox, kernel)
-    seconds = time.perf_counter() - t0
-    if isinstance(b, str) or isinstance(p, str):
-        raise RuntimeError(f"reference correlation failed: {b if isinstance(b, str) else p}")
-    padded_sample = float(np.prod([e + k - 1 for e, k in zip(sub_shape, kshape)]))
-    padded_full = float(np.prod([e + k - 1 for e, k in zip(shape, kshape)]))
-    return seconds, padded_sample, padded_full, tuple(int(v) for v in kshape), tuple(int(v) for v in sub_shape)
-
-
-def _sample_worker(workload, z_planes, orientation, barrier, queue):
+def _page_worker(workload, worker, orientations, warmup_orientations, barrier, queue):
+    """One host process of the reference arm: the reference's own session on
+    the workload's empty layout (container blocker, proximity and kernels
+    built by the reference's code), untimed warm-up pages, then whole pages
+    of `orientations` after `barrier`.  Reports (worker, seconds per page,
+    start, end) with perf_counter times, or an error string."""
     try:
-        wl = pkg("workloads").WORKLOADS[workload]()
-        queue.put((orientation, reference_sample(wl, z_planes, orientation, barrier)))
+        from oracle.bindings import Ref
+
+        spec = pkg("workloads").SPECS[workload]()
+        ref = Ref()
+        obj = ref.asset(spec.object_stl)
+        container = tuple(spec.container_box) if spec.container_box is not None else \
+            ref.asset(spec.container_stl, container=True)
+        catalog = ref.catalog(1) if spec.catalog_kind == "cube" else ref.catalog(4, spec.raw_quaternions())
+        session = ref.session(obj, container, spec.pair_clearance, spec.wall_clearance, spec.origin, spec.pitch,
+                              catalog)
+        for o in warmup_orientations:  # the first builds the environment fields
+            session.page(o % len(catalog))
+        barrier.wait()
+        start = time.perf_counter()
+        times = []
+        for o in orientations:
+            t0 = time.perf_counter()
+            session.page(o % len(catalog))
+            times.append(time.perf_counter() - t0)
+        queue.put((worker, times, start, time.perf_counter()))
     except Exception as exc:  # reported to the parent, which fails the measurement
         try:
             barrier.abort()
         except Exception:
             pass
-        queue.put((orientation, f"{type(exc).__name__}: {exc}"))
+        queue.put((worker, f"{type(exc).__name__}: {exc}", 0.0, 0.0))
 
 
 def host_cores() -> int:
@@ -412,97 +438,122 @@ def host_cores() -> int:
         return os.cpu_count() or 1
 
 
-def reference_throughput(wl, z_planes: int = 16, workers: int = 0):
-    """Reference CPU placements/s for the workload: `workers` processes (one
-    per host core by default; spawned, so they are safe beside a CUDA
-    context) each correlate a different orientation's sampled page at the
-    same time.  The reference parallelises its FFT only on Windows, so on
-    this host concurrency comes from independent orientations, which is how a
-    multi-core caller would use it.  Each sample is scaled by P log P to the
-    full page; the step takes ceil(O / workers) rounds of the slowest worker.
-    Returns (placements/s, workers, description)."""
+def reference_pages(workload: str, pages: int, workers: int = 0, first_orientation: int = 0, warmup: int = 1):
+    """Whole pages of the reference's own spectral pipeline
+    (build_spectral_pipeline, spectral_pipeline.cpp:914-1876: the kernel's
+    raster, the binary and proximity FFT correlations, the page scan and the
+    exact recount), compiled from its sources into oracle/_ref, for `pages`
+    distinct orientations spread over `workers` concurrent processes (one per
+    host core by default; spawned, so they are safe beside a CUDA context),
+    after `warmup` untimed pages (at least one per worker).  The reference
+    parallelises its FFT only on Windows (fft_execution.cpp:201), so on this
+    host concurrency comes from independent orientations, which is how a
+    multi-core caller would use it.  Returns (wall seconds from the common
+    start to the last page's end, per-page seconds, workers)."""
     import multiprocessing as mp
 
-    O = len(wl.catalog)
-    workers = max(1, min(workers or host_cores(), O, 128))
+    workers = max(1, min(workers or host_cores(), pages))
     ctx = mp.get_context("spawn")
     barrier = ctx.Barrier(workers)
     queue = ctx.Queue()
-    stride = max(1, O // workers)
-    procs = [ctx.Process(target=_sample_worker, args=(wl.name, z_planes, (i * stride) % O, barrier, queue))
-             for i in range(workers)]
+    share = [list(range(first_orientation + w, first_orientation + pages, workers)) for w in range(workers)]
+    per_worker = max(1, -(-warmup // workers))
+    warm = [[first_orientation + pages + w * per_worker + i for i in range(per_worker)] for w in range(workers)]
+    procs = [ctx.Process(target=_page_worker, args=(workload, w, share[w], warm[w], barrier, queue))
+             for w in range(workers)]
     for p in procs:
         p.start()
-    results = [queue.get(timeout=1800) for _ in procs]
+    results = [queue.get(timeout=3600) for _ in procs]
     for p in procs:
-        p.join(timeout=60)
-    errors = [r for _, r in results if isinstance(r, str)]
+        p.join(timeout=120)
+    errors = [r[1] for r in results if isinstance(r[1], str)]
     if errors:
         raise RuntimeError(errors[0])
-    scaled = [scaled_step_seconds(r[0], r[1], r[2], 1) for _, r in results]
-    rounds = -(-O // workers)
-    step = max(scaled) * rounds
-    sec = [r[0] for _, r in results]
-    r0 = results[0][1]
-    desc = (f"reference correlate_binary_cpu + correlate_proximity_cpu (FP64, Bluestein stand-in for pocketfft) "
-            f"in {workers} concurrent processes, each one orientation's ~{r0[3]} kernel against the lowest "
-            f"{r0[4][2]} z-planes of the window ({min(sec):.1f}-{max(sec):.1f} s, {r0[1]:.3g} padded cells); "
-            f"each scaled by P log P to the full {r0[2]:.3g}-cell page, slowest worker x {rounds} rounds "
-            f"for {O} orientations per placement")
-    return 1.0 / step, workers, desc
+    start = min(r[2] for r in results)
+    end = max(r[3] for r in results)
+    per_page = [t for r in results for t in r[1]]
+    return end - start, per_page, workers
 
 
-def scaled_step_seconds(seconds, padded_sample, padded_full, orientations):
-    return seconds * (padded_full * np.log2(padded_full)) / (padded_sample * np.log2(padded_sample)) * orientations
+def reference_config(workload: str, world: int) -> dict:
+    """The arms' shared config, computed without this library: the window
+    from the workload's container bounds and lattice (the reference's
+    GridWindow rule, spectral_pipeline.cpp:107-140: a one-cell halo)."""
+    import math
+
+    spec = pkg("workloads").SPECS[workload]()
+    assets = pkg("assets")
+    if spec.container_box is not None:
+        lo, hi = np.zeros(3), np.array(spec.container_box, np.float64)
+        container_triangles = 0
+    else:
+        mesh = assets.accept_stl(spec.container_stl, role="container")
+        lo, hi = mesh.bounds
+        container_triangles = int(len(mesh.triangles))
+    grid = [int(math.ceil((hi[a] - spec.origin[a]) / spec.pitch)) -
+            int(math.floor((lo[a] - spec.origin[a]) / spec.pitch)) + 2 for a in range(3)]
+    orientations = spec.catalog_count if spec.catalog_kind == "hopf" else 24
+    return {"workload": workload, "grid": grid, "orientations": orientations,
+            "object_triangles": int(len(assets.accept_stl(spec.object_stl).triangles)),
+            "container_triangles": container_triangles,
+            "l2": "working set above L2 (all orientations' kernel spectra stay in HBM)",
+            "parallelism": f"replicas x{world}"}
 
 
-def cpu_baseline(wl, orientations):
-    """Reported baseline only: the reference's own CPU correlation work for a
-    bounded sample of the same workload on all host cores, scaled to a
-    placement step."""
+def page_sample_description(pages, wall, per_page, cores, orientations, warmup):
+    return (f"{pages} whole pages of the reference's build_spectral_pipeline (kernel raster, FP64 binary and "
+            f"proximity FFT correlations with the oracle build's FFT in place of pocketfft, page scan, exact "
+            f"recount), distinct orientations on the empty layout after {warmup} warm-up pages, {cores} concurrent "
+            f"processes, {wall:.1f} s wall ({min(per_page):.1f}-{max(per_page):.1f} s per page); a step is one page, "
+            f"and placements/s = pages / {orientations} (pages per placement) / wall")
+
+
+def cpu_baseline(workload: str, orientations: int):
+    """Reported baseline only: one whole reference page per host core, run
+    concurrently (a bounded sample of the same workload), scaled linearly by
+    the orientation count to placements/s."""
     cores = host_cores()
     try:
         from oracle.bindings import REF_SO
 
-        if not os.path.exists(REF_SO) or not wl.object_stl:
+        if not os.path.exists(REF_SO):
             return None
-        value, cores, desc = reference_throughput(wl)
-        return {"value": round(value, 8), "unit": UNIT, "cores": cores, "kind": "reference", "sample": desc}
+        wall, per_page, cores = reference_pages(workload, cores)
+        value = (len(per_page) / orientations) / wall
+        return {"value": round(value, 8), "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": page_sample_description(len(per_page), wall, per_page, cores, orientations, cores)}
     except Exception as exc:  # the baseline is reported, never required
         return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference", "sample": f"unavailable: {exc}"}
 
 
 def run_reference(args, rank, world):
     """The reference's own CPU implementation of the path (compiled from its
-    sources into oracle/_ref), on every host core: each step is one bounded
-    concurrent sample (see reference_throughput), scaled to placements/s of
-    the same workload."""
+    sources into oracle/_ref), on every host core, loading nothing of this
+    library: each timed step is one whole page of a distinct orientation
+    (all steps run concurrently, one process per core), and placements/s is
+    the pages completed / the orientations a placement pages / the wall time
+    of the timed steps."""
     if rank != 0:
         return
-    workloads = pkg("workloads")
-    wl = workloads.WORKLOADS[args.workload]()
-    if args.orientations:
-        wl.catalog = wl.catalog[: args.orientations]
-    O = len(wl.catalog)
     try:
         from oracle.bindings import REF_SO
 
         if not os.path.exists(REF_SO):
             print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref/libspk_ref.so missing"}))
             return
-        for _ in range(args.warmup):
-            reference_sample(wl, z_planes=2)
-        values = []
-        desc, cores = "", 1
-        for _ in range(args.steps):
-            v, cores, desc = reference_throughput(wl)
-            values.append(v)
-        value = float(np.mean(values))
+        config = reference_config(args.workload, world)
+        O = args.orientations or config["orientations"]
+        config["orientations"] = O
+        wall, per_page, cores = reference_pages(args.workload, args.steps, workers=min(host_cores(), args.steps),
+                                                warmup=args.warmup)
+        value = (len(per_page) / O) / wall
+        desc = page_sample_description(len(per_page), wall, per_page, cores, O, args.warmup)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": round(value, 8), "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000.0 / value, 1),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000.0 * wall / max(args.steps, 1), 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": wl.name, "orientations": O, "mode": "exhaustive"},
+            "data": "synthetic (seeded rounded-box STL container, spherical-harmonic blob item, seeded SO(3) catalog)",
+            "config": config, "mode": "exhaustive (the reference pages every orientation)",
             "cpu_baseline": {"value": round(value, 8), "unit": UNIT, "cores": cores, "kind": "reference",
                              "sample": desc},
             "e2e": {"value": round(value, 8), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -521,6 +572,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--orientations", type=int, default=0, help="use the first N catalog entries (profiling runs)")
     ap.add_argument("--no-extras", action="store_true", help="skip the roofline and e2e passes (profiling runs)")
+    ap.add_argument("--profile-region", default="", choices=["", "learned", "exhaustive"],
+                    help="bracket that arm's timed steps with cudaProfilerStart/Stop (ncu --profile-from-start off)")
     ap.add_argument("--mode", default="learned", choices=["learned", "exhaustive"],
                     help="headline path (the exhaustive path is always timed beside it)")
     ap.add_argument("--k", type=int, default=32, help="orientations the proposal pages per step")
