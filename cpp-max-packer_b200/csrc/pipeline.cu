@@ -21,6 +21,7 @@
 // cursor and certifies that no excluded candidate could enter the page; an
 // uncertified page is recomputed in threshold mode (every candidate whose
 // approximate score is within the error bound of the page's last entry).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,6 +41,8 @@
 #include "superacc.cuh"
 
 namespace spk {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -575,43 +578,34 @@ __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ i
 //     is ever left out.
 //   mode 1: every candidate with approximate score <= threshold is appended
 //     and every candidate past the cursor floor is counted in *tau.
-__global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
-                                                         int legal_y, int legal_z,
-                                                         const float2* __restrict__ twiddles,
-                                                         const double* __restrict__ t65, double inv_occ, int mode,
-                                                         double threshold, double cursor_floor,
-                                                         unsigned long long* __restrict__ keys,
-                                                         unsigned int* __restrict__ count, unsigned int cap,
-                                                         unsigned long long* __restrict__ tau,
-                                                         unsigned long long* __restrict__ resid)
+struct B2Shared {
+    unsigned int hist[1024];
+    unsigned int block_lo, block_hi, warp_sums[8];
+    int cut_bin;
+    unsigned long long emit_bound;
+};
+
+// The inverse x transform of 16 legal rows and the fused epilogue above.
+// Thread (row j = threadIdx / 16, lane t = threadIdx % 16) holds in v[n1]
+// its row's value at kx = 16 n1 + t; `valid` rows are (y, zz).  Every thread
+// of the block calls it; it may be called again for the next 16 rows.
+__device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+                                           bool valid, int y, int zz, int legal_x, int legal_y,
+                                           const double* __restrict__ t65, double inv_occ, int mode,
+                                           double threshold, double cursor_floor,
+                                           unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
+                                           unsigned int cap, unsigned long long* __restrict__ tau,
+                                           unsigned long long* __restrict__ resid)
 {
     constexpr int kBins = 1024;
-    __shared__ float2 tw[256];
-    __shared__ float2 lines[16 * kRegLine];
-    __shared__ unsigned int hist[kBins];
-    __shared__ unsigned int block_lo, block_hi, warp_sums[8];
-    __shared__ int cut_bin;
-    __shared__ unsigned long long emit_bound;
-    tw[threadIdx.x] = twiddles[threadIdx.x];
-    if (threadIdx.x == 0) {
-        block_lo = 0xffffffffu;
-        block_hi = 0u;
-        cut_bin = kBins - 1;
-    }
-    __syncthreads();
     const int t = threadIdx.x & 15;  // lane within the row (coalesced direction)
     const int j = threadIdx.x >> 4;  // row within the block
     const int lane = threadIdx.x & 31;
-    const long long rows = static_cast<long long>(legal_y) * legal_z;
-    const long long row = static_cast<long long>(blockIdx.x) * 16 + j;
-    const bool valid = row < rows;
-    const int y = valid ? static_cast<int>(row % legal_y) : 0;
-    const int zz = valid ? static_cast<int>(row / legal_y) : 0;
-    const long long base = 256LL * (y + 256LL * zz);
-    float2 v[16];
-#pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1) {
-        v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
+    __syncthreads();  // the previous rows' readers of `sh` are done
+    if (threadIdx.x == 0) {
+        sh.block_lo = 0xffffffffu;
+        sh.block_hi = 0u;
+        sh.cut_bin = kBins - 1;
     }
     float2* line = lines + j * kRegLine;
     fft256<true>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
@@ -691,19 +685,19 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
         hi = max(hi, __shfl_xor_sync(kFull, hi, o));
     }
     for (int b = threadIdx.x; b < kBins; b += 256) {
-        hist[b] = 0;
+        sh.hist[b] = 0;
     }
     if (lane == 0 && lo <= hi) {
-        atomicMin(&block_lo, lo);
-        atomicMax(&block_hi, hi);
+        atomicMin(&sh.block_lo, lo);
+        atomicMax(&sh.block_hi, hi);
     }
     __syncthreads();
-    const unsigned int range_lo = block_lo;
-    if (range_lo > block_hi) {
-        return;  // no key in this block (uniform: every thread sees the same shared values)
+    const unsigned int range_lo = sh.block_lo;
+    if (range_lo > sh.block_hi) {
+        return;  // no key in these rows (uniform: every thread sees the same shared values)
     }
     int shift = 0;
-    while (shift < 32 && ((block_hi - range_lo) >> shift) >= static_cast<unsigned int>(kBins)) {
+    while (shift < 32 && ((sh.block_hi - range_lo) >> shift) >= static_cast<unsigned int>(kBins)) {
         ++shift;
     }
 #pragma unroll 1
@@ -712,7 +706,7 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
         if (valid && x < legal_x) {
             const unsigned long long key = row_keys[x];
             if (key != kEmptyKey) {
-                atomicAdd(&hist[(static_cast<unsigned int>(key >> 32) - range_lo) >> shift], 1u);
+                atomicAdd(&sh.hist[(static_cast<unsigned int>(key >> 32) - range_lo) >> shift], 1u);
             }
         }
     }
@@ -722,7 +716,7 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     unsigned int mine = 0;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-        mine += hist[4 * threadIdx.x + q];
+        mine += sh.hist[4 * threadIdx.x + q];
     }
     unsigned int inclusive = mine;
     for (int o = 1; o < 32; o <<= 1) {
@@ -733,28 +727,28 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     }
     const int warp = threadIdx.x >> 5;
     if (lane == 31) {
-        warp_sums[warp] = inclusive;
+        sh.warp_sums[warp] = inclusive;
     }
     __syncthreads();
     unsigned int before = 0, total = 0;
     for (int w = 0; w < 8; ++w) {
-        before += w < warp ? warp_sums[w] : 0u;
-        total += warp_sums[w];
+        before += w < warp ? sh.warp_sums[w] : 0u;
+        total += sh.warp_sums[w];
     }
     const unsigned int start = before + inclusive - mine;
     constexpr unsigned int kNeed = kExactPerOrientation;
     if (total >= kNeed && start < kNeed && start + mine >= kNeed) {
         unsigned int running = start;
         for (int q = 0; q < 4; ++q) {
-            running += hist[4 * threadIdx.x + q];
+            running += sh.hist[4 * threadIdx.x + q];
             if (running >= kNeed) {
-                cut_bin = 4 * threadIdx.x + q;
+                sh.cut_bin = 4 * threadIdx.x + q;
                 break;
             }
         }
     }
     __syncthreads();
-    const int cut = cut_bin;
+    const int cut = sh.cut_bin;
     if (threadIdx.x == 0) {
         unsigned long long b = *reinterpret_cast<volatile unsigned long long*>(tau);
         const unsigned long long edge = static_cast<unsigned long long>(range_lo) +
@@ -766,10 +760,10 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
             const unsigned long long old = atomicMin(tau, upper);
             b = old < upper ? old : upper;
         }
-        emit_bound = b;
+        sh.emit_bound = b;
     }
     __syncthreads();
-    const unsigned long long limit = emit_bound;
+    const unsigned long long limit = sh.emit_bound;
 #pragma unroll 1
     for (int m2 = 0; m2 < 16; ++m2) {
         const int x = t + 16 * m2;
@@ -793,6 +787,103 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
+                                                         int legal_y, int legal_z,
+                                                         const float2* __restrict__ twiddles,
+                                                         const double* __restrict__ t65, double inv_occ, int mode,
+                                                         double threshold, double cursor_floor,
+                                                         unsigned long long* __restrict__ keys,
+                                                         unsigned int* __restrict__ count, unsigned int cap,
+                                                         unsigned long long* __restrict__ tau,
+                                                         unsigned long long* __restrict__ resid)
+{
+    __shared__ float2 tw[256];
+    __shared__ float2 lines[16 * kRegLine];
+    __shared__ B2Shared sh;
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const int t = threadIdx.x & 15;
+    const int j = threadIdx.x >> 4;
+    const long long rows = static_cast<long long>(legal_y) * legal_z;
+    const long long row = static_cast<long long>(blockIdx.x) * 16 + j;
+    const bool valid = row < rows;
+    const int y = valid ? static_cast<int>(row % legal_y) : 0;
+    const int zz = valid ? static_cast<int>(row / legal_y) : 0;
+    const long long base = 256LL * (y + 256LL * zz);
+    float2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
+    }
+    b2_rows256(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, threshold, cursor_floor, keys,
+               count, cap, tau, resid);
+}
+
+// Passes B1 and B2 fused on 256^3 grids: one cluster of 8 CTAs per legal z
+// plane.  CTA c inverts along y the 32 columns kx = 32c..32c+31 of the plane
+// (read from HBM once) and keeps them in its shared memory; after a cluster
+// barrier each CTA gathers whole rows y = c, c + 8, ... from the 8 CTAs'
+// shared memory (distributed shared memory) and runs the inverse x
+// transform and the epilogue of pass B2 on them.  The legal-row
+// intermediate that B1 wrote and B2 read back never reaches HBM.
+constexpr int kFusedCluster = 8;
+constexpr std::size_t kFusedSmem = sizeof(float2) * (256 * 32 + 16 * kRegLine + 256) + sizeof(B2Shared);
+
+__global__ void __cluster_dims__(kFusedCluster, 1, 1) __launch_bounds__(256)
+    pass_b_fused_256_kernel(const float2* __restrict__ inter, int legal_x, int legal_y,
+                            const float2* __restrict__ twiddles, const double* __restrict__ t65, double inv_occ,
+                            int mode, double threshold, double cursor_floor, unsigned long long* __restrict__ keys,
+                            unsigned int* __restrict__ count, unsigned int cap, unsigned long long* __restrict__ tau,
+                            unsigned long long* __restrict__ resid)
+{
+    extern __shared__ __align__(16) unsigned char fused_smem[];
+    float2* cols = reinterpret_cast<float2*>(fused_smem);  // [y < 256][kx_local < 32]
+    float2* lines = cols + 256 * 32;
+    float2* tw = lines + 16 * kRegLine;
+    B2Shared& sh = *reinterpret_cast<B2Shared*>(tw + 256);
+    cg::cluster_group cluster = cg::this_cluster();
+    const unsigned int rank = cluster.block_rank();
+    const int zz = static_cast<int>(blockIdx.x / kFusedCluster);
+    tw[threadIdx.x] = twiddles[threadIdx.x];
+    __syncthreads();
+    const long long plane = 65536LL * zz;
+    // Inverse y of this CTA's 32 columns, 16 at a time (coalesced along kx).
+#pragma unroll 1
+    for (int r = 0; r < 2; ++r) {
+        const int j = threadIdx.x & 15, t = threadIdx.x >> 4;
+        const int kx_local = 16 * r + j;
+        const int kx = 32 * static_cast<int>(rank) + kx_local;
+        float2 v[16];
+#pragma unroll
+        for (int n1 = 0; n1 < 16; ++n1) {
+            v[n1] = inter[plane + 256LL * (16 * n1 + t) + kx];
+        }
+        fft256<true>(v, lines + j * kRegLine, t, tw);  // v[m2] = value at y = t + 16 m2
+#pragma unroll
+        for (int m2 = 0; m2 < 16; ++m2) {
+            cols[(t + 16 * m2) * 32 + kx_local] = v[m2];
+        }
+    }
+    cluster.sync();
+    // Rows y = rank + 8 i, gathered across the cluster: kx = 16 n1 + t lives
+    // in CTA n1 / 2 at local column 16 (n1 % 2) + t.
+#pragma unroll 1
+    for (int r = 0; r < 2; ++r) {
+        const int t = threadIdx.x & 15, j = threadIdx.x >> 4;
+        const int y = static_cast<int>(rank) + kFusedCluster * (16 * r + j);
+        const bool valid = y < legal_y;
+        float2 v[16];
+#pragma unroll
+        for (int n1 = 0; n1 < 16; ++n1) {
+            const float2* src = cluster.map_shared_rank(cols, n1 >> 1);
+            v[n1] = valid ? src[y * 32 + 16 * (n1 & 1) + t] : make_float2(0.f, 0.f);
+        }
+        b2_rows256(v, lines, tw, sh, valid, valid ? y : 0, zz, legal_x, legal_y, t65, inv_occ, mode, threshold,
+                   cursor_floor, keys, count, cap, tau, resid);
+    }
+    cluster.sync();  // no CTA leaves while another may still read its columns
 }
 
 // Bitonic sort of n <= capacity keys in shared memory (padded with kEmptyKey
@@ -969,6 +1060,12 @@ void allow_large_smem(Kernel k)
 }
 
 }  // namespace
+
+Pipeline::Pipeline(spk_context* ctx) : ctx_(ctx)
+{
+    const char* mode = std::getenv("SPK_PASS_B");
+    fused_b_ = !(mode && std::strcmp(mode, "split") == 0);
+}
 
 Pipeline::~Pipeline()
 {
@@ -1299,8 +1396,23 @@ int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double thre
         return status;
     }
     // Algorithmic bytes: B1 reads the legal-z planes and writes their legal
-    // rows; B2 reads those rows (its keys are a few KB).
+    // rows; B2 reads those rows (its keys are a few KB).  Fused, the planes
+    // are read once and nothing else crosses HBM.
     const double legal_rows = static_cast<double>(s.legal[1]) * s.legal[2];
+    if (fused_b_) {
+        static std::once_flag configured[64];
+        once_per_device(configured, [] {
+            cudaFuncSetAttribute(pass_b_fused_256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kFusedSmem));
+        });
+        auto ev = pass_begin(ctx_);
+        pass_b_fused_256_kernel<<<kFusedCluster * s.legal[2], 256, kFusedSmem, st>>>(
+            inter, s.legal[0], s.legal[1], tw1, s.t65, 1.0 / static_cast<double>(s.occupied), mode, threshold,
+            cursor_floor, keys, count, cap, tau, resid);
+        pass_end(ctx_, 2, ev, 8.0 * L_[0] * L_[1] * s.legal[2]);
+        ctx_->launches++;
+        return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+    }
     auto ev = pass_begin(ctx_);
     pass_b1_256_kernel<<<16 * s.legal[2], 256, 0, st>>>(inter, s.legal[1], tw1);
     pass_end(ctx_, 1, ev, 8.0 * L_[0] * L_[1] * s.legal[2] + 8.0 * L_[0] * legal_rows);

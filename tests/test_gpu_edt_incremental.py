@@ -44,9 +44,10 @@ def _fill_and_compare(gpu_ctx, wl, steps):
 
 
 def test_incremental_edt_blob128(gpu_ctx):
+    # The 63 mm box holds about 30 copies of this blob in 8 orientations.
     wl = package("workloads").box63_blob_hopf96()
     wl.catalog = wl.catalog[:8]
-    assert _fill_and_compare(gpu_ctx, wl, 60) >= 50
+    assert _fill_and_compare(gpu_ctx, wl, 60) >= 25
 
 
 def test_incremental_edt_cuboid66(gpu_ctx):
@@ -56,4 +57,4 @@ def test_incremental_edt_cuboid66(gpu_ctx):
 
 def test_incremental_edt_rounded256(gpu_ctx):
     wl = package("workloads").rounded256_blob_hopf512(orientations=8)
-    assert _fill_and_compare(gpu_ctx, wl, 20) == 20
+    assert _fill_and_compare(gpu_ctx, wl, 60) == 60
