@@ -1064,7 +1064,7 @@ void allow_large_smem(Kernel k)
 Pipeline::Pipeline(spk_context* ctx) : ctx_(ctx)
 {
     const char* mode = std::getenv("SPK_PASS_B");
-    fused_b_ = !(mode && std::strcmp(mode, "split") == 0);
+    fused_b_ = mode && std::strcmp(mode, "fused") == 0;
 }
 
 Pipeline::~Pipeline()

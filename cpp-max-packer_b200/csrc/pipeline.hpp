@@ -144,7 +144,7 @@ private:
     float2* spectrum_ {};
     float2* inter_ {};
     std::size_t inter_bytes_ {};
-    bool fused_b_ { true };  // 256^3: passes B1 and B2 as one cluster kernel (SPK_PASS_B=split: two passes)
+    bool fused_b_ {};  // 256^3: passes B1 and B2 as one cluster kernel (SPK_PASS_B=fused), else two passes
     const double* table_ {};
     double z_norm_ {};  // sqrt(sum over cells of b^2 + p^2)
     std::vector<KernelSlot> slots_;
