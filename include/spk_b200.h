@@ -190,7 +190,10 @@ int spk_build_proximity(spk_context* context, const uint32_t shape[3], const uin
  * are rejected with SPK_SCRATCH_LIMIT (status 25).  The first call on a device looks up the array's address
  * and uploads the table (synchronising `stream`); make that first call before
  * any stream capture.  All calls share the array: calls that overlap on the
- * GPU (concurrent streams) race, so serialise them. */
+ * GPU (concurrent streams) race, so serialise them.  The looked-up address is
+ * kept per device index for the life of the process and does not survive a
+ * reset of the device's context (cudaDeviceReset): do not call this again
+ * after one. */
 int spk_build_proximity_static(void* stream, const uint32_t shape[3], const uint8_t* occupied, double* values);
 
 /* ---- spectral pages ---------------------------------------------------- */
