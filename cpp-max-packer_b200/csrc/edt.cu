@@ -398,18 +398,20 @@ __global__ void edt_region_kernel(const std::int32_t* __restrict__ tile_max, int
     }
 }
 
-// First pass of the new sites' EDT over the region: along x, the squared
-// distance to the nearest site on the same line (a left and a right sweep).
+// First pass of the new sites' EDT: along x, over the region's x range, the
+// squared distance to the nearest site on the same line (a left and a right
+// sweep).  Only lines through the sites' box hold sites; every other line of
+// the region is infinite and is never read.
 __global__ void edt_region_x_kernel(const std::uint8_t* __restrict__ sites, std::int32_t* __restrict__ tmp, int sx,
-                                    int sy, const EdtBox* __restrict__ region)
+                                    int sy, EdtBox b, const EdtBox* __restrict__ region)
 {
     const EdtBox r = *region;
-    const int ny = r.hi[1] - r.lo[1], nz = r.hi[2] - r.lo[2];
+    const int ny = b.hi[1] - b.lo[1], nz = b.hi[2] - b.lo[2];
     const long long line = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
     if (line >= static_cast<long long>(ny) * nz) {
         return;
     }
-    const int y = r.lo[1] + static_cast<int>(line % ny), z = r.lo[2] + static_cast<int>(line / ny);
+    const int y = b.lo[1] + static_cast<int>(line % ny), z = b.lo[2] + static_cast<int>(line / ny);
     const long long base = static_cast<long long>(sx) * (y + static_cast<long long>(sy) * z);
     constexpr int kFar = 1 << 24;
     int last = -kFar;
@@ -429,35 +431,43 @@ __global__ void edt_region_x_kernel(const std::uint8_t* __restrict__ sites, std:
     }
 }
 
-// Later passes over the region, along `axis` (1: y, 2: z): one thread per
-// line builds the lower envelope of the line's parabolas in shared memory
-// (f, site, first cell it wins: the integer rule of the full passes above)
-// and evaluates it; the last pass takes min with the old d2.
+// Later passes, along `axis` (1: y, 2: z): one thread per line builds the
+// lower envelope of the line's parabolas in shared memory (f, site, first
+// cell it wins: the integer rule of the full passes above) and evaluates it
+// over the region's extent; the last pass takes min with the old d2.  A line
+// holds finite values only inside the sites' box along its axis, so only
+// those cells are read.  The y pass covers the lines (x in the region,
+// z in the sites' box), which are all the z pass reads; the z pass covers
+// every (x, y) of the region.
 __global__ void __launch_bounds__(32) edt_region_envelope_kernel(std::int32_t* __restrict__ tmp,
                                                                 std::int32_t* __restrict__ d2, int sx, int sy,
-                                                                int axis, int last, int max_length,
+                                                                int axis, int last, int max_sites, EdtBox b,
                                                                 const EdtBox* __restrict__ region)
 {
     extern __shared__ __align__(16) unsigned char stack_raw[];
-    std::int32_t* sf = reinterpret_cast<std::int32_t*>(stack_raw);            // [max_length][32]
-    std::int16_t* sq = reinterpret_cast<std::int16_t*>(sf + max_length * 32);  // [max_length][32]
-    std::int16_t* ss = sq + max_length * 32;                                   // [max_length][32]
+    std::int32_t* sf = reinterpret_cast<std::int32_t*>(stack_raw);           // [max_sites][32]
+    std::int16_t* sq = reinterpret_cast<std::int16_t*>(sf + max_sites * 32);  // [max_sites][32]
+    std::int16_t* ss = sq + max_sites * 32;                                   // [max_sites][32]
     const EdtBox r = *region;
     const int lane = threadIdx.x;
     const int length = r.hi[axis] - r.lo[axis];
     const int other = axis == 1 ? 2 : 1;  // the second line coordinate; x is the first
-    const int n0 = r.hi[0] - r.lo[0], n1 = r.hi[other] - r.lo[other];
+    const int w0 = axis == 1 ? b.lo[2] : r.lo[1];
+    const int n0 = r.hi[0] - r.lo[0], n1 = axis == 1 ? b.hi[2] - b.lo[2] : r.hi[1] - r.lo[1];
     const long long line = static_cast<long long>(blockIdx.x) * 32 + lane;
     if (line >= static_cast<long long>(n0) * n1) {
         return;
     }
     const int x = r.lo[0] + static_cast<int>(line % n0);
-    const int w = r.lo[other] + static_cast<int>(line / n0);
+    const int w = w0 + static_cast<int>(line / n0);
+    (void)other;
     const long long plane = static_cast<long long>(sx) * sy;
     const long long stride = axis == 1 ? sx : plane;
     const long long base = x + (axis == 1 ? plane * w : static_cast<long long>(sx) * w) + stride * r.lo[axis];
+    // Sites along this axis lie in [b.lo, b.hi), as offsets from the region's start.
+    const int q_first = b.lo[axis] - r.lo[axis], q_end = b.hi[axis] - r.lo[axis];
     int count = 0;
-    for (int q = 0; q < length; ++q) {
+    for (int q = q_first; q < q_end; ++q) {
         const std::int32_t f = tmp[base + q * stride];
         if (f == kInf) {
             continue;
@@ -548,7 +558,7 @@ int edt_add_sites(spk_context* ctx, const std::uint8_t* d_sites, const EdtBox& s
     const int tx = (sx + kEdtTile - 1) / kEdtTile, ty = (sy + kEdtTile - 1) / kEdtTile,
               tz = (sz + kEdtTile - 1) / kEdtTile;
     const long long tiles = static_cast<long long>(tx) * ty * tz;
-    const int longest = std::max(sy, sz);
+    const int longest = std::max(box.hi[1] - box.lo[1], box.hi[2] - box.lo[2]);
     if (static_cast<long long>(longest) * 32 * 8 > 227LL * 1024) {
         return kInvalidArgument;
     }
@@ -558,13 +568,14 @@ int edt_add_sites(spk_context* ctx, const std::uint8_t* d_sites, const EdtBox& s
     });
     edt_region_init_kernel<<<1, 32, 0, stream>>>(box, region);
     edt_region_kernel<<<blocks_for(tiles, 256), 256, 0, stream>>>(d_tile_max, sx, sy, sz, tx, ty, tz, box, region);
-    edt_region_x_kernel<<<static_cast<unsigned>((static_cast<long long>(sy) * sz + 127) / 128), 128, 0, stream>>>(
-        d_sites, tmp, sx, sy, region);
-    edt_region_envelope_kernel<<<static_cast<unsigned>((static_cast<long long>(sx) * sz + 31) / 32), 32,
-                                 static_cast<std::size_t>(sy) * 32 * 8, stream>>>(tmp, d_d2, sx, sy, 1, 0, sy,
+    const int by = box.hi[1] - box.lo[1], bz = box.hi[2] - box.lo[2];
+    edt_region_x_kernel<<<static_cast<unsigned>((static_cast<long long>(by) * bz + 127) / 128), 128, 0, stream>>>(
+        d_sites, tmp, sx, sy, box, region);
+    edt_region_envelope_kernel<<<static_cast<unsigned>((static_cast<long long>(sx) * bz + 31) / 32), 32,
+                                 static_cast<std::size_t>(by) * 32 * 8, stream>>>(tmp, d_d2, sx, sy, 1, 0, by, box,
                                                                                   region);
     edt_region_envelope_kernel<<<static_cast<unsigned>((static_cast<long long>(sx) * sy + 31) / 32), 32,
-                                 static_cast<std::size_t>(sz) * 32 * 8, stream>>>(tmp, d_d2, sx, sy, 2, 1, sz,
+                                 static_cast<std::size_t>(bz) * 32 * 8, stream>>>(tmp, d_d2, sx, sy, 2, 1, bz, box,
                                                                                   region);
     edt_tile_max_kernel<<<static_cast<unsigned>(tiles), 64, 0, stream>>>(d_d2, sx, sy, sz, tx, ty, d_tile_max,
                                                                           region);

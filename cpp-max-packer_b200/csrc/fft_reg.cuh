@@ -111,4 +111,33 @@ __device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, con
     dft16<INV>(v);  // thread t: X[t + 16 k2] = v[k2]
 }
 
+// The forward transform of a line whose inputs are zero beyond index 31:
+// thread t holds x[t] in a and x[16 + t] in b.  The first 16-point DFT over
+// n1 then has two non-zero terms, Y[k1] = a + b w16^k1; the rest is the
+// four-step transform above.  Output distribution as fft256.
+__device__ __forceinline__ void fft256_first32(float2 a, float2 b, float2 (&v)[16], float2* line, int t,
+                                               const float2* __restrict__ tw)
+{
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+        const float2 w = tw[16 * k1];  // w16^k1 = w256^(16 k1)
+        v[k1] = make_float2(a.x + b.x * w.x - b.y * w.y, a.y + b.x * w.y + b.y * w.x);
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) {
+        v[k1] = cmulf(v[k1], tw[(t * k1) & 255]);
+    }
+    __syncthreads();  // the previous reader of `line` is done
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) {
+        line[t * 17 + k1] = v[k1];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int n2 = 0; n2 < 16; ++n2) {
+        v[n2] = line[n2 * 17 + t];
+    }
+    dft16<false>(v);  // thread t: X[t + 16 k2] = v[k2]
+}
+
 }  // namespace spk

@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
 // inverts along z.  The spectrum (134 MB at 256^3) then crosses HBM once per
 // batch instead of once per orientation.  The next orientation's kernel
 // planes are fetched before the current one's transforms.
-__global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
+__global__ void __launch_bounds__(256, 3) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
                                                              const PassABatch batch,
                                                              const float2* __restrict__ twiddles)
 {
@@ -436,19 +436,25 @@ __global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __re
     for (int g = 0; g < batch.count; ++g) {
         const PassASlot s = batch.slot[g];
         float2 v[16];
-        v[0] = next0;
-        v[1] = next1;
-#pragma unroll
-        for (int n1 = 2; n1 < 16; ++n1) {
-            const int z = 16 * n1 + t;
-            v[n1] = z < s.K2 ? s.partial[col + plane * z] : make_float2(0.f, 0.f);
-        }
+        const float2 first = next0, second = next1;
         if (g + 1 < batch.count) {
             const PassASlot& sn = batch.slot[g + 1];
             next0 = t < sn.K2 ? sn.partial[col + plane * t] : make_float2(0.f, 0.f);
             next1 = 16 + t < sn.K2 ? sn.partial[col + plane * (16 + t)] : make_float2(0.f, 0.f);
         }
-        fft256<false>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
+        if (s.K2 <= 32) {
+            fft256_first32(first, second, v, line, t, tw);  // v[k2] = K^(t + 16 k2)
+        }
+        else {
+            v[0] = first;
+            v[1] = second;
+#pragma unroll
+            for (int n1 = 2; n1 < 16; ++n1) {
+                const int z = 16 * n1 + t;
+                v[n1] = z < s.K2 ? s.partial[col + plane * z] : make_float2(0.f, 0.f);
+            }
+            fft256<false>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
+        }
 #pragma unroll
         for (int k2 = 0; k2 < 16; ++k2) {
             const float2 sv = sp[k2];
@@ -589,7 +595,7 @@ struct B2Shared {
 // Thread (row j = threadIdx / 16, lane t = threadIdx % 16) holds in v[n1]
 // its row's value at kx = 16 n1 + t; `valid` rows are (y, zz).  Every thread
 // of the block calls it; it may be called again for the next 16 rows.
-__device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+__device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
                                            bool valid, int y, int zz, int legal_x, int legal_y,
                                            const double* __restrict__ t65, double inv_occ, int mode,
                                            double threshold, double cursor_floor,
@@ -789,7 +795,195 @@ __device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const
     }
 }
 
-__global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
+// Mode 0 of the epilogue above with the values kept in registers: every
+// cell gets the residual check and two FP32 compares, and only cells that
+// pass them (below the prefilter's bound) get an FP64 score and a key slot
+// in shared memory; `present` marks those slots, so the histogram and the
+// emission visit only them.  Same keys, same emission rule as the generic
+// path.
+__device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+                                                  bool valid, int y, int zz, int legal_x, int legal_y,
+                                                  const double* __restrict__ t65, double inv_occ,
+                                                  double cursor_floor, unsigned long long* __restrict__ keys,
+                                                  unsigned int* __restrict__ count, unsigned int cap,
+                                                  unsigned long long* __restrict__ tau,
+                                                  unsigned long long* __restrict__ resid)
+{
+    constexpr int kBins = 1024;
+    const int t = threadIdx.x & 15;  // lane within the row (coalesced direction)
+    const int j = threadIdx.x >> 4;  // row within the block
+    const int lane = threadIdx.x & 31;
+    __syncthreads();  // the previous rows' readers of `sh` are done
+    if (threadIdx.x == 0) {
+        sh.block_lo = 0xffffffffu;
+        sh.block_hi = 0u;
+        sh.cut_bin = kBins - 1;
+    }
+    float2* line = lines + j * kRegLine;
+    fft256<true>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
+    auto* row_keys = reinterpret_cast<unsigned long long*>(line);
+    const double t65z = valid ? t65[zz] : 0.0;
+    const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
+    // Keys above the request's pruning bound cannot enter its top 64.
+    const unsigned long long bound = *reinterpret_cast<volatile unsigned long long*>(tau);
+    const float skip = valid ? skip_below(bound, t65z, inv_occ) : -INFINITY;
+    float residual = 0.f;
+    unsigned int lo = 0xffffffffu, hi = 0u, present = 0u;
+    __syncthreads();  // the transform's reads of `line` are done before keys overwrite it
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int x = t + 16 * m2;
+        const float2 w = v[m2];
+        if (valid && x < legal_x) {
+            residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
+            if (fabsf(w.x) < 0.5f && !(w.y < skip)) {
+                const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
+                if (score >= cursor_floor) {
+                    const unsigned long long key = make_key(score, row_index + x);
+                    if (key <= bound) {
+                        row_keys[x] = key;
+                        present |= 1u << m2;
+                        const unsigned int h = static_cast<unsigned int>(key >> 32);
+                        lo = min(lo, h);
+                        hi = max(hi, h);
+                    }
+                }
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        residual = fmaxf(residual, __shfl_xor_sync(kFull, residual, o));
+    }
+    if (lane == 0 && residual > 0.f) {
+        atomicMax(resid, static_cast<unsigned long long>(__float_as_uint(residual)));
+    }
+    // Block range of the keys' high words, then the histogram over it.
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+    }
+    for (int b = threadIdx.x; b < kBins; b += 256) {
+        sh.hist[b] = 0;
+    }
+    if (lane == 0 && lo <= hi) {
+        atomicMin(&sh.block_lo, lo);
+        atomicMax(&sh.block_hi, hi);
+    }
+    __syncthreads();
+    const unsigned int range_lo = sh.block_lo;
+    if (range_lo > sh.block_hi) {
+        return;  // no key in these rows (uniform: every thread sees the same shared values)
+    }
+    int shift = 0;
+    while (shift < 32 && ((sh.block_hi - range_lo) >> shift) >= static_cast<unsigned int>(kBins)) {
+        ++shift;
+    }
+    for (unsigned int bits = present; bits; bits &= bits - 1) {
+        const int m2 = __ffs(bits) - 1;
+        const unsigned long long key = row_keys[t + 16 * m2];
+        atomicAdd(&sh.hist[(static_cast<unsigned int>(key >> 32) - range_lo) >> shift], 1u);
+    }
+    __syncthreads();
+    // First bin at which 64 keys have accumulated: each thread sums four
+    // consecutive bins, a block scan of those sums locates the crossing.
+    unsigned int mine = 0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        mine += sh.hist[4 * threadIdx.x + q];
+    }
+    unsigned int inclusive = mine;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int other = __shfl_up_sync(kFull, inclusive, o);
+        if (lane >= o) {
+            inclusive += other;
+        }
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane == 31) {
+        sh.warp_sums[warp] = inclusive;
+    }
+    __syncthreads();
+    unsigned int before = 0, total = 0;
+    for (int w = 0; w < 8; ++w) {
+        before += w < warp ? sh.warp_sums[w] : 0u;
+        total += sh.warp_sums[w];
+    }
+    const unsigned int start = before + inclusive - mine;
+    constexpr unsigned int kNeed = kExactPerOrientation;
+    if (total >= kNeed && start < kNeed && start + mine >= kNeed) {
+        unsigned int running = start;
+        for (int q = 0; q < 4; ++q) {
+            running += sh.hist[4 * threadIdx.x + q];
+            if (running >= kNeed) {
+                sh.cut_bin = 4 * threadIdx.x + q;
+                break;
+            }
+        }
+    }
+    __syncthreads();
+    const int cut = sh.cut_bin;
+    if (threadIdx.x == 0) {
+        unsigned long long b = *reinterpret_cast<volatile unsigned long long*>(tau);
+        const unsigned long long edge = static_cast<unsigned long long>(range_lo) +
+                                        (static_cast<unsigned long long>(cut + 1) << shift);
+        if (total >= kNeed && edge <= 0xffffffffULL) {
+            // Every key of bins <= cut is below (edge << 32): an upper bound of
+            // this block's 64th smallest key, hence of the request's.
+            const unsigned long long upper = (edge << 32) - 1;
+            const unsigned long long old = atomicMin(tau, upper);
+            b = old < upper ? old : upper;
+        }
+        sh.emit_bound = b;
+    }
+    __syncthreads();
+    const unsigned long long limit = sh.emit_bound;
+    // Slots any lane of the warp holds, visited together by the whole warp.
+    const unsigned int warp_present = __reduce_or_sync(kFull, present);
+    for (unsigned int bits = warp_present; bits; bits &= bits - 1) {
+        const int m2 = __ffs(bits) - 1;
+        bool take = false;
+        unsigned long long key = kEmptyKey;
+        if ((present >> m2) & 1u) {
+            key = row_keys[t + 16 * m2];
+            take = key <= limit &&
+                   static_cast<int>((static_cast<unsigned int>(key >> 32) - range_lo) >> shift) <= cut;
+        }
+        const unsigned mask = __ballot_sync(kFull, take);
+        if (mask) {
+            unsigned int slot = 0;
+            if (lane == 0) {
+                slot = atomicAdd(count, static_cast<unsigned int>(__popc(mask)));
+            }
+            slot = __shfl_sync(kFull, slot, 0);
+            const unsigned int rank = __popc(mask & ((1u << lane) - 1u));
+            if (take && slot + rank < cap) {
+                keys[slot + rank] = key;
+            }
+        }
+    }
+}
+
+// Mode 0 (first pass) takes the register path, mode 1 (threshold pass) the
+// generic one.
+__device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+                                           bool valid, int y, int zz, int legal_x, int legal_y,
+                                           const double* __restrict__ t65, double inv_occ, int mode,
+                                           double threshold, double cursor_floor,
+                                           unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
+                                           unsigned int cap, unsigned long long* __restrict__ tau,
+                                           unsigned long long* __restrict__ resid)
+{
+    if (mode == 0) {
+        b2_rows256_select(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, cursor_floor, keys, count,
+                          cap, tau, resid);
+    }
+    else {
+        b2_rows256_generic(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, threshold,
+                           cursor_floor, keys, count, cap, tau, resid);
+    }
+}
+
+__global__ void __launch_bounds__(256, 4) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
                                                          int legal_y, int legal_z,
                                                          const float2* __restrict__ twiddles,
                                                          const double* __restrict__ t65, double inv_occ, int mode,
