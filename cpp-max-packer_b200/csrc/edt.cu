@@ -75,7 +75,7 @@ __global__ void edt_pass_kernel(std::int32_t* __restrict__ d2, std::int32_t* __r
             const long long numerator =
                 static_cast<long long>(f) - static_cast<long long>(line_f[base + p * stride]) + 1LL * q * q - p * p;
             const long long denominator = 2LL * (q - p);
-            // Floor division, then the first integer where q is strictly nearer.
+            // The intersection of the two parabolas, rounded down: from one past it on, site q wins.
             long long quotient = numerator / denominator;
             if ((numerator % denominator != 0) && ((numerator < 0) != (denominator < 0))) {
                 --quotient;

@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
 // inverts along z.  The spectrum (134 MB at 256^3) then crosses HBM once per
 // batch instead of once per orientation.  The next orientation's kernel
 // planes are fetched before the current one's transforms.
-__global__ void __launch_bounds__(256, 3) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
+__global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
                                                              const PassABatch batch,
                                                              const float2* __restrict__ twiddles)
 {
@@ -983,7 +983,7 @@ __device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const
     }
 }
 
-__global__ void __launch_bounds__(256, 4) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
+__global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
                                                          int legal_y, int legal_z,
                                                          const float2* __restrict__ twiddles,
                                                          const double* __restrict__ t65, double inv_occ, int mode,
