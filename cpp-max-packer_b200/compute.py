@@ -216,6 +216,15 @@ def _field_failure(es, ks, env, ker, control=None) -> Optional[CorrelationFailur
     return None
 
 
+def _message(context) -> str:
+    """The reference's message for the failing site (spk_context_message)."""
+    f = lib().spk_context_message
+    f.restype = ctypes.c_char_p
+    f.argtypes = [ctypes.c_void_p]
+    raw = f(context.handle)
+    return raw.decode() if raw else ""
+
+
 def _correlate(name, spec, environment, kernel, limits, control, precision, context, env_dtype):
     limits = limits or CorrelationLimits()
     es = [int(v) for v in spec.environment_shape]
@@ -241,7 +250,7 @@ def _correlate(name, spec, environment, kernel, limits, control, precision, cont
         code = _lib.status_code(status)
         if code in ("CUDA_RUNTIME_ERROR", "SPK_INVALID_ARGUMENT"):
             raise SpkError(status, code, name)
-        return CorrelationFailure(code, _MESSAGES.get(code, code), stats)
+        return CorrelationFailure(code, _message(context) or _MESSAGES.get(code, code), stats)
     return CorrelationResult(tuple(res.translation_first), tuple(res.shape), out[:count],
                              NumericReport(res.max_integer_residual, res.mass_residual, res.max_probe_error), stats,
                              tuple(res.padded_shape))

@@ -79,9 +79,9 @@ __global__ void spectrum_product_kernel(const cplx_t<T>* __restrict__ z, cplx_t<
         const long long r = i / g.L[0];
         const int y = static_cast<int>(r % g.L[1]);
         const int zz = static_cast<int>(r / g.L[1]);
-        const int mx = (g.L[0] - x) & (g.L[0] - 1);
-        const int my = (g.L[1] - y) & (g.L[1] - 1);
-        const int mz = (g.L[2] - zz) & (g.L[2] - 1);
+        const int mx = x == 0 ? 0 : g.L[0] - x;
+        const int my = y == 0 ? 0 : g.L[1] - y;
+        const int mz = zz == 0 ? 0 : g.L[2] - zz;
         const C a = z[i];
         const C b = cconj(z[mx + static_cast<long long>(g.L[0]) * (my + static_cast<long long>(g.L[1]) * mz)]);
         const C e = cscale(cadd(a, b), static_cast<T>(0.5));
@@ -111,9 +111,9 @@ __global__ void spectrum_product_half_kernel(const __half2* __restrict__ zh, flo
         const long long r = i / g.L[0];
         const int y = static_cast<int>(r % g.L[1]);
         const int zz = static_cast<int>(r / g.L[1]);
-        const int mx = (g.L[0] - x) & (g.L[0] - 1);
-        const int my = (g.L[1] - y) & (g.L[1] - 1);
-        const int mz = (g.L[2] - zz) & (g.L[2] - 1);
+        const int mx = x == 0 ? 0 : g.L[0] - x;
+        const int my = y == 0 ? 0 : g.L[1] - y;
+        const int mz = zz == 0 ? 0 : g.L[2] - zz;
         const float2 a0 = __half22float2(zh[i]);
         const float2 b0 = __half22float2(zh[mx + static_cast<long long>(g.L[0]) * (my + static_cast<long long>(g.L[1]) * mz)]);
         const float2 a = make_float2(a0.x * unscale, a0.y * unscale);
@@ -123,6 +123,12 @@ __global__ void spectrum_product_half_kernel(const __half2* __restrict__ zh, flo
         const float2 k = make_float2(d.y * 0.5f, -d.x * 0.5f);
         w[i] = cmulconj(e, k);
     }
+}
+
+// v mod L for v in (-L, 2L).
+__device__ __forceinline__ int wrap(int v, int L)
+{
+    return v < 0 ? v + L : v >= L ? v - L : v;
 }
 
 struct ExtractStats {
@@ -154,9 +160,10 @@ __global__ void extract_kernel(const cplx_t<T>* __restrict__ w, Grid g, int ox, 
         const long long r = i / ox;
         const int y = static_cast<int>(r % oy);
         const int z = static_cast<int>(r / oy);
-        const int sx = (x - (kx - 1)) & (g.L[0] - 1);
-        const int sy = (y - (ky - 1)) & (g.L[1] - 1);
-        const int sz = (z - (kz - 1)) & (g.L[2] - 1);
+        // The output's cell on the transform grid, wrapped into [0, L).
+        const int sx = wrap(x - (kx - 1), g.L[0]);
+        const int sy = wrap(y - (ky - 1), g.L[1]);
+        const int sz = wrap(z - (kz - 1), g.L[2]);
         const cplx_t<T> v = w[sx + static_cast<long long>(g.L[0]) * (sy + static_cast<long long>(g.L[1]) * sz)];
         const double value = static_cast<double>(v.x);
         const double imag = static_cast<double>(v.y);
@@ -441,8 +448,8 @@ int correlate(spk_context* ctx, const spk_correlation_spec* spec_ptr, const E* e
     }
     Grid g;
     for (int a = 0; a != 3; ++a) {
-        const std::uint32_t L = next_pow2(padded[a]);
-        if (L > static_cast<std::uint32_t>(kMaxFftLength)) {
+        const std::uint32_t L = transform_length(padded[a]);
+        if (L == 0) {
             return fail(ctx, kUnsupportedLength, "Padded extent exceeds the device FFT's longest axis.");
         }
         g.L[a] = static_cast<int>(L);
@@ -682,8 +689,8 @@ int spk_estimate_correlation(const spk_correlation_spec* spec, uint32_t precisio
             !checked_mul(padded_cells, length, padded_cells)) {
             return kShapeOverflow;
         }
-        const std::uint32_t L = next_pow2(length);
-        if (L > static_cast<std::uint32_t>(kMaxFftLength)) {
+        const std::uint32_t L = transform_length(length);
+        if (L == 0) {
             return kUnsupportedLength;
         }
         out->padded_shape[a] = L;

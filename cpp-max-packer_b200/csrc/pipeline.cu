@@ -1270,6 +1270,164 @@ Pipeline::~Pipeline()
     }
 }
 
+// ---- transform-length autotuner --------------------------------------------
+//
+// A window of E cells per axis needs a circular transform of any length
+// L >= E (legal translations never wrap).  The candidates are the supported
+// 2^a 3^b 5^c lengths from max(E, 16) to the next power of two; the x axis
+// also needs a multiple of 16 (pass A's column groups).  Each candidate's cost
+// per transformed point is measured once per device and axis (fft_axis on a
+// scratch grid, the fastest of three timed runs after a warm-up); the register
+// four-step path, used when every axis is 256, is measured the same way on
+// its own column kernel.  The chosen lengths minimise the modelled page cost,
+// points x the sum of the three axes' per-point costs.
+namespace {
+
+std::mutex g_tune_mutex;
+std::map<std::tuple<int, int, int>, double> g_tune_cost;  // (device, axis or -1 for the 256 path, L) -> ns/point
+
+std::vector<int> length_candidates(int E, int axis)
+{
+    const int lo = std::max(E, 16);
+    const int hi = static_cast<int>(next_pow2(static_cast<std::uint32_t>(lo)));
+    std::vector<int> out;
+    for (int L = lo; L <= hi && L <= kMaxFftLength; ++L) {
+        if (fft_length_supported(static_cast<std::uint64_t>(L)) && (axis != 0 || L % 16 == 0)) {
+            out.push_back(L);
+        }
+    }
+    return out;
+}
+
+// Nanoseconds per point of one transform pass, measured on `scratch`
+// (512 x 64 x 64 complex values).
+double measure_pass(spk_context* ctx, int axis, int L, float2* scratch, int& status)
+{
+    cudaStream_t st = ctx->stream;
+    const auto* tw = twiddle_table<float>(ctx, L, status);
+    if (!tw) {
+        return -1.0;
+    }
+    int shape[3] = { 64, 64, 64 };
+    long long points = 0;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(a, st);
+        if (axis < 0) {
+            // The register four-step path: the y pass of env_column256_kernel
+            // over 256 x 256 x 16 values.
+            env_column256_kernel<<<16 * 16, 256, 0, st>>>(scratch, 256, 65536, 1.f, tw);
+            points = 256LL * 256 * 16;
+        }
+        else {
+            shape[axis] = L;
+            fft_axis<float>(scratch, shape[0], shape[1], shape[2], axis, false, 1.f, tw, st);
+            points = static_cast<long long>(shape[0]) * shape[1] * shape[2];
+        }
+        cudaEventRecord(b, st);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0) {
+            best = std::min(best, ms);
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ctx->launches += 4;
+    if (cudaGetLastError() != cudaSuccess) {
+        status = kCuda;
+        return -1.0;
+    }
+    return 1e6 * static_cast<double>(best) / static_cast<double>(points);
+}
+
+double pass_cost(spk_context* ctx, int axis, int L, float2*& scratch, int& status)
+{
+    int device = 0;
+    cudaGetDevice(&device);
+    const auto key = std::make_tuple(device, axis, L);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        const auto it = g_tune_cost.find(key);
+        if (it != g_tune_cost.end()) {
+            return it->second;
+        }
+    }
+    if (!scratch) {
+        // Large enough for 512 x 64 x 64 (any axis) and 256 x 256 x 16 values.
+        const std::size_t bytes = sizeof(float2) * 512ULL * 64 * 64;
+        scratch = static_cast<float2*>(device_buffer(ctx, "tune.scratch", bytes, status));
+        if (!scratch) {
+            return -1.0;
+        }
+        cudaMemsetAsync(scratch, 0, bytes, ctx->stream);
+    }
+    const double cost = measure_pass(ctx, axis, L, scratch, status);
+    if (cost >= 0) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        g_tune_cost[key] = cost;
+    }
+    return cost;
+}
+
+}  // namespace
+
+int Pipeline::choose_lengths(const std::uint32_t* env_shape)
+{
+    std::vector<int> cand[3];
+    for (int a = 0; a < 3; ++a) {
+        cand[a] = length_candidates(static_cast<int>(env_shape[a]), a);
+        if (cand[a].empty()) {
+            return kUnsupportedLength;
+        }
+    }
+    if (cand[0].size() == 1 && cand[1].size() == 1 && cand[2].size() == 1) {
+        for (int a = 0; a < 3; ++a) {
+            L_[a] = cand[a][0];
+        }
+        return kOk;
+    }
+    int status = kOk;
+    float2* scratch = nullptr;
+    double best = INFINITY;
+    std::vector<double> cost[3];
+    for (int a = 0; a < 3; ++a) {
+        for (int L : cand[a]) {
+            const double c = pass_cost(ctx_, a, L, scratch, status);
+            if (c < 0) {
+                return status ? status : kCuda;
+            }
+            cost[a].push_back(c);
+        }
+    }
+    for (std::size_t i = 0; i < cand[0].size(); ++i) {
+        for (std::size_t j = 0; j < cand[1].size(); ++j) {
+            for (std::size_t k = 0; k < cand[2].size(); ++k) {
+                const double points = static_cast<double>(cand[0][i]) * cand[1][j] * cand[2][k];
+                double model = points * (cost[0][i] + cost[1][j] + cost[2][k]);
+                if (cand[0][i] == 256 && cand[1][j] == 256 && cand[2][k] == 256) {
+                    const double reg = pass_cost(ctx_, -1, 256, scratch, status);
+                    if (reg < 0) {
+                        return status ? status : kCuda;
+                    }
+                    model = points * 3 * reg;
+                }
+                if (model < best) {
+                    best = model;
+                    L_[0] = cand[0][i];
+                    L_[1] = cand[1][j];
+                    L_[2] = cand[2][k];
+                }
+            }
+        }
+    }
+    return kOk;
+}
+
 int Pipeline::set_geometry(const std::int64_t* env_first, const std::uint32_t* env_shape, const double* origin,
                            double pitch, double container_min_z, double container_height)
 {
@@ -1278,13 +1436,20 @@ int Pipeline::set_geometry(const std::int64_t* env_first, const std::uint32_t* e
             return kInvalidArgument;
         }
         E_[a] = static_cast<int>(env_shape[a]);
-        const std::uint32_t L = next_pow2(std::max<std::uint32_t>(env_shape[a], 16));
-        if (L > static_cast<std::uint32_t>(kMaxFftLength)) {
-            return kUnsupportedLength;
-        }
-        L_[a] = static_cast<int>(L);
         env_first_[a] = env_first[a];
         origin_[a] = origin[a];
+    }
+    if (const char* fixed = std::getenv("SPK_FFT_LENGTHS"); fixed && std::strcmp(fixed, "pow2") == 0) {
+        for (int a = 0; a != 3; ++a) {
+            const std::uint32_t L = next_pow2(std::max<std::uint32_t>(env_shape[a], 16));
+            if (L > static_cast<std::uint32_t>(kMaxFftLength)) {
+                return kUnsupportedLength;
+            }
+            L_[a] = static_cast<int>(L);
+        }
+    }
+    else if (int status = choose_lengths(env_shape)) {
+        return status;
     }
     pitch_ = pitch;
     cmin_z_ = container_min_z;

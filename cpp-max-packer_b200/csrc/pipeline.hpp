@@ -124,6 +124,8 @@ private:
                  unsigned long long* resid);
     double pass_a_bytes(const KernelSlot& s) const;
     int update_spectrum();
+    // Transform lengths per axis for the window (the autotuner); sets L_.
+    int choose_lengths(const std::uint32_t* env_shape);
     // Pass A for up to kPassABatch orientations in one launch (256^3 grids);
     // orientation i's legal-z intermediate goes to inter[i].
     int run_a256_batch(const KernelSlot* const* slots, int count, float2* const* inter);
