@@ -37,5 +37,6 @@ def test_status_codes_map_to_reference_strings():
 def test_estimate_is_host_only():
     compute = package("compute")
     est = compute.estimate_correlation(compute.CorrelationSpec((66, 66, 66), (12, 16, 22)))
-    assert est.padded_shape == (128, 128, 128)
+    # The transform length per axis is the smallest 2^a 3^b 5^c >= E + K - 1.
+    assert est.padded_shape == (80, 81, 90)
     assert est.padded_cells == 77 * 81 * 87
