@@ -1,6 +1,12 @@
 """Full greedy fill with the learned proposal against the exhaustive fill.
 
     python cpp-max-packer_b200/compare_fill.py [--workload rounded256_blob_hopf512] [--k 32]
+        [--configs 32,64,32:4]
+
+--configs runs one exhaustive fill and then a learned fill per entry: "k"
+pages the k proposed orientations, "k:m" also widens by k at a time while
+fewer than m paged orientations admit a copy
+(spk_session_greedy_proposed_adaptive).
 
 Both fills start from the empty container and run until no orientation
 admits a copy.
@@ -59,6 +65,7 @@ def main():
     ap.add_argument("--weights", default=os.path.join(HERE, "weights", "proposal_rounded256.npz"))
     ap.add_argument("--max-copies", type=int, default=100000)
     ap.add_argument("--report", default="")
+    ap.add_argument("--configs", default="", help="comma-separated learned configurations: k or k:min_feasible")
     args = ap.parse_args()
     compute, session_mod, workloads, proposal = pkg("compute"), pkg("session"), pkg("workloads"), pkg("proposal")
     ctx = compute.Context(0)
@@ -75,27 +82,40 @@ def main():
     s.close()
     net = proposal.Proposal(seed=0, context=ctx)
     net.load(args.weights)
-    s = open_session()
-    print("learned fill", flush=True)
-
-    def learned(n):
-        placed, fb = proposal.greedy_proposed(s, net, args.k, n)
-        return len(placed), fb
-
-    ln = fill(s, learned, max_copies=args.max_copies)
-    ln_scores = [p.score for p in s.placements]
-    s.close()
+    configs = [c for c in args.configs.split(",") if c] or [str(args.k)]
     report = {
-        "workload": wl.name, "orientations": len(wl.catalog), "k": args.k,
+        "workload": wl.name, "orientations": len(wl.catalog),
         "exhaustive": {"copies": ex[0], "seconds": round(ex[2], 2), "placements_per_s": round(ex[0] / ex[2], 3)},
-        "learned": {"copies": ln[0], "fallback_steps": ln[1], "seconds": round(ln[2], 2),
-                    "placements_per_s": round(ln[0] / ln[2], 3)},
-        "packed_count_ratio": round(ln[0] / ex[0], 4) if ex[0] else None,
-        "same_prefix": next((i for i, (a, b) in enumerate(zip(ex_scores, ln_scores)) if a != b),
-                            min(len(ex_scores), len(ln_scores))),
-        "mean_score": {"exhaustive": sum(ex_scores) / max(len(ex_scores), 1),
-                       "learned": sum(ln_scores) / max(len(ln_scores), 1)},
+        "learned": [],
     }
+    for config in configs:
+        k, _, m = config.partition(":")
+        k, m = int(k), int(m or 0)
+        s = open_session()
+        print(f"learned fill k={k} min_feasible={m}", flush=True)
+        widened = [0]
+
+        def learned(n):
+            if m:
+                placed, fb, w = proposal.greedy_proposed_adaptive(s, net, k, m, n)
+                widened[0] += w
+            else:
+                placed, fb = proposal.greedy_proposed(s, net, k, n)
+            return len(placed), fb
+
+        ln = fill(s, learned, max_copies=args.max_copies)
+        ln_scores = [p.score for p in s.placements]
+        s.close()
+        entry = {"k": k, "min_feasible": m, "copies": ln[0], "fallback_steps": ln[1], "widenings": widened[0],
+                 "seconds": round(ln[2], 2), "placements_per_s": round(ln[0] / ln[2], 3),
+                 "packed_count_ratio": round(ln[0] / ex[0], 4) if ex[0] else None,
+                 "speed_over_exhaustive": round((ln[0] / ln[2]) / (ex[0] / ex[2]), 3) if ex[2] and ln[2] else None,
+                 "same_prefix": next((i for i, (a, b) in enumerate(zip(ex_scores, ln_scores)) if a != b),
+                                     min(len(ex_scores), len(ln_scores))),
+                 "mean_score": sum(ln_scores) / max(len(ln_scores), 1)}
+        report["learned"].append(entry)
+        print(json.dumps(entry), flush=True)
+    report["exhaustive"]["mean_score"] = sum(ex_scores) / max(len(ex_scores), 1)
     print(json.dumps(report), flush=True)
     if args.report:
         with open(args.report, "w") as f:

@@ -346,9 +346,19 @@ int session_pages(spk_context* ctx, Session& s, const std::vector<PageRequest>& 
 // entry is not yet exact is resolved (certified page) only when its lower
 // bound could reach the current best head.  Places the chosen candidate and
 // returns it in `chosen` (empty when no orientation of the subset admits one).
-int greedy_step(spk_context* ctx, Session& s, const std::vector<std::size_t>& subset, std::optional<Candidate>& chosen)
+//
+// Widening (the learned proposal's adaptive policy): `reserve` lists further
+// orientations in the order they should join.  After the subset's first
+// pages are loaded, while fewer than `min_feasible` of the active
+// orientations have a non-empty page, the next `block` orientations of the
+// reserve are activated and paged before anything is chosen.  With an empty
+// reserve this is the plain merge over `subset`.
+int greedy_step(spk_context* ctx, Session& s, const std::vector<std::size_t>& subset, std::optional<Candidate>& chosen,
+                const std::vector<std::size_t>& reserve = {}, std::size_t min_feasible = 0, std::size_t block = 0,
+                std::size_t* widened = nullptr)
 {
     chosen.reset();
+    std::size_t next_reserve = 0;
     const std::size_t O = s.catalog.size();
     std::vector<bool> active(O, false);
     for (std::size_t o : subset) {
@@ -403,6 +413,28 @@ int greedy_step(spk_context* ctx, Session& s, const std::vector<std::size_t>& su
                 if (pages[o].empty() && floor[o] == INFINITY) {
                     exhausted[o] = true;
                 }
+            }
+            // Widen while too few active orientations admit a copy.
+            if (next_reserve < reserve.size() && block > 0) {
+                std::size_t feasible = 0;
+                for (std::size_t o = 0; o < O; ++o) {
+                    feasible += active[o] && !pages[o].empty() ? 1 : 0;
+                }
+                if (feasible < min_feasible) {
+                    for (std::size_t added = 0; added < block && next_reserve < reserve.size(); ++next_reserve) {
+                        const std::size_t o = reserve[next_reserve];
+                        if (o < O && !active[o]) {
+                            active[o] = true;
+                            exhausted[o] = false;
+                            ++added;
+                        }
+                    }
+                    if (widened) {
+                        ++*widened;
+                    }
+                    continue;
+                }
+                next_reserve = reserve.size();  // enough feasible orientations: no more widening
             }
         }
         // Best exact head.
@@ -1220,6 +1252,70 @@ int spk_session_greedy_proposed(spk_context* ctx, spk_proposal* proposal, uint32
             }
             if (!chosen) {
                 // No proposed orientation admits a copy: the exhaustive step decides.
+                if ((status = greedy_step(ctx, s, all, chosen))) {
+                    return status;
+                }
+                if (!chosen) {
+                    break;
+                }
+                if (fallbacks) {
+                    ++*fallbacks;
+                }
+            }
+            record(*chosen, *placed, orientations, translations, scores);
+            ++*placed;
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
+int spk_session_greedy_proposed_adaptive(spk_context* ctx, spk_proposal* proposal, uint32_t k,
+                                         uint32_t min_feasible, uint64_t max_steps, uint64_t* placed,
+                                         uint64_t* orientations, int64_t* translations, double* scores,
+                                         uint64_t* fallbacks, uint64_t* widenings)
+{
+    try {
+        if (!ctx || !session_of(ctx) || !placed) {
+            return kNotReady;
+        }
+        ProposalNet* net = proposal_net(proposal);
+        if (!net || k == 0) {
+            return kInvalidArgument;
+        }
+        auto& s = *session_of(ctx);
+        *placed = 0;
+        if (fallbacks) {
+            *fallbacks = 0;
+        }
+        if (widenings) {
+            *widenings = 0;
+        }
+        const std::size_t O = s.catalog.size();
+        std::vector<std::size_t> all(O);
+        for (std::size_t o = 0; o < O; ++o) {
+            all[o] = o;
+        }
+        std::vector<float> pred;
+        while (*placed < max_steps) {
+            int status = session_predict(ctx, s, net, pred);
+            if (status) {
+                return status;
+            }
+            const std::vector<std::size_t> ranked = top_k(pred, O);
+            const std::vector<std::size_t> subset(ranked.begin(), ranked.begin() + std::min<std::size_t>(k, O));
+            const std::vector<std::size_t> reserve(ranked.begin() + subset.size(), ranked.end());
+            std::optional<Candidate> chosen;
+            std::size_t widened = 0;
+            if ((status = greedy_step(ctx, s, subset, chosen, reserve, min_feasible, k, &widened))) {
+                return status;
+            }
+            if (widenings) {
+                *widenings += widened;
+            }
+            if (!chosen) {
                 if ((status = greedy_step(ctx, s, all, chosen))) {
                     return status;
                 }

@@ -444,6 +444,15 @@ int spk_session_propose(spk_context* context, spk_proposal* proposal, uint32_t k
 int spk_session_greedy_proposed(spk_context* context, spk_proposal* proposal, uint32_t k, uint64_t max_steps,
                                 uint64_t* placed, uint64_t* orientations, int64_t* translations, double* scores,
                                 uint64_t* fallbacks);
+/* No counterpart in the reference.  The proposed greedy with widening: when
+ * fewer than min_feasible of the k proposed orientations admit any copy, the
+ * step pages the next k in the network's order, and so on, before choosing
+ * (counted in *widenings, one per block added).  min_feasible = 0 is
+ * spk_session_greedy_proposed. */
+int spk_session_greedy_proposed_adaptive(spk_context* context, spk_proposal* proposal, uint32_t k,
+                                         uint32_t min_feasible, uint64_t max_steps, uint64_t* placed,
+                                         uint64_t* orientations, int64_t* translations, double* scores,
+                                         uint64_t* fallbacks, uint64_t* widenings);
 
 /* ---- independent jobs -------------------------------------------------------
  * No counterpart in the reference: several packing jobs (each a context with
