@@ -301,7 +301,8 @@ int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& 
     cudaMemsetAsync(d_misc, 0, 64, st);
     const int threads = 256;
     if (total > 0) {
-        raster_kernel<<<blocks_for(total, threads), threads, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets,
+        // 128-thread blocks: at ~146 registers a thread, three blocks fit an SM.
+        raster_kernel<<<blocks_for(total, 128), 128, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets,
                                                                       static_cast<int>(F), total, w, d_cells, d_misc);
     }
     ccl_init_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, n);

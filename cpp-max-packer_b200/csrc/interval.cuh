@@ -201,6 +201,7 @@ SPK_HD Interval ivec_dot(const IVec3& a, const IVec3& b)
 SPK_HD bool projection_separates(const IVec3* tri, const IVec3& box, const IVec3& axis)
 {
     Interval tp = ivec_dot(tri[0], axis);
+#pragma unroll
     for (int k = 1; k < 3; ++k) {
         const Interval p = ivec_dot(tri[k], axis);
         if (!p.valid) {
@@ -216,8 +217,13 @@ SPK_HD bool projection_separates(const IVec3* tri, const IVec3& box, const IVec3
 // 13-axis separating-axis test of a triangle (vertex intervals) and a box.
 SPK_HD bool triangle_box_disjoint(const IVec3* tri, const IVec3& box)
 {
+    // The loops are unrolled so that every array index is a constant and the
+    // intervals stay in registers; the operations and their order are as
+    // written.
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
         double lo = tri[0].v[a].low, hi = tri[0].v[a].high;
+#pragma unroll
         for (int k = 1; k < 3; ++k) {
             lo = f_min(lo, tri[k].v[a].low);
             hi = f_max(hi, tri[k].v[a].high);
@@ -232,7 +238,9 @@ SPK_HD bool triangle_box_disjoint(const IVec3* tri, const IVec3& box)
         return true;
     }
     const IVec3 edges[3] = { first, second, ivec_sub(tri[2], tri[1]) };
+#pragma unroll
     for (int e = 0; e < 3; ++e) {
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
             IVec3 axis = { { point_interval(0.0), point_interval(0.0), point_interval(0.0) } };
             axis.v[a] = point_interval(1.0);
