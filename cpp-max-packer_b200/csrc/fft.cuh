@@ -9,6 +9,8 @@
 // exp(-2 pi i m / L), m < L, computed on the host in FP64.
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace spk {
@@ -294,11 +296,17 @@ cudaError_t fft_axis(cplx_t<T>* data, int Lx, int Ly, int Lz, int axis, bool inv
     const int L = axis == 0 ? Lx : axis == 1 ? Ly : Lz;
     const long long lines = static_cast<long long>(Lx) * Ly * Lz / L;
     int group = sizeof(T) == 4 ? 16 : 8;
-    if (axis == 1 && group > Lx) {
-        group = Lx;
+    if (axis == 1) {
+        // A block's lines are consecutive x at one z: the group divides Lx.
+        group = std::min(group, Lx);
+        while (Lx % group) {
+            --group;
+        }
     }
-    while (group > 1 && lines % group) {
-        group >>= 1;
+    else {
+        while (group > 1 && lines % group) {
+            group >>= 1;
+        }
     }
     const size_t smem = sizeof(C) * (L + 2 * static_cast<size_t>(group) * (L + 1));
     static std::once_flag attribute[64];
