@@ -42,11 +42,15 @@ PASSES = [
     ("pass_b2_256_kernel", "inverse x with the fused threshold / score / top-k epilogue"),
     ("merge_kernel + exact_kernel", "key merge and exact recount"),
 ]
-# dram__bytes_read.sum + dram__bytes_write.sum per launch of each kernel on
-# the 256^3 workload, from the ncu captures summarised in profiles/ (the file
-# named beside each figure); absent where no capture of the current kernel
-# exists yet.
-NCU_DRAM_BYTES = {}
+# DRAM read + write bytes per launch of each kernel on the 256^3 workload,
+# from the ncu capture summarised in profiles/page_passes_rounded256_o16.md
+# (dram__bytes.sum.per_second x duration; each launch there does the same
+# work as in the 512-orientation workload).
+NCU_DRAM_BYTES = {
+    "pass_a256_batch_kernel": 2231196881,
+    "pass_b1_256_kernel": 182485494,
+    "pass_b2_256_kernel": 119751955,
+}
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp-max-packer_b200", "weights",
                                "proposal_rounded256.npz")
 
