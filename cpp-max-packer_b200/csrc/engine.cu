@@ -1049,10 +1049,11 @@ int spk_session_pages(spk_context* ctx, uint64_t n, const spk_page_query* querie
             if (queries[i].orientation_index >= s.catalog.size()) {
                 return kCatalog;
             }
-            if (queries[i].mode != 0) {
-                return kInvalidArgument;
+            if (queries[i].mode > 1) {
+                return kInvalidArgument;  // 0 ordinary, 1 low-overlap
             }
             requests[i].slot = s.slot_of[queries[i].orientation_index];
+            requests[i].low_overlap = queries[i].mode == 1;
             requests[i].has_cursor = queries[i].has_cursor != 0;
             if (requests[i].has_cursor) {
                 requests[i].cursor = from_c(queries[i].exclusive_cursor);

@@ -19,8 +19,8 @@ extern "C" int spk_spectral_page(spk_context* ctx, const spk_page_scene* scene, 
             return kInvalidArgument;
         }
         *count = 0;
-        if (query->mode != 0) {
-            return kInvalidArgument;
+        if (query->mode > 1) {
+            return kInvalidArgument;  // 0 ordinary, 1 low-overlap
         }
         if (cudaSetDevice(ctx->device) != cudaSuccess) {
             return kCuda;
@@ -49,6 +49,7 @@ extern "C" int spk_spectral_page(spk_context* ctx, const spk_page_scene* scene, 
         }
         PageRequest request;
         request.slot = slot;
+        request.low_overlap = query->mode == 1;
         request.has_cursor = query->has_cursor != 0;
         if (request.has_cursor) {
             const auto& c = query->exclusive_cursor;

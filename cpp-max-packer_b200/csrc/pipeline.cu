@@ -238,12 +238,15 @@ __device__ __forceinline__ void warp_insert(unsigned long long& lo, unsigned lon
 }
 
 // Pass B2: inverse FFT along x for 8 legal rows, then the fused epilogue.
-// mode 0: warp top-32 lists + pruning bound in *tau; mode 1: append every
-// candidate whose approximate score is <= threshold and count every candidate
-// past the cursor floor in *tau.
+// A candidate is a legal translation whose rounded overlap count is `target`
+// (0 for ordinary pages).  mode 0: warp top-32 lists + pruning bound in *tau;
+// mode 1: append every candidate whose approximate score is <= threshold and
+// count every candidate past the cursor floor in *tau; mode 2: histogram of
+// the rounded overlap counts of every legal translation into `keys` read as
+// `cap` u32 bins (the last bin holds every larger count).
 __global__ void pass_b2_kernel(const float2* __restrict__ inter, int L0, int L1, int legal_x, int legal_y,
                                int legal_z, const float2* __restrict__ twiddles, const double* __restrict__ t65,
-                               double inv_occ, int mode, double threshold, double cursor_floor,
+                               double inv_occ, int mode, float target, double threshold, double cursor_floor,
                                unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
                                unsigned int cap, unsigned long long* __restrict__ tau,
                                unsigned long long* __restrict__ resid)
@@ -293,7 +296,13 @@ __global__ void pass_b2_kernel(const float2* __restrict__ inter, int L0, int L1,
         if (x < legal_x) {
             const float2 v = res[warp * pitch + x];
             residual = fmaxf(residual, fabsf(v.x - rintf(v.x)));
-            if (fabsf(v.x) < 0.5f && !(v.y < skip)) {
+            if (mode == 2) {
+                const float c = rintf(v.x);
+                const unsigned int bin = c <= 0.f ? 0u : c >= static_cast<float>(cap - 1) ? cap - 1
+                                                                                           : static_cast<unsigned int>(c);
+                atomicAdd(reinterpret_cast<unsigned int*>(keys) + bin, 1u);
+            }
+            else if (fabsf(v.x - target) < 0.5f && !(v.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(v.y) * inv_occ);
                 if (score >= cursor_floor) {
                     key = make_key(score, row_index + x);
@@ -597,7 +606,7 @@ struct B2Shared {
 // of the block calls it; it may be called again for the next 16 rows.
 __device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
                                            bool valid, int y, int zz, int legal_x, int legal_y,
-                                           const double* __restrict__ t65, double inv_occ, int mode,
+                                           const double* __restrict__ t65, double inv_occ, int mode, float target,
                                            double threshold, double cursor_floor,
                                            unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
                                            unsigned int cap, unsigned long long* __restrict__ tau,
@@ -639,7 +648,7 @@ __device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* line
         if (valid && x < legal_x) {
             const float2 w = line[x];
             residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
-            if (fabsf(w.x) < 0.5f && !(w.y < skip)) {
+            if (fabsf(w.x - target) < 0.5f && !(w.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
                 if (score >= cursor_floor) {
                     key = make_key(score, row_index + x);
@@ -803,7 +812,7 @@ __device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* line
 // path.
 __device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
                                                   bool valid, int y, int zz, int legal_x, int legal_y,
-                                                  const double* __restrict__ t65, double inv_occ,
+                                                  const double* __restrict__ t65, double inv_occ, float target,
                                                   double cursor_floor, unsigned long long* __restrict__ keys,
                                                   unsigned int* __restrict__ count, unsigned int cap,
                                                   unsigned long long* __restrict__ tau,
@@ -836,7 +845,7 @@ __device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines
         const float2 w = v[m2];
         if (valid && x < legal_x) {
             residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
-            if (fabsf(w.x) < 0.5f && !(w.y < skip)) {
+            if (fabsf(w.x - target) < 0.5f && !(w.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
                 if (score >= cursor_floor) {
                     const unsigned long long key = make_key(score, row_index + x);
@@ -963,22 +972,73 @@ __device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines
     }
 }
 
+// Mode 2 of the epilogue: the histogram of the 16 rows' rounded overlap
+// counts, gathered in shared memory and added to the request's `bins` u32
+// bins in `hist` (the last bin holds every larger count).
+__device__ __forceinline__ void b2_rows256_hist(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+                                                bool valid, int legal_x, unsigned int* __restrict__ hist,
+                                                unsigned int bins, unsigned long long* __restrict__ resid)
+{
+    const int t = threadIdx.x & 15;
+    const int j = threadIdx.x >> 4;
+    const int lane = threadIdx.x & 31;
+    const unsigned int local_bins = bins < 1024u ? bins : 1024u;
+    __syncthreads();  // the previous rows' readers of `sh` are done
+    for (unsigned int b = threadIdx.x; b < local_bins; b += blockDim.x) {
+        sh.hist[b] = 0;
+    }
+    fft256<true>(v, lines + j * kRegLine, t, tw);  // v[m2] = value at x = t + 16 m2
+    float residual = 0.f;
+#pragma unroll
+    for (int m2 = 0; m2 < 16; ++m2) {
+        const int x = t + 16 * m2;
+        if (valid && x < legal_x) {
+            const float w = v[m2].x;
+            residual = fmaxf(residual, fabsf(w - rintf(w)));
+            const float c = rintf(w);
+            const unsigned int bin = c <= 0.f ? 0u : c >= static_cast<float>(bins - 1) ? bins - 1
+                                                                                       : static_cast<unsigned int>(c);
+            if (bin < local_bins) {
+                atomicAdd(&sh.hist[bin], 1u);
+            }
+            else {
+                atomicAdd(hist + bin, 1u);
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        residual = fmaxf(residual, __shfl_xor_sync(kFull, residual, o));
+    }
+    if (lane == 0 && residual > 0.f) {
+        atomicMax(resid, static_cast<unsigned long long>(__float_as_uint(residual)));
+    }
+    __syncthreads();
+    for (unsigned int b = threadIdx.x; b < local_bins; b += blockDim.x) {
+        if (sh.hist[b]) {
+            atomicAdd(hist + b, sh.hist[b]);
+        }
+    }
+}
+
 // Mode 0 (first pass) takes the register path, mode 1 (threshold pass) the
-// generic one.
+// generic one, mode 2 the count histogram.
 __device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
                                            bool valid, int y, int zz, int legal_x, int legal_y,
-                                           const double* __restrict__ t65, double inv_occ, int mode,
+                                           const double* __restrict__ t65, double inv_occ, int mode, float target,
                                            double threshold, double cursor_floor,
                                            unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
                                            unsigned int cap, unsigned long long* __restrict__ tau,
                                            unsigned long long* __restrict__ resid)
 {
     if (mode == 0) {
-        b2_rows256_select(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, cursor_floor, keys, count,
-                          cap, tau, resid);
+        b2_rows256_select(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, target, cursor_floor, keys,
+                          count, cap, tau, resid);
+    }
+    else if (mode == 2) {
+        b2_rows256_hist(v, lines, tw, sh, valid, legal_x, reinterpret_cast<unsigned int*>(keys), cap, resid);
     }
     else {
-        b2_rows256_generic(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, threshold,
+        b2_rows256_generic(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, target, threshold,
                            cursor_floor, keys, count, cap, tau, resid);
     }
 }
@@ -987,7 +1047,7 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
                                                          int legal_y, int legal_z,
                                                          const float2* __restrict__ twiddles,
                                                          const double* __restrict__ t65, double inv_occ, int mode,
-                                                         double threshold, double cursor_floor,
+                                                         float target, double threshold, double cursor_floor,
                                                          unsigned long long* __restrict__ keys,
                                                          unsigned int* __restrict__ count, unsigned int cap,
                                                          unsigned long long* __restrict__ tau,
@@ -1011,8 +1071,8 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     for (int n1 = 0; n1 < 16; ++n1) {
         v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
     }
-    b2_rows256(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, threshold, cursor_floor, keys,
-               count, cap, tau, resid);
+    b2_rows256(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, target, threshold, cursor_floor,
+               keys, count, cap, tau, resid);
 }
 
 // Passes B1 and B2 fused on 256^3 grids: one cluster of 8 CTAs per legal z
@@ -1028,7 +1088,8 @@ constexpr std::size_t kFusedSmem = sizeof(float2) * (256 * 32 + 16 * kRegLine + 
 __global__ void __cluster_dims__(kFusedCluster, 1, 1) __launch_bounds__(256)
     pass_b_fused_256_kernel(const float2* __restrict__ inter, int legal_x, int legal_y,
                             const float2* __restrict__ twiddles, const double* __restrict__ t65, double inv_occ,
-                            int mode, double threshold, double cursor_floor, unsigned long long* __restrict__ keys,
+                            int mode, float target, double threshold, double cursor_floor,
+                            unsigned long long* __restrict__ keys,
                             unsigned int* __restrict__ count, unsigned int cap, unsigned long long* __restrict__ tau,
                             unsigned long long* __restrict__ resid)
 {
@@ -1074,8 +1135,8 @@ __global__ void __cluster_dims__(kFusedCluster, 1, 1) __launch_bounds__(256)
             const float2* src = cluster.map_shared_rank(cols, n1 >> 1);
             v[n1] = valid ? src[y * 32 + 16 * (n1 & 1) + t] : make_float2(0.f, 0.f);
         }
-        b2_rows256(v, lines, tw, sh, valid, valid ? y : 0, zz, legal_x, legal_y, t65, inv_occ, mode, threshold,
-                   cursor_floor, keys, count, cap, tau, resid);
+        b2_rows256(v, lines, tw, sh, valid, valid ? y : 0, zz, legal_x, legal_y, t65, inv_occ, mode, target,
+                   threshold, cursor_floor, keys, count, cap, tau, resid);
     }
     cluster.sync();  // no CTA leaves while another may still read its columns
 }
@@ -1660,7 +1721,7 @@ double Pipeline::score(const KernelSlot& s, const std::int64_t* t, double p) con
     return .65 * top - .35 * mean_proximity;
 }
 
-int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, double cursor_floor,
+int Pipeline::run_orientation(const KernelSlot& s, int mode, float target, double threshold, double cursor_floor,
                               unsigned long long* keys, unsigned int* count, unsigned int cap,
                               unsigned long long* tau, unsigned long long* resid)
 {
@@ -1690,7 +1751,7 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
         pass_a256_kernel<<<16 * 256, 256, 0, st>>>(spectrum_, s.partial, inter_, s.K[2], s.legal[2], tw2);
         pass_end(ctx_, 0, ev, pass_a_bytes(s));
         ctx_->launches++;
-        return run_b256(s, inter_, mode, threshold, cursor_floor, keys, count, cap, tau, resid);
+        return run_b256(s, inter_, mode, target, threshold, cursor_floor, keys, count, cap, tau, resid);
     }
     const std::size_t smem_a = sizeof(float2) * (L_[2] + 2 * kColumnGroup * (L_[2] + 1) + kColumnGroup * L_[2]);
     auto ev = pass_begin(ctx_);
@@ -1709,7 +1770,7 @@ int Pipeline::run_orientation(const KernelSlot& s, int mode, double threshold, d
     ev = pass_begin(ctx_);
     pass_b2_kernel<<<static_cast<unsigned>((rows + kB2Rows - 1) / kB2Rows), 32 * kB2Rows, smem_b, st>>>(
         inter_, L_[0], L_[1], s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied),
-        mode, threshold, cursor_floor, keys, count, cap, tau, resid);
+        mode, target, threshold, cursor_floor, keys, count, cap, tau, resid);
     pass_end(ctx_, 2, ev);
     ctx_->launches++;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
@@ -1743,7 +1804,7 @@ int Pipeline::run_a256_batch(const KernelSlot* const* slots, int count, float2* 
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
-int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double threshold, double cursor_floor,
+int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, float target, double threshold, double cursor_floor,
                        unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
                        unsigned long long* resid)
 {
@@ -1766,7 +1827,7 @@ int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double thre
         });
         auto ev = pass_begin(ctx_);
         pass_b_fused_256_kernel<<<kFusedCluster * s.legal[2], 256, kFusedSmem, st>>>(
-            inter, s.legal[0], s.legal[1], tw1, s.t65, 1.0 / static_cast<double>(s.occupied), mode, threshold,
+            inter, s.legal[0], s.legal[1], tw1, s.t65, 1.0 / static_cast<double>(s.occupied), mode, target, threshold,
             cursor_floor, keys, count, cap, tau, resid);
         pass_end(ctx_, 2, ev, 8.0 * L_[0] * L_[1] * s.legal[2]);
         ctx_->launches++;
@@ -1778,14 +1839,138 @@ int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, double thre
     const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
     ev = pass_begin(ctx_);
     pass_b2_256_kernel<<<static_cast<unsigned>((rows + 15) / 16), 256, 0, st>>>(
-        inter, s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied), mode, threshold,
-        cursor_floor, keys, count, cap, tau, resid);
+        inter, s.legal[0], s.legal[1], s.legal[2], tw0, s.t65, 1.0 / static_cast<double>(s.occupied), mode, target,
+        threshold, cursor_floor, keys, count, cap, tau, resid);
     pass_end(ctx_, 2, ev, 8.0 * L_[0] * legal_rows);
     ctx_->launches += 2;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
 int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out, bool full)
+{
+    std::vector<std::size_t> ordinary;
+    for (std::size_t r = 0; r < requests.size(); ++r) {
+        if (!requests[r].low_overlap) {
+            ordinary.push_back(r);
+        }
+    }
+    if (ordinary.size() == requests.size()) {
+        return ordinary_pages(requests, out, full);
+    }
+    out.assign(requests.size(), {});
+    if (!ordinary.empty()) {
+        std::vector<PageRequest> sub;
+        for (std::size_t r : ordinary) {
+            sub.push_back(requests[r]);
+        }
+        std::vector<PageOutcome> sub_out;
+        if (int status = ordinary_pages(sub, sub_out, full)) {
+            return status;
+        }
+        for (std::size_t i = 0; i < ordinary.size(); ++i) {
+            out[ordinary[i]] = std::move(sub_out[i]);
+        }
+    }
+    for (std::size_t r = 0; r < requests.size(); ++r) {
+        if (requests[r].low_overlap) {
+            if (int status = low_overlap_page(requests[r], out[r])) {
+                return status;
+            }
+        }
+    }
+    return kOk;
+}
+
+// A low-overlap page (spectral_pipeline.cpp:1758-1824, mode low_overlap):
+// the 32 legal translations after the cursor that are smallest by
+// (rounded overlap count, score, z, y, x), over every legal translation, with
+// no recount (direct_zero_overlap stays false).  A histogram pass counts the
+// translations per rounded overlap; then, from the cursor's count upward,
+// each count with translations contributes its certified ordinary-style page
+// (candidates: overlap == that count) until 32 entries are gathered.  Counts
+// of kOverlapBins - 1 and above share the last bin; a page that would need
+// them fails with SPK_SCRATCH_LIMIT.
+int Pipeline::low_overlap_page(const PageRequest& req, PageOutcome& out)
+{
+    out = {};
+    const auto& s = slots_[req.slot];
+    if (!s.legal[0] || !s.legal[1] || !s.legal[2]) {
+        out.certified = true;
+        return kOk;
+    }
+    if (!s.occupied) {
+        out.status = kEmptyKernel;
+        return kOk;
+    }
+    constexpr unsigned int kOverlapBins = 4096;
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
+    auto* hist = static_cast<unsigned int*>(device_buffer(ctx_, "pipe.overlap_hist", kOverlapBins * 4, status));
+    auto* meta = static_cast<unsigned long long*>(device_buffer(ctx_, "pipe.overlap_meta", 24, status));
+    if (!hist || !meta) {
+        return status;
+    }
+    cudaMemsetAsync(hist, 0, kOverlapBins * 4, st);
+    cudaMemsetAsync(meta, 0, 24, st);
+    if ((status = run_orientation(s, 2, 0.f, 0.0, -INFINITY, reinterpret_cast<unsigned long long*>(hist),
+                                  reinterpret_cast<unsigned int*>(meta + 2), kOverlapBins, meta, meta + 1))) {
+        return status;
+    }
+    std::vector<unsigned int> h(kOverlapBins);
+    unsigned long long h_meta[3] {};
+    cudaMemcpyAsync(h.data(), hist, kOverlapBins * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h_meta, meta, 24, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    std::uint32_t rbits = static_cast<std::uint32_t>(h_meta[1]);
+    float rf;
+    std::memcpy(&rf, &rbits, 4);
+    out.max_integer_residual = rf;
+    if (rf >= 0.25f) {
+        out.status = kNumeric;  // correlation.cpp:521-528 residual guard
+        return kOk;
+    }
+    // The cursor's overlap is a rounded count held as a double.
+    const std::uint32_t first =
+        req.has_cursor ? static_cast<std::uint32_t>(std::max(0.0, std::nearbyint(req.cursor.binary_overlap))) : 0u;
+    for (std::uint32_t c = first; c < kOverlapBins && out.page.size() < static_cast<std::size_t>(kPageSize); ++c) {
+        if (h[c] == 0) {
+            continue;
+        }
+        if (c == kOverlapBins - 1) {
+            out.status = kScratchLimit;  // the counts beyond the histogram are not resolved
+            return kOk;
+        }
+        PageRequest bin = req;
+        bin.low_overlap = false;
+        bin.overlap = c;
+        bin.has_cursor = req.has_cursor && c == first;
+        std::vector<PageOutcome> bin_out;
+        if ((status = ordinary_pages({ bin }, bin_out, true))) {
+            return status;
+        }
+        if (bin_out[0].status) {
+            out.status = bin_out[0].status;
+            return kOk;
+        }
+        out.rescored += bin_out[0].rescored;
+        out.max_score_error = std::max(out.max_score_error, bin_out[0].max_score_error);
+        for (auto& candidate : bin_out[0].page) {
+            if (out.page.size() == static_cast<std::size_t>(kPageSize)) {
+                break;
+            }
+            candidate.direct_zero = false;
+            out.page.push_back(candidate);
+        }
+    }
+    out.certified = true;
+    out.exact_floor = INFINITY;
+    return kOk;
+}
+
+int Pipeline::ordinary_pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out, bool full)
 {
     const int R = static_cast<int>(requests.size());
     out.assign(R, {});
@@ -1865,8 +2050,9 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
             }
             for (int g = 0; g < n; ++g) {
                 const int r = runnable[i0 + g];
-                if ((status = run_b256(*group[g], outs[g], 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap,
-                                       count + r, cap, tau + r, resid + r))) {
+                if ((status = run_b256(*group[g], outs[g], 0, static_cast<float>(requests[r].overlap), 0.0, floor[r],
+                                       keys + static_cast<long long>(r) * cap, count + r, cap, tau + r,
+                                       resid + r))) {
                     return status;
                 }
             }
@@ -1876,8 +2062,9 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
         for (std::size_t i = 0; i < runnable.size(); ++i) {
             const int r = runnable[i];
             const auto& s = slots_[requests[r].slot];
-            if ((status = run_orientation(s, 0, 0.0, floor[r], keys + static_cast<long long>(r) * cap, count + r,
-                                          cap, tau + r, resid + r))) {
+            if ((status = run_orientation(s, 0, static_cast<float>(requests[r].overlap), 0.0, floor[r],
+                                          keys + static_cast<long long>(r) * cap, count + r, cap, tau + r,
+                                          resid + r))) {
                 return status;
             }
         }
@@ -1964,7 +2151,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
             const double approx = decode_key_score(key);
             max_error = std::max(max_error, std::fabs(approx - c.score));
             ++o.rescored;
-            if (overlap != 0) {
+            if (overlap != static_cast<long long>(req.overlap)) {
                 continue;  // the reference's FFT rounding never admits these
             }
             if (req.has_cursor && !rank_less(req.cursor, c)) {
@@ -2048,8 +2235,8 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
             }
             unsigned long long zero[3] = { 0, 0, 0 };
             cudaMemcpyAsync(meta, zero, 24, cudaMemcpyHostToDevice, st);
-            if ((status = run_orientation(s, 1, threshold, floor[r], tkeys, reinterpret_cast<unsigned int*>(meta + 2),
-                                          cap, meta, meta + 1))) {
+            if ((status = run_orientation(s, 1, static_cast<float>(req.overlap), threshold, floor[r], tkeys,
+                                          reinterpret_cast<unsigned int*>(meta + 2), cap, meta, meta + 1))) {
                 return status;
             }
             ++stat_threshold_passes;
@@ -2098,7 +2285,7 @@ int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOu
                     c.direct_zero = cnt[i] == 0;
                     o.max_score_error = std::max(o.max_score_error, std::fabs(decode_key_score(hk[i]) - c.score));
                     ++o.rescored;
-                    if (cnt[i] != 0 || (req.has_cursor && !rank_less(req.cursor, c))) {
+                    if (cnt[i] != static_cast<long long>(req.overlap) || (req.has_cursor && !rank_less(req.cursor, c))) {
                         continue;
                     }
                     all.push_back(c);

@@ -70,6 +70,11 @@ struct PageRequest {
     std::uint64_t slot {};
     bool has_cursor {};
     Candidate cursor {};
+    // Candidates are the legal translations whose overlap count is this
+    // (0: ordinary pages; low-overlap pages use one count at a time).
+    std::uint32_t overlap {};
+    // A low-overlap page (spectral_pipeline.hpp:45, CandidatePageMode::low_overlap).
+    bool low_overlap {};
 };
 
 struct PageOutcome {
@@ -116,10 +121,12 @@ public:
     double epsilon_p(const KernelSlot& s) const;
 
 private:
-    int run_orientation(const KernelSlot& s, int mode, double threshold, double cursor_floor, unsigned long long* keys,
-                        unsigned int* count, unsigned int cap, unsigned long long* tau,
+    int ordinary_pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out, bool full);
+    int low_overlap_page(const PageRequest& request, PageOutcome& out);
+    int run_orientation(const KernelSlot& s, int mode, float target, double threshold, double cursor_floor,
+                        unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
                         unsigned long long* resid);
-    int run_b256(const KernelSlot& s, float2* inter, int mode, double threshold, double cursor_floor,
+    int run_b256(const KernelSlot& s, float2* inter, int mode, float target, double threshold, double cursor_floor,
                  unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
                  unsigned long long* resid);
     double pass_a_bytes(const KernelSlot& s) const;

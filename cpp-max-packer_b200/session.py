@@ -129,12 +129,16 @@ class Session:
         _lib.check(self.lib.spk_session_remove_last(self.context.handle), "spk_session_remove_last")
         self.placements.pop()
 
-    def pages(self, orientations, cursors=None, reports: Optional[list] = None) -> List[List[RankedCandidate]]:
+    def pages(self, orientations, cursors=None, reports: Optional[list] = None,
+              low_overlap: bool = False) -> List[List[RankedCandidate]]:
+        """Ordinary pages, or with `low_overlap` the reference's low-overlap
+        pages (every legal translation ranked by overlap count, then score)."""
         orientations = list(orientations)
         n = len(orientations)
         queries = (PageQueryC * n)()
         for i, o in enumerate(orientations):
             queries[i].orientation_index = o
+            queries[i].mode = 1 if low_overlap else 0
             if cursors is not None and cursors[i] is not None:
                 queries[i].has_cursor = 1
                 queries[i].exclusive_cursor = cursors[i].to_c()

@@ -210,7 +210,10 @@ typedef struct spk_candidate {
 } spk_candidate;
 
 /* Reference: CandidatePageQuery, spectral_pipeline.hpp:45-51.  mode 0 is
- * CandidatePageMode::ordinary; low_overlap is not offered (SPK_INVALID_ARGUMENT). */
+ * CandidatePageMode::ordinary (candidates with a zero rounded overlap,
+ * recounted exactly); mode 1 is CandidatePageMode::low_overlap (every legal
+ * translation, ranked by (binary_overlap, score, orientation, z, y, x), not
+ * recounted: direct_zero_overlap is 0), spectral_pipeline.cpp:1758-1824. */
 typedef struct spk_page_query {
     uint64_t orientation_index;
     int32_t has_cursor;
