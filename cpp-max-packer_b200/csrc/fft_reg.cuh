@@ -82,11 +82,22 @@ __device__ __forceinline__ void dft16(float2 (&x)[16])
     }
 }
 
+// How fft256 orders its shared-memory exchange:
+//   kBlockSync - the line's threads may lie in different warps; the block
+//                synchronises before the exchange (earlier readers of `line`
+//                are done) and between its writes and reads;
+//   kFirstUse  - as kBlockSync, for the first use of `line` in the kernel
+//                after a block barrier: only the second synchronisation;
+//   kHalfWarp  - the line's 16 threads are one half of a warp (thread t of
+//                line j is threadIdx 16 j + t): __syncwarp orders the
+//                exchange, and only the calling warps need take part.
+enum FftSync { kBlockSync = 0, kFirstUse = 1, kHalfWarp = 2 };
+
 // Four-step 256-point transform of the line held by the 16 threads with
 // lane-in-line index t.  `line` points at this line's kRegLine shared slots;
-// tw is exp(-2 pi i m / 256), m < 256.  Every thread of the block must call it
-// (it synchronises the block twice).
-template <bool INV>
+// tw is exp(-2 pi i m / 256), m < 256.  With kBlockSync or kFirstUse every
+// thread of the block must call it; with kHalfWarp every thread of the warp.
+template <bool INV, int SYNC = kBlockSync>
 __device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, const float2* __restrict__ tw)
 {
     dft16<INV>(v);  // thread t: Y[t][k1] = v[k1]
@@ -98,12 +109,22 @@ __device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, con
         }
         v[k1] = cmulf(v[k1], w);
     }
-    __syncthreads();  // the previous reader of `line` is done
+    if (SYNC == kBlockSync) {
+        __syncthreads();  // the previous reader of `line` is done
+    }
+    else if (SYNC == kHalfWarp) {
+        __syncwarp();
+    }
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
         line[t * 17 + k1] = v[k1];
     }
-    __syncthreads();
+    if (SYNC == kHalfWarp) {
+        __syncwarp();
+    }
+    else {
+        __syncthreads();
+    }
 #pragma unroll
     for (int n2 = 0; n2 < 16; ++n2) {
         v[n2] = line[n2 * 17 + t];

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
         v[n1] = z < K2 ? partial[col + plane * z] : make_float2(0.f, 0.f);
     }
     float2* line = lines + j * kRegLine;
-    fft256<false>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
+    fft256<false, kFirstUse>(v, line, t, tw);  // v[k2] = K^(t + 16 k2)
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) {
         const float2 sv = sp[k2];
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(256) env_row256_kernel(float2* __restrict__ sp
         acc += static_cast<double>(b) * b + static_cast<double>(p) * p;
         v[n1] = make_float2(b, p);
     }
-    fft256<false>(v, lines + j * kRegLine, t, tw);
+    fft256<false, kHalfWarp>(v, lines + j * kRegLine, t, tw);
     float2* out = spectrum + 256LL * row;
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) {
@@ -549,7 +549,7 @@ __global__ void __launch_bounds__(256) env_column256_kernel(float2* __restrict__
     for (int n1 = 0; n1 < 16; ++n1) {
         v[n1] = spectrum[col + line_stride * (16 * n1 + t)];
     }
-    fft256<false>(v, lines + j * kRegLine, t, tw);
+    fft256<false, kFirstUse>(v, lines + j * kRegLine, t, tw);
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) {
         spectrum[col + line_stride * (t + 16 * k2)] = make_float2(v[k2].x * scale, v[k2].y * scale);
@@ -572,7 +572,7 @@ __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ i
     for (int n1 = 0; n1 < 16; ++n1) {
         v[n1] = inter[col + 256LL * (16 * n1 + t)];
     }
-    fft256<true>(v, lines + j * kRegLine, t, tw);
+    fft256<true, kFirstUse>(v, lines + j * kRegLine, t, tw);
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {
         const int y = t + 16 * m2;
@@ -623,7 +623,7 @@ __device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* line
         sh.cut_bin = kBins - 1;
     }
     float2* line = lines + j * kRegLine;
-    fft256<true>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
+    fft256<true, kHalfWarp>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
     // Stage the row in shared memory (each thread reads back only its own
     // outputs) so the epilogue loop indexes it without a local-memory array.
     __syncthreads();
@@ -829,7 +829,7 @@ __device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines
         sh.cut_bin = kBins - 1;
     }
     float2* line = lines + j * kRegLine;
-    fft256<true>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
+    fft256<true, kHalfWarp>(v, line, t, tw);  // v[m2] = value at x = t + 16 m2
     auto* row_keys = reinterpret_cast<unsigned long long*>(line);
     const double t65z = valid ? t65[zz] : 0.0;
     const unsigned int row_index = static_cast<unsigned int>(legal_x) * (y + static_cast<unsigned int>(legal_y) * zz);
@@ -987,7 +987,7 @@ __device__ __forceinline__ void b2_rows256_hist(float2 (&v)[16], float2* lines, 
     for (unsigned int b = threadIdx.x; b < local_bins; b += blockDim.x) {
         sh.hist[b] = 0;
     }
-    fft256<true>(v, lines + j * kRegLine, t, tw);  // v[m2] = value at x = t + 16 m2
+    fft256<true, kHalfWarp>(v, lines + j * kRegLine, t, tw);  // v[m2] = value at x = t + 16 m2
     float residual = 0.f;
 #pragma unroll
     for (int m2 = 0; m2 < 16; ++m2) {

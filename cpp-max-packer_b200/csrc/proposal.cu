@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -40,7 +41,7 @@ constexpr int kKC = 32;      // K elements per stage (two MMA K-steps of 16)
 constexpr int kStages = 4;
 constexpr int kThreads = 128;
 constexpr int kStepBytesA = kRows * 16 * 2;  // one K-step block of A: 128 rows x 16 bf16
-enum Mode { kFwd = 0, kData = 1, kWeight = 2 };
+enum Mode { kFwd = 0, kData = 1, kWeight = 2, kFwdBox = 3 };
 
 int cin_pad(int cin) { return cin < 8 ? 8 : cin; }
 
@@ -61,11 +62,33 @@ struct ConvArgs {
     // log2 of the power-of-two extents and channel counts (every layer of the
     // network has them), so the gathers index with shifts and masks.
     int lg_s_in, lg_s_out, lg_cin, lg_cinp, lg_cout;
+    // Corner-box forward (kFwdBox): the GEMM rows are the voxels of the box
+    // [0, box_out) of every sample, row m = n * box_out_vol + (z * box_out[1]
+    // + y) * box_out[0] + x, and `out` / `out_f32` are laid out by row as
+    // always.  An input voxel inside [0, box_in) is read from x, laid out
+    // [n][box_in voxels][cin] the same way; any other input voxel is read
+    // from x_shared ([s_in^3][cin], one sample shared by all), or is zero
+    // when x_shared is null.
+    const bf16* x_shared;
+    int box_in[3], box_out[3];
+    int box_in_vol, box_out_vol;
 };
 
 struct Vox {
     int n, z, y, x;
 };
+
+// Voxel of row m of a corner-box GEMM (rows < 2^32).
+__device__ __forceinline__ Vox decode_box(unsigned m, const int (&box)[3], int vol)
+{
+    Vox v;
+    v.n = static_cast<int>(m / static_cast<unsigned>(vol));
+    const int r = static_cast<int>(m % static_cast<unsigned>(vol));
+    v.x = r % box[0];
+    v.y = (r / box[0]) % box[1];
+    v.z = r / (box[0] * box[1]);
+    return v;
+}
 
 // Voxel of row m in a batch of cubes of side 2^lg (rows < 2^32).
 __device__ __forceinline__ Vox decode_pow2(unsigned m, int lg)
@@ -149,7 +172,7 @@ template <int MODE>
 __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, long long m0, int chunk, int tid,
                                          const Vox& row_vox, bool row_ok)
 {
-    if (MODE == kFwd || MODE == kData) {
+    if (MODE != kWeight) {
         // K-major: thread tid owns row tid; unit j covers K half (j & 1) of K-step (j >> 1).
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
@@ -160,16 +183,32 @@ __device__ __forceinline__ void gather_a(const ConvArgs& a, unsigned char* A, lo
             bool valid = false;
             if (row_ok && k < a.k_total) {
                 const int kk = static_cast<int>(k);
-                if (MODE == kFwd) {
+                if (MODE == kFwd || MODE == kFwdBox) {
                     const int tap = kk >> a.lg_cinp, ci0 = kk & ((1 << a.lg_cinp) - 1);
                     int iz, iy, ix;
                     if (tap < 27 && (a.cin >= 8 || ci0 == 0) && tap_input(row_vox, tap, a.stride, a.s_in, iz, iy, ix)) {
-                        const long long at = voxel_offset(row_vox, iz, iy, ix, a.lg_s_in, a.lg_cin);
-                        if (a.cin < 8) {
-                            put(A, off, load_channels(a.x + at, a.cin, ci0));
+                        const bf16* base = a.x;
+                        long long at;
+                        if (MODE == kFwd) {
+                            at = voxel_offset(row_vox, iz, iy, ix, a.lg_s_in, a.lg_cin);
+                        }
+                        else if (iz < a.box_in[2] && iy < a.box_in[1] && ix < a.box_in[0]) {
+                            at = (static_cast<long long>(row_vox.n) * a.box_in_vol +
+                                  (iz * a.box_in[1] + iy) * a.box_in[0] + ix) << a.lg_cin;
+                        }
+                        else if (a.x_shared) {
+                            base = a.x_shared;
+                            at = voxel_offset(Vox { 0, 0, 0, 0 }, iz, iy, ix, a.lg_s_in, a.lg_cin);
+                        }
+                        else {
+                            copy16(A, off, src, false);  // zero outside the box
                             continue;
                         }
-                        src = a.x + at + ci0;
+                        if (a.cin < 8) {
+                            put(A, off, load_channels(base + at, a.cin, ci0));
+                            continue;
+                        }
+                        src = base + at + ci0;
                         valid = true;
                     }
                 }
@@ -231,7 +270,7 @@ __device__ __forceinline__ void gather_b(const ConvArgs& a, unsigned char* B, in
         const void* src = a.w;
         bool valid = false;
         std::uint32_t off;
-        if (MODE == kFwd) {
+        if (MODE == kFwd || MODE == kFwdBox) {
             // K-major rows cout.
             const int c = rem / N, co = rem % N;
             const long long k = static_cast<long long>(chunk) * kKC + ks * 16 + c * 8;
@@ -301,10 +340,16 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
     if (MODE != kWeight) {
         const long long m = m0 + tid;
         row_ok = m < a.m_total;
-        row_vox = decode_pow2(static_cast<unsigned>(row_ok ? m : 0), MODE == kFwd ? a.lg_s_out : a.lg_s_in);
+        if (MODE == kFwdBox) {
+            row_vox = decode_box(static_cast<unsigned>(row_ok ? m : 0), a.box_out, a.box_out_vol);
+        }
+        else {
+            row_vox = decode_pow2(static_cast<unsigned>(row_ok ? m : 0), MODE == kFwd ? a.lg_s_out : a.lg_s_in);
+        }
     }
+    constexpr bool fwd = MODE == kFwd || MODE == kFwdBox;
     constexpr bool a_mn = MODE == kWeight;
-    constexpr bool b_mn = MODE != kFwd;
+    constexpr bool b_mn = !fwd;
     const std::uint32_t idesc = umma::idesc_bf16(kRows, N, a_mn, b_mn);
 
     // Gathers run kAhead chunks in front of the MMA as asynchronous copies;
@@ -375,7 +420,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
                 v[i] = 0.f;
             }
         }
-        if (MODE == kFwd && a.out_f32) {
+        if (fwd && a.out_f32) {
             if (row < a.m_total) {
                 float4* dst = reinterpret_cast<float4*>(a.out_f32 + row * a.cout + c0);
 #pragma unroll
@@ -384,7 +429,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
                 }
             }
         }
-        else if (MODE == kFwd) {
+        else if (fwd) {
             if (row < a.m_total) {
                 __align__(16) bf16 h[16];
 #pragma unroll
@@ -572,7 +617,8 @@ __global__ void assemble_kernel(const bf16* crops, const std::uint32_t* crop_ind
 
 // First-layer activation from its two linear halves: the item channel's sums
 // (per sample) plus the layout channel's sums (shared by every sample).  One
-// thread per 8 channels of one voxel (cout is a multiple of 8).
+// thread per 8 channels of one voxel (cout is a multiple of 8).  A null
+// item_half stands for zero item sums (the voxels no item reaches).
 __global__ void combine_first_kernel(const float* __restrict__ item_half, const float* __restrict__ crop_half,
                                      const float* __restrict__ bias, int batch, int cout, bf16* __restrict__ act)
 {
@@ -585,7 +631,9 @@ __global__ void combine_first_kernel(const float* __restrict__ item_half, const 
         const int c0 = static_cast<int>(j % groups) * 8;
         const float4* a = reinterpret_cast<const float4*>(item_half + i * 8);
         const float4* c = reinterpret_cast<const float4*>(crop_half + j * 8);
-        const float4 a0 = __ldcs(a), a1 = __ldcs(a + 1), b0 = c[0], b1 = c[1];
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 a0 = item_half ? __ldcs(a) : zero, a1 = item_half ? __ldcs(a + 1) : zero;
+        const float4 b0 = c[0], b1 = c[1];
         const float v[8] = { a0.x + b0.x, a0.y + b0.y, a0.z + b0.z, a0.w + b0.w,
                              a1.x + b1.x, a1.y + b1.y, a1.z + b1.z, a1.w + b1.w };
         __align__(16) bf16 h[8];
@@ -594,6 +642,108 @@ __global__ void combine_first_kernel(const float* __restrict__ item_half, const 
             h[k] = __float2bfloat16_rn(fmaxf(v[k] + bias[c0 + k], 0.f));
         }
         reinterpret_cast<uint4*>(act)[i] = *reinterpret_cast<const uint4*>(h);
+    }
+}
+
+// The corner box that holds every non-zero voxel of `batch` pooled item
+// channels ([batch][32^3], x fastest): support[a] = 1 + the largest
+// coordinate along axis a of a non-zero voxel (0 when every voxel is zero).
+__global__ void item_support_kernel(const bf16* __restrict__ items, int batch, unsigned* __restrict__ support)
+{
+    unsigned hi[3] = { 0u, 0u, 0u };
+    const long long total = static_cast<long long>(batch) * kProposalVoxels;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        if (__bfloat162float(items[i]) != 0.f) {
+            const int v = static_cast<int>(i % kProposalVoxels);
+            hi[0] = max(hi[0], static_cast<unsigned>(v % kProposalGrid) + 1u);
+            hi[1] = max(hi[1], static_cast<unsigned>((v / kProposalGrid) % kProposalGrid) + 1u);
+            hi[2] = max(hi[2], static_cast<unsigned>(v / (kProposalGrid * kProposalGrid)) + 1u);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int o = 16; o > 0; o >>= 1) {
+            hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+        if ((threadIdx.x & 31) == 0 && hi[a]) {
+            atomicMax(support + a, hi[a]);
+        }
+    }
+}
+
+// Network inputs of the item channels inside a corner box: x[b][v] =
+// (0, items[b][voxel v of the box]), 2 channels, box voxels x fastest.
+__global__ void assemble_box_kernel(const bf16* __restrict__ items, int batch, int b0, int b1, int b2,
+                                    bf16* __restrict__ x)
+{
+    const int vol = b0 * b1 * b2;
+    const long long total = static_cast<long long>(batch) * vol;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long b = i / vol;
+        const int r = static_cast<int>(i % vol);
+        const int vx = r % b0, vy = (r / b0) % b1, vz = r / (b0 * b1);
+        __nv_bfloat162 pair;
+        pair.x = __float2bfloat16_rn(0.f);
+        pair.y = items[b * kProposalVoxels + (vz * kProposalGrid + vy) * kProposalGrid + vx];
+        reinterpret_cast<__nv_bfloat162*>(x)[i] = pair;
+    }
+}
+
+// First-layer activations of the corner box from the item channel's sums
+// over the box ([batch][box voxels][cout]) and the layout channel's sums
+// ([32^3][cout]), with the expression of combine_first_kernel.
+__global__ void combine_box_kernel(const float* __restrict__ item_box, const float* __restrict__ crop_half,
+                                   const float* __restrict__ bias, int batch, int cout, int b0, int b1, int b2,
+                                   bf16* __restrict__ act)
+{
+    const int groups = cout / 8;
+    const int vol = b0 * b1 * b2;
+    const long long total = static_cast<long long>(batch) * vol * groups;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int g = static_cast<int>(i % groups);
+        const int r = static_cast<int>((i / groups) % vol);
+        const int vx = r % b0, vy = (r / b0) % b1, vz = r / (b0 * b1);
+        const long long voxel = (vz * kProposalGrid + vy) * kProposalGrid + vx;
+        const int c0 = g * 8;
+        const float4* a = reinterpret_cast<const float4*>(item_box + i * 8);
+        const float4* c = reinterpret_cast<const float4*>(crop_half + voxel * cout + c0);
+        const float4 a0 = a[0], a1 = a[1], q0 = c[0], q1 = c[1];
+        const float v[8] = { a0.x + q0.x, a0.y + q0.y, a0.z + q0.z, a0.w + q0.w,
+                             a1.x + q1.x, a1.y + q1.y, a1.z + q1.z, a1.w + q1.w };
+        __align__(16) bf16 h[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            h[k] = __float2bfloat16_rn(fmaxf(v[k] + bias[c0 + k], 0.f));
+        }
+        reinterpret_cast<uint4*>(act)[i] = *reinterpret_cast<const uint4*>(h);
+    }
+}
+
+// Last-layer activations of every sample ([batch][side^3][c]) from the shared
+// ones ([side^3][c]) and the corner box's ([batch][box voxels][c]).
+__global__ void expand_box_kernel(const bf16* __restrict__ shared, const bf16* __restrict__ box, int batch, int side,
+                                  int c, int b0, int b1, int b2, bf16* __restrict__ act)
+{
+    const int groups = c / 8;
+    const int voxels = side * side * side;
+    const int vol = b0 * b1 * b2;
+    const long long total = static_cast<long long>(batch) * voxels * groups;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int g = static_cast<int>(i % groups);
+        const int v = static_cast<int>((i / groups) % voxels);
+        const long long n = i / (static_cast<long long>(groups) * voxels);
+        const int x = v % side, y = (v / side) % side, z = v / (side * side);
+        const uint4* src;
+        if (x < b0 && y < b1 && z < b2) {
+            src = reinterpret_cast<const uint4*>(box + ((n * vol + (z * b1 + y) * b0 + x) * c)) + g;
+        }
+        else {
+            src = reinterpret_cast<const uint4*>(shared + static_cast<long long>(v) * c) + g;
+        }
+        reinterpret_cast<uint4*>(act)[i] = *src;
     }
 }
 
@@ -689,6 +839,21 @@ struct ProposalNet {
     std::uint32_t item_half_batch {};
     std::uint64_t item_half_version {};
     float* crop_half {};
+    bool item_half_box {};  // item_half holds the corner-box layout below
+    // Corner-box trunk of the session path (proposal_predict): the item
+    // channels' support, each layer's output box, the per-sample box
+    // activations and the activations shared by every sample.
+    unsigned* support {};
+    int box[kProposalLayers][3] {};
+    int item_box[3] {};
+    bf16* x_item {};
+    std::size_t x_item_capacity {};
+    bf16* x_crop {};
+    bf16* act_box[kProposalLayers] {};
+    std::size_t act_box_capacity[kProposalLayers] {};
+    bf16* act_shared[kProposalLayers] {};
+    bf16* box_last {};
+    std::size_t box_last_capacity {};
     std::vector<void*> owned;
 };
 
@@ -769,6 +934,22 @@ int ensure_batch(ProposalNet* net, std::uint32_t batch)
     return kOk;
 }
 
+// Grows a device buffer to at least `count` elements (contents discarded).
+template <typename T>
+int reserve(ProposalNet* net, T*& p, std::size_t& capacity, std::size_t count)
+{
+    if (p && count <= capacity) {
+        return kOk;
+    }
+    release(net, p);
+    capacity = 0;
+    if (int status = alloc(net, p, count)) {
+        return status;
+    }
+    capacity = count;
+    return kOk;
+}
+
 int grid_for(long long n, int threads = 256)
 {
     const long long g = (n + threads - 1) / threads;
@@ -812,6 +993,32 @@ void launch_conv_forward(spk_context* ctx, ProposalNet* net, int l, std::uint32_
     const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
     const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
     conv_kernel<kFwd><<<blocks, kThreads, smem, ctx->stream>>>(a);
+    ctx->launches++;
+}
+
+// Forward layer l over the corner box `box_out` of every sample (kFwdBox).
+void launch_conv_box(spk_context* ctx, ProposalNet* net, int l, std::uint32_t batch, const bf16* x,
+                     const int (&box_in)[3], const bf16* x_shared, const int (&box_out)[3], bf16* out,
+                     float* out_f32)
+{
+    ConvArgs a = layer_args(net, l, batch);
+    a.x = x;
+    a.x_shared = x_shared;
+    a.out = out;
+    a.out_f32 = out_f32;
+    a.box_in_vol = 1;
+    a.box_out_vol = 1;
+    for (int i = 0; i < 3; ++i) {
+        a.box_in[i] = box_in[i];
+        a.box_out[i] = box_out[i];
+        a.box_in_vol *= box_in[i];
+        a.box_out_vol *= box_out[i];
+    }
+    a.m_total = static_cast<long long>(batch) * a.box_out_vol;
+    a.k_total = a.kw;
+    const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
+    const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
+    conv_kernel<kFwdBox><<<blocks, kThreads, smem, ctx->stream>>>(a);
     ctx->launches++;
 }
 
@@ -938,12 +1145,134 @@ std::uint64_t proposal_parameter_count()
     return n + 64 + 1;
 }
 
+namespace {
+
+// One layout scored against a fixed set of items, by the corner-box trunk.
+// Each item channel is zero outside a corner box of the 32^3 grid (the
+// pooled item is corner aligned and small), so every layer's output is the
+// same for all samples outside a corner box of its own: a voxel of layer l
+// depends on the item only if its 3^3 window, at its stride, reaches the
+// box of layer l - 1.  The layers therefore run once on the layout alone
+// (one sample, item sums zero) and, per sample, only over their boxes,
+// reading the layout-only activations wherever a window leaves the box.
+// Every output row is the same dot product in the same K order as in the
+// full forward, so the predictions equal the full split forward's.
+int predict_box(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const bf16* crops, const bf16* items,
+                std::uint64_t items_tag, float* pred)
+{
+    set_smem_attribute<kFwd>();
+    set_smem_attribute<kFwdBox>();
+    const int c1 = kProposalSpec[0].cout;
+    int status = kOk;
+    if (net->item_half_tag != items_tag || net->item_half_batch != batch || net->item_half_version != net->version ||
+        !net->item_half_box) {
+        if (!net->support && (status = alloc(net, net->support, 3))) {
+            return status;
+        }
+        cudaMemsetAsync(net->support, 0, 3 * sizeof(unsigned), ctx->stream);
+        item_support_kernel<<<grid_for(static_cast<long long>(batch) * kProposalVoxels), 256, 0, ctx->stream>>>(
+            items, static_cast<int>(batch), net->support);
+        unsigned support[3] {};
+        if (cudaMemcpyAsync(support, net->support, sizeof(support), cudaMemcpyDeviceToHost, ctx->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return kCuda;
+        }
+        ctx->launches++;
+        for (int a = 0; a < 3; ++a) {
+            net->item_box[a] = static_cast<int>(support[a]);
+            int r = net->item_box[a];
+            for (int l = 0; l < kProposalLayers; ++l) {
+                const ProposalLayer& L = kProposalSpec[l];
+                r = std::min(r / L.stride + 1, out_side(L));  // output o reads o * stride - 1 .. o * stride + 1
+                net->box[l][a] = r;
+            }
+        }
+        const std::size_t item_vol = static_cast<std::size_t>(net->item_box[0]) * net->item_box[1] * net->item_box[2];
+        const std::size_t vol0 = static_cast<std::size_t>(net->box[0][0]) * net->box[0][1] * net->box[0][2];
+        if ((status = reserve(net, net->x_item, net->x_item_capacity, batch * item_vol * 2)) ||
+            (status = reserve(net, net->item_half, net->item_half_capacity, batch * vol0 * c1))) {
+            return status;
+        }
+        if (item_vol) {
+            assemble_box_kernel<<<grid_for(static_cast<long long>(batch * item_vol)), 256, 0, ctx->stream>>>(
+                items, static_cast<int>(batch), net->item_box[0], net->item_box[1], net->item_box[2], net->x_item);
+            ctx->launches++;
+        }
+        launch_conv_box(ctx, net, 0, batch, net->x_item, net->item_box, nullptr, net->box[0], nullptr,
+                        net->item_half);
+        net->item_half_tag = items_tag;
+        net->item_half_batch = batch;
+        net->item_half_version = net->version;
+        net->item_half_box = true;
+    }
+    if ((!net->x_crop && (status = alloc(net, net->x_crop, static_cast<std::size_t>(kProposalVoxels) * 2))) ||
+        (!net->crop_half && (status = alloc(net, net->crop_half, static_cast<std::size_t>(kProposalVoxels) * c1)))) {
+        return status;
+    }
+    for (int l = 0; l < kProposalLayers; ++l) {
+        const ProposalLayer& L = kProposalSpec[l];
+        const std::size_t so = static_cast<std::size_t>(out_side(L));
+        const std::size_t vol = static_cast<std::size_t>(net->box[l][0]) * net->box[l][1] * net->box[l][2];
+        if ((!net->act_shared[l] && (status = alloc(net, net->act_shared[l], so * so * so * L.cout))) ||
+            (status = reserve(net, net->act_box[l], net->act_box_capacity[l], batch * vol * L.cout))) {
+            return status;
+        }
+    }
+    const int s3 = out_side(kProposalSpec[kProposalLayers - 1]);
+    const int c3 = kProposalSpec[kProposalLayers - 1].cout;
+    if ((status = reserve(net, net->box_last, net->box_last_capacity,
+                          static_cast<std::size_t>(batch) * s3 * s3 * s3 * c3))) {
+        return status;
+    }
+    // The layout's first-layer sums (one sample, item channel zero).
+    assemble_kernel<<<grid_for(kProposalVoxels), 256, 0, ctx->stream>>>(crops, nullptr, nullptr, nullptr, 1,
+                                                                        net->x_crop);
+    launch_conv_forward(ctx, net, 0, 1, net->x_crop, nullptr, net->crop_half);
+    const float* bias0 = net->params + net->b_off[0];
+    combine_first_kernel<<<grid_for(static_cast<long long>(kProposalVoxels) * c1 / 8), 256, 0, ctx->stream>>>(
+        nullptr, net->crop_half, bias0, 1, c1, net->act_shared[0]);
+    const long long box0 = static_cast<long long>(batch) * net->box[0][0] * net->box[0][1] * net->box[0][2];
+    combine_box_kernel<<<grid_for(box0 * c1 / 8), 256, 0, ctx->stream>>>(
+        net->item_half, net->crop_half, bias0, static_cast<int>(batch), c1, net->box[0][0], net->box[0][1],
+        net->box[0][2], net->act_box[0]);
+    ctx->launches += 3;
+    for (int l = 1; l < kProposalLayers; ++l) {
+        launch_conv_forward(ctx, net, l, 1, net->act_shared[l - 1], net->act_shared[l], nullptr);
+        launch_conv_box(ctx, net, l, batch, net->act_box[l - 1], net->box[l - 1], net->act_shared[l - 1],
+                        net->box[l], net->act_box[l], nullptr);
+    }
+    const int* b3 = net->box[kProposalLayers - 1];
+    expand_box_kernel<<<grid_for(static_cast<long long>(batch) * s3 * s3 * s3 * c3 / 8), 256, 0, ctx->stream>>>(
+        net->act_shared[kProposalLayers - 1], net->act_box[kProposalLayers - 1], static_cast<int>(batch), s3, c3,
+        b3[0], b3[1], b3[2], net->box_last);
+    head_kernel<<<batch, 64, 0, ctx->stream>>>(net->box_last, net->params + net->head_w, net->params + net->head_b,
+                                                static_cast<int>(batch), nullptr, pred, nullptr, nullptr, nullptr,
+                                                nullptr);
+    ctx->launches += 2;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+// SPK_PROPOSAL_TRUNK=full scores the session path with the full split forward
+// (every voxel of every sample), kept to check the corner-box trunk against.
+bool full_trunk()
+{
+    const char* v = std::getenv("SPK_PROPOSAL_TRUNK");
+    return v && std::strcmp(v, "full") == 0;
+}
+
+}  // namespace
+
 int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const bf16* crops,
                      const std::uint32_t* crop_index, const bf16* items, const std::uint32_t* item_index,
                      std::uint64_t items_tag, float* pred)
 {
     if (batch == 0 || batch > (1u << 16)) {
         return kInvalidArgument;  // row indices of the gathers are 32-bit
+    }
+    if (!crop_index && !item_index && crops && items && items_tag && !full_trunk()) {
+        return predict_box(ctx, net, batch, crops, items, items_tag, pred);
     }
     int status = ensure_batch(net, batch);
     if (status) {
@@ -959,7 +1288,7 @@ int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, co
         set_smem_attribute<kFwd>();
         const std::size_t half = static_cast<std::size_t>(batch) * grid1 * grid1 * grid1 * c1;
         if (net->item_half_tag != items_tag || net->item_half_batch != batch ||
-            net->item_half_version != net->version) {
+            net->item_half_version != net->version || net->item_half_box) {
             if (half > net->item_half_capacity) {
                 release(net, net->item_half);
                 net->item_half_capacity = 0;
@@ -975,6 +1304,7 @@ int proposal_predict(spk_context* ctx, ProposalNet* net, std::uint32_t batch, co
             net->item_half_tag = items_tag;
             net->item_half_batch = batch;
             net->item_half_version = net->version;
+            net->item_half_box = false;
         }
         if (!net->crop_half && (status = alloc(net, net->crop_half, static_cast<std::size_t>(kProposalVoxels) * c1))) {
             return status;
