@@ -18,6 +18,25 @@
 namespace spk {
 
 constexpr int kRegLine = 273;  // shared complex slots per line (16 x 17 + 1: bank spread)
+constexpr int kTwRow = 18;     // complex slots per twiddle row (16 + 2: bank spread of 16-byte reads)
+
+// Shared twiddles of the register FFT: the 256 roots w256^m and, for each
+// lane-in-line t, the row w256^(t k) for k < 16.  A thread reads its row
+// two roots at a time (16-byte loads); with rows 144 bytes apart, the eight
+// threads of a quarter warp that hold different t read distinct banks.
+struct RegTwiddles {
+    float2 root[256];
+    __align__(16) float2 row[16 * kTwRow];
+};
+
+// Fills `tw` from the 256 roots in global memory; a block of 256 threads
+// calls it, then synchronises before the first transform.
+__device__ __forceinline__ void load_twiddles(RegTwiddles& tw, const float2* __restrict__ twiddles)
+{
+    const int i = threadIdx.x, t = i >> 4, k = i & 15;
+    tw.root[i] = twiddles[i];
+    tw.row[t * kTwRow + k] = twiddles[(t * k) & 255];
+}
 
 template <bool INV>
 __device__ __forceinline__ void dft4(float2& a, float2& b, float2& c, float2& d)
@@ -59,6 +78,12 @@ __device__ __forceinline__ void dft16(float2 (&x)[16])
     for (int c = 1; c < 4; ++c) {
 #pragma unroll
         for (int b = 1; b < 4; ++b) {
+            if (b * c == 4) {
+                // w16^4 = -i (forward) or +i (inverse): a swap and a sign.
+                const float2 u = x[4 * c + b];
+                x[4 * c + b] = INV ? make_float2(-u.y, u.x) : make_float2(u.y, -u.x);
+                continue;
+            }
             float2 tw = w[b * c];
             if (INV) {
                 tw.y = -tw.y;
@@ -93,22 +118,31 @@ __device__ __forceinline__ void dft16(float2 (&x)[16])
 //                exchange, and only the calling warps need take part.
 enum FftSync { kBlockSync = 0, kFirstUse = 1, kHalfWarp = 2 };
 
+// v[k1] *= w256^(t k1) (conjugated for the inverse), k1 = 1..15, from the
+// thread's twiddle row.
+template <bool INV>
+__device__ __forceinline__ void twiddle_row(float2 (&v)[16], const RegTwiddles& tw, int t)
+{
+    const float4* row = reinterpret_cast<const float4*>(tw.row + t * kTwRow);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const float4 q = row[i];
+        if (i > 0) {
+            v[2 * i] = cmulf(v[2 * i], make_float2(q.x, INV ? -q.y : q.y));
+        }
+        v[2 * i + 1] = cmulf(v[2 * i + 1], make_float2(q.z, INV ? -q.w : q.w));
+    }
+}
+
 // Four-step 256-point transform of the line held by the 16 threads with
-// lane-in-line index t.  `line` points at this line's kRegLine shared slots;
-// tw is exp(-2 pi i m / 256), m < 256.  With kBlockSync or kFirstUse every
-// thread of the block must call it; with kHalfWarp every thread of the warp.
+// lane-in-line index t.  `line` points at this line's kRegLine shared slots.
+// With kBlockSync or kFirstUse every thread of the block must call it; with
+// kHalfWarp every thread of the warp.
 template <bool INV, int SYNC = kBlockSync>
-__device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, const float2* __restrict__ tw)
+__device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, const RegTwiddles& tw)
 {
     dft16<INV>(v);  // thread t: Y[t][k1] = v[k1]
-#pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) {
-        float2 w = tw[(t * k1) & 255];
-        if (INV) {
-            w.y = -w.y;
-        }
-        v[k1] = cmulf(v[k1], w);
-    }
+    twiddle_row<INV>(v, tw, t);
     if (SYNC == kBlockSync) {
         __syncthreads();  // the previous reader of `line` is done
     }
@@ -137,17 +171,14 @@ __device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, con
 // n1 then has two non-zero terms, Y[k1] = a + b w16^k1; the rest is the
 // four-step transform above.  Output distribution as fft256.
 __device__ __forceinline__ void fft256_first32(float2 a, float2 b, float2 (&v)[16], float2* line, int t,
-                                               const float2* __restrict__ tw)
+                                               const RegTwiddles& tw)
 {
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
-        const float2 w = tw[16 * k1];  // w16^k1 = w256^(16 k1)
+        const float2 w = tw.root[16 * k1];  // w16^k1 = w256^(16 k1)
         v[k1] = make_float2(a.x + b.x * w.x - b.y * w.y, a.y + b.x * w.y + b.y * w.x);
     }
-#pragma unroll
-    for (int k1 = 1; k1 < 16; ++k1) {
-        v[k1] = cmulf(v[k1], tw[(t * k1) & 255]);
-    }
+    twiddle_row<false>(v, tw, t);
     __syncthreads();  // the previous reader of `line` is done
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {

@@ -370,9 +370,9 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
                                                        float2* __restrict__ inter, int K2, int legal_z,
                                                        const float2* __restrict__ twiddles)
 {
-    __shared__ float2 tw[256];
+    __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const int j = threadIdx.x & 15;  // column within the group (coalesced direction)
     const int t = threadIdx.x >> 4;  // lane within the line
@@ -418,9 +418,9 @@ __global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __re
                                                              const PassABatch batch,
                                                              const float2* __restrict__ twiddles)
 {
-    __shared__ float2 tw[256];
+    __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const int j = threadIdx.x & 15;  // column within the group (coalesced direction)
     const int t = threadIdx.x >> 4;  // lane within the line
@@ -492,10 +492,10 @@ __global__ void __launch_bounds__(256) env_row256_kernel(float2* __restrict__ sp
                                                         const float2* __restrict__ twiddles,
                                                         double* __restrict__ norm_partial)
 {
-    __shared__ float2 tw[256];
+    __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
     __shared__ double red[256];
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const int t = threadIdx.x & 15, j = threadIdx.x >> 4;
     const int row = blockIdx.x * 16 + j;  // y + 256 z
@@ -538,9 +538,9 @@ __global__ void __launch_bounds__(256) env_column256_kernel(float2* __restrict__
                                                            long long other_stride, float scale,
                                                            const float2* __restrict__ twiddles)
 {
-    __shared__ float2 tw[256];
+    __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const int j = threadIdx.x & 15, t = threadIdx.x >> 4;
     const long long col = 16 * (blockIdx.x & 15) + j + other_stride * (blockIdx.x >> 4);
@@ -559,9 +559,9 @@ __global__ void __launch_bounds__(256) env_column256_kernel(float2* __restrict__
 __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ inter, int legal_y,
                                                          const float2* __restrict__ twiddles)
 {
-    __shared__ float2 tw[256];
+    __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const int j = threadIdx.x & 15;
     const int t = threadIdx.x >> 4;
@@ -604,7 +604,7 @@ struct B2Shared {
 // Thread (row j = threadIdx / 16, lane t = threadIdx % 16) holds in v[n1]
 // its row's value at kx = 16 n1 + t; `valid` rows are (y, zz).  Every thread
 // of the block calls it; it may be called again for the next 16 rows.
-__device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+__device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* lines, const RegTwiddles& tw, B2Shared& sh,
                                            bool valid, int y, int zz, int legal_x, int legal_y,
                                            const double* __restrict__ t65, double inv_occ, int mode, float target,
                                            double threshold, double cursor_floor,
@@ -647,8 +647,11 @@ __device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* line
         bool take = false;
         if (valid && x < legal_x) {
             const float2 w = line[x];
-            residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
-            if (fabsf(w.x - target) < 0.5f && !(w.y < skip)) {
+            // Under the residual guard (< 0.25) the rounded value is the
+            // overlap count, so the rounding doubles as the feasibility test.
+            const float rounded = rintf(w.x);
+            residual = fmaxf(residual, fabsf(w.x - rounded));
+            if (rounded == target && !(w.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
                 if (score >= cursor_floor) {
                     key = make_key(score, row_index + x);
@@ -810,7 +813,7 @@ __device__ __forceinline__ void b2_rows256_generic(float2 (&v)[16], float2* line
 // in shared memory; `present` marks those slots, so the histogram and the
 // emission visit only them.  Same keys, same emission rule as the generic
 // path.
-__device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+__device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines, const RegTwiddles& tw, B2Shared& sh,
                                                   bool valid, int y, int zz, int legal_x, int legal_y,
                                                   const double* __restrict__ t65, double inv_occ, float target,
                                                   double cursor_floor, unsigned long long* __restrict__ keys,
@@ -844,8 +847,11 @@ __device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines
         const int x = t + 16 * m2;
         const float2 w = v[m2];
         if (valid && x < legal_x) {
-            residual = fmaxf(residual, fabsf(w.x - rintf(w.x)));
-            if (fabsf(w.x - target) < 0.5f && !(w.y < skip)) {
+            // Under the residual guard (< 0.25) the rounded value is the
+            // overlap count, so the rounding doubles as the feasibility test.
+            const float rounded = rintf(w.x);
+            residual = fmaxf(residual, fabsf(w.x - rounded));
+            if (rounded == target && !(w.y < skip)) {
                 const double score = t65z - 0.35 * (static_cast<double>(w.y) * inv_occ);
                 if (score >= cursor_floor) {
                     const unsigned long long key = make_key(score, row_index + x);
@@ -975,7 +981,7 @@ __device__ __forceinline__ void b2_rows256_select(float2 (&v)[16], float2* lines
 // Mode 2 of the epilogue: the histogram of the 16 rows' rounded overlap
 // counts, gathered in shared memory and added to the request's `bins` u32
 // bins in `hist` (the last bin holds every larger count).
-__device__ __forceinline__ void b2_rows256_hist(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+__device__ __forceinline__ void b2_rows256_hist(float2 (&v)[16], float2* lines, const RegTwiddles& tw, B2Shared& sh,
                                                 bool valid, int legal_x, unsigned int* __restrict__ hist,
                                                 unsigned int bins, unsigned long long* __restrict__ resid)
 {
@@ -1022,7 +1028,7 @@ __device__ __forceinline__ void b2_rows256_hist(float2 (&v)[16], float2* lines, 
 
 // Mode 0 (first pass) takes the register path, mode 1 (threshold pass) the
 // generic one, mode 2 the count histogram.
-__device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const float2* tw, B2Shared& sh,
+__device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const RegTwiddles& tw, B2Shared& sh,
                                            bool valid, int y, int zz, int legal_x, int legal_y,
                                            const double* __restrict__ t65, double inv_occ, int mode, float target,
                                            double threshold, double cursor_floor,
@@ -1053,10 +1059,10 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
                                                          unsigned long long* __restrict__ tau,
                                                          unsigned long long* __restrict__ resid)
 {
-    __shared__ float2 tw[256];
+    __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
     __shared__ B2Shared sh;
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const int t = threadIdx.x & 15;
     const int j = threadIdx.x >> 4;
@@ -1083,7 +1089,8 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
 // transform and the epilogue of pass B2 on them.  The legal-row
 // intermediate that B1 wrote and B2 read back never reaches HBM.
 constexpr int kFusedCluster = 8;
-constexpr std::size_t kFusedSmem = sizeof(float2) * (256 * 32 + 16 * kRegLine + 256) + sizeof(B2Shared);
+constexpr std::size_t kFusedSmem = sizeof(float2) * (256 * 32 + 16 * kRegLine) + sizeof(RegTwiddles) + sizeof(B2Shared);
+static_assert(sizeof(float2) * (256 * 32 + 16 * kRegLine) % 16 == 0, "the twiddle rows need 16-byte alignment");
 
 __global__ void __cluster_dims__(kFusedCluster, 1, 1) __launch_bounds__(256)
     pass_b_fused_256_kernel(const float2* __restrict__ inter, int legal_x, int legal_y,
@@ -1096,12 +1103,12 @@ __global__ void __cluster_dims__(kFusedCluster, 1, 1) __launch_bounds__(256)
     extern __shared__ __align__(16) unsigned char fused_smem[];
     float2* cols = reinterpret_cast<float2*>(fused_smem);  // [y < 256][kx_local < 32]
     float2* lines = cols + 256 * 32;
-    float2* tw = lines + 16 * kRegLine;
-    B2Shared& sh = *reinterpret_cast<B2Shared*>(tw + 256);
+    RegTwiddles& tw = *reinterpret_cast<RegTwiddles*>(lines + 16 * kRegLine);
+    B2Shared& sh = *reinterpret_cast<B2Shared*>(&tw + 1);
     cg::cluster_group cluster = cg::this_cluster();
     const unsigned int rank = cluster.block_rank();
     const int zz = static_cast<int>(blockIdx.x / kFusedCluster);
-    tw[threadIdx.x] = twiddles[threadIdx.x];
+    load_twiddles(tw, twiddles);
     __syncthreads();
     const long long plane = 65536LL * zz;
     // Inverse y of this CTA's 32 columns, 16 at a time (coalesced along kx).

@@ -854,6 +854,10 @@ struct ProposalNet {
     bf16* act_shared[kProposalLayers] {};
     bf16* box_last {};
     std::size_t box_last_capacity {};
+    // The layout-only layers run on a stream of their own, ahead of the
+    // per-sample boxes that read them (one event per layer).
+    cudaStream_t side {};
+    cudaEvent_t layer_done[kProposalLayers] {};
     std::vector<void*> owned;
 };
 
@@ -982,7 +986,7 @@ ConvArgs layer_args(ProposalNet* net, int l, std::uint32_t batch)
 }
 
 void launch_conv_forward(spk_context* ctx, ProposalNet* net, int l, std::uint32_t batch, const bf16* x, bf16* out,
-                         float* out_f32)
+                         float* out_f32, cudaStream_t stream = nullptr)
 {
     ConvArgs a = layer_args(net, l, batch);
     a.x = x;
@@ -992,7 +996,7 @@ void launch_conv_forward(spk_context* ctx, ProposalNet* net, int l, std::uint32_
     a.k_total = a.kw;
     const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
     const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
-    conv_kernel<kFwd><<<blocks, kThreads, smem, ctx->stream>>>(a);
+    conv_kernel<kFwd><<<blocks, kThreads, smem, stream ? stream : ctx->stream>>>(a);
     ctx->launches++;
 }
 
@@ -1233,16 +1237,50 @@ int predict_box(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const b
     const float* bias0 = net->params + net->b_off[0];
     combine_first_kernel<<<grid_for(static_cast<long long>(kProposalVoxels) * c1 / 8), 256, 0, ctx->stream>>>(
         nullptr, net->crop_half, bias0, 1, c1, net->act_shared[0]);
+    ctx->launches += 2;
+    // A layer's layout-only activations are read only where its box does not
+    // cover it (boxes never shrink back once they cover their layer).
+    bool shared_needed[kProposalLayers];
+    for (int l = 0; l < kProposalLayers; ++l) {
+        const int so = out_side(kProposalSpec[l]);
+        shared_needed[l] = net->box[l][0] < so || net->box[l][1] < so || net->box[l][2] < so;
+    }
+    if (!net->side) {
+        if (cudaStreamCreateWithFlags(&net->side, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            net->side = nullptr;
+            return kCuda;
+        }
+        for (auto& e : net->layer_done) {
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                return kCuda;
+            }
+        }
+    }
+    cudaEventRecord(net->layer_done[0], ctx->stream);
+    cudaStreamWaitEvent(net->side, net->layer_done[0], 0);
+    for (int l = 1; l < kProposalLayers; ++l) {
+        if (shared_needed[l]) {
+            launch_conv_forward(ctx, net, l, 1, net->act_shared[l - 1], net->act_shared[l], nullptr, net->side);
+        }
+        cudaEventRecord(net->layer_done[l], net->side);
+    }
     const long long box0 = static_cast<long long>(batch) * net->box[0][0] * net->box[0][1] * net->box[0][2];
     combine_box_kernel<<<grid_for(box0 * c1 / 8), 256, 0, ctx->stream>>>(
         net->item_half, net->crop_half, bias0, static_cast<int>(batch), c1, net->box[0][0], net->box[0][1],
         net->box[0][2], net->act_box[0]);
-    ctx->launches += 3;
+    ctx->launches++;
     for (int l = 1; l < kProposalLayers; ++l) {
-        launch_conv_forward(ctx, net, l, 1, net->act_shared[l - 1], net->act_shared[l], nullptr);
-        launch_conv_box(ctx, net, l, batch, net->act_box[l - 1], net->box[l - 1], net->act_shared[l - 1],
-                        net->box[l], net->act_box[l], nullptr);
+        if (l >= 2) {
+            cudaStreamWaitEvent(ctx->stream, net->layer_done[l - 1], 0);
+        }
+        launch_conv_box(ctx, net, l, batch, net->act_box[l - 1], net->box[l - 1],
+                        shared_needed[l - 1] ? net->act_shared[l - 1] : nullptr, net->box[l], net->act_box[l],
+                        nullptr);
     }
+    // Joins the side stream (the next call rewrites what it read).
+    cudaStreamWaitEvent(ctx->stream, net->layer_done[kProposalLayers - 1], 0);
     const int* b3 = net->box[kProposalLayers - 1];
     expand_box_kernel<<<grid_for(static_cast<long long>(batch) * s3 * s3 * s3 * c3 / 8), 256, 0, ctx->stream>>>(
         net->act_shared[kProposalLayers - 1], net->act_box[kProposalLayers - 1], static_cast<int>(batch), s3, c3,
@@ -1456,6 +1494,15 @@ void spk_proposal_destroy(spk_proposal* p)
         return;
     }
     cudaSetDevice(p->net.device);
+    if (p->net.side) {
+        cudaStreamSynchronize(p->net.side);
+        for (auto& e : p->net.layer_done) {
+            if (e) {
+                cudaEventDestroy(e);
+            }
+        }
+        cudaStreamDestroy(p->net.side);
+    }
     for (void* q : p->net.owned) {
         cudaFree(q);
     }
