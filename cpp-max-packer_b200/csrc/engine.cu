@@ -800,6 +800,32 @@ int spk_oriented_bounds(const spk_mesh* object, const double q[4], double bounds
     }
 }
 
+int spk_posed_bounds(const spk_mesh* object, const double* translations_mm, const double* q_xyzw, uint64_t count,
+                     double* bounds_min, double* bounds_max, uint8_t* finite)
+{
+    try {
+        if (!valid_mesh(object) || (count && (!translations_mm || !q_xyzw || !bounds_min || !bounds_max || !finite))) {
+            return kFieldInput;
+        }
+        const geo::Mesh mesh = to_mesh(*object);
+        for (uint64_t i = 0; i < count; ++i) {
+            geo::Bounds b;
+            const double* t = translations_mm + 3 * i;
+            const double* q = q_xyzw + 4 * i;
+            const bool ok = geo::posed_bounds(mesh, { t[0], t[1], t[2] }, { q[0], q[1], q[2], q[3] }, b);
+            finite[i] = ok ? 1 : 0;
+            for (int a = 0; a < 3; ++a) {
+                bounds_min[3 * i + a] = ok ? b.min[a] : 0.0;
+                bounds_max[3 * i + a] = ok ? b.max[a] : 0.0;
+            }
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
 int spk_environment_window(const double bounds[6], const double origin[3], double pitch, int64_t first[3],
                            uint32_t shape[3])
 {

@@ -36,7 +36,7 @@ int blocks_for(long long n, int threads)
 // One thread per (face, cell) pair.  `offsets` is the exclusive prefix sum of
 // the faces' clipped cell-range sizes (outside faces count 0), so small faces
 // pack densely into warps instead of leaving most lanes of a per-face warp idle.
-__global__ void raster_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint,
+__global__ void __launch_bounds__(128, 6) raster_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint,
                               const geo::FaceRange* __restrict__ ranges, const long long* __restrict__ offsets,
                               int faces, long long total, FieldWindow w, std::uint8_t* __restrict__ cells,
                               int* __restrict__ error)
@@ -301,7 +301,8 @@ int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& 
     cudaMemsetAsync(d_misc, 0, 64, st);
     const int threads = 256;
     if (total > 0) {
-        // 128-thread blocks: at ~146 registers a thread, three blocks fit an SM.
+        // 128-thread blocks, six to an SM: the SAT's dependent FP64 chains need
+        // the resident warps more than the registers that spill (measured).
         raster_kernel<<<blocks_for(total, 128), 128, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets,
                                                                       static_cast<int>(F), total, w, d_cells, d_misc);
     }

@@ -1097,6 +1097,67 @@ bool oriented_bounds(const Mesh& mesh, const Quat& q, Bounds& out)
     return !first;
 }
 
+// validation_kernel::posed_bounds (validation_kernel.cpp:1000-1088) with
+// transformed_source_box (:949-997): the conservative bounds the validator's
+// pair loop tests.  Cardinal rotations map the source box by the signed axis
+// permutation and move each bound one ulp outward; every other rotation
+// encloses the eight corners of the source box by their transformed
+// intervals.  False where the reference returns no bounds.
+bool posed_bounds(const Mesh& mesh, const Vec3& translation, const Quat& q, Bounds& out)
+{
+    if (!finite_pose(translation, q)) {
+        return false;
+    }
+    const auto transform = rotation_transform(q);
+    if (!transform) {
+        return false;
+    }
+    const Bounds& local = mesh.bounds;
+    constexpr double inf = std::numeric_limits<double>::infinity();
+    if (transform->exact_cardinal) {
+        for (int axis = 0; axis < 3; ++axis) {
+            const int source = transform->source_axis[axis], sign = transform->sign[axis];
+            const double low = translation[axis] + sign * (sign > 0 ? local.min[source] : local.max[source]);
+            const double high = translation[axis] + sign * (sign > 0 ? local.max[source] : local.min[source]);
+            out.min[axis] = std::nextafter(low, -inf);
+            out.max[axis] = std::nextafter(high, inf);
+        }
+    }
+    else {
+        for (int axis = 0; axis < 3; ++axis) {
+            if (!std::isfinite(local.min[axis]) || !std::isfinite(local.max[axis]) || local.min[axis] > local.max[axis]) {
+                return false;
+            }
+        }
+        Interval rotation[3][3];
+        rotation_intervals(q, rotation);
+        for (int axis = 0; axis < 3; ++axis) {
+            out.min[axis] = inf;
+            out.max[axis] = -inf;
+        }
+        for (unsigned corner = 0; corner != 8; ++corner) {
+            Vec3 point;
+            for (unsigned axis = 0; axis != 3; ++axis) {
+                point[axis] = corner & (1U << axis) ? local.max[axis] : local.min[axis];
+            }
+            for (int axis = 0; axis < 3; ++axis) {
+                const Interval interval = transformed_interval(point, translation, rotation, axis);
+                if (!interval.valid) {
+                    return false;
+                }
+                out.min[axis] = std::min(out.min[axis], interval.low);
+                out.max[axis] = std::max(out.max[axis], interval.high);
+            }
+        }
+    }
+    for (int axis = 0; axis < 3; ++axis) {
+        if (!std::isfinite(out.min[axis]) || !std::isfinite(out.max[axis])) {
+            return false;
+        }
+    }
+    return true;
+}
+
 std::array<Quat, 24> cube_catalog()
 {
     using Matrix = std::array<int, 9>;

@@ -123,6 +123,8 @@ std::vector<std::array<std::int64_t, 3>> make_stencil(std::uint64_t halo, double
 // physical_bounds (validation_kernel.cpp:1099-1242): oriented bounds of the
 // rotated mesh (exact for signed permutations, interval hull otherwise).
 bool oriented_bounds(const Mesh& mesh, const Quat& q, Bounds& out);
+// validation_kernel::posed_bounds (validation_kernel.cpp:1000-1088).
+bool posed_bounds(const Mesh& mesh, const Vec3& translation, const Quat& q, Bounds& out);
 
 // Orientation catalogs (engine/pack_solver/src/orientation_cube.hpp:10-80,
 // orientations.cpp:40-66 canonical()).

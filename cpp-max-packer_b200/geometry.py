@@ -53,6 +53,9 @@ def _declare(lib):
     lib.spk_voxelize_container.argtypes = [P, P, M, P, ctypes.c_double, P, P, ctypes.c_double, P]
     lib.spk_voxelize_placed.argtypes = [P, M, P, ctypes.c_double, P, P, P, P, ctypes.c_double, P]
     lib.spk_oriented_bounds.argtypes = [M, P, P]
+    lib.spk_posed_bounds.argtypes = [M, P, P, ctypes.c_uint64, P, P, P]
+    lib.spk_broad_phase.argtypes = [P, P, P, P, P, ctypes.c_uint64, ctypes.c_double, P, ctypes.c_uint64,
+                                    ctypes.POINTER(ctypes.c_uint64)]
     lib.spk_environment_window.argtypes = [P, P, ctypes.c_double, P, P]
     lib.spk_cube_catalog.argtypes = [P]
     lib.spk_custom_catalog.argtypes = [P, ctypes.c_uint64, P, ctypes.POINTER(ctypes.c_uint64)]
@@ -127,6 +130,42 @@ def oriented_bounds(mesh: AcceptedMesh, q_xyzw) -> np.ndarray:
     q = _arr(q_xyzw, np.float64)
     _lib.check(lib.spk_oriented_bounds(ctypes.byref(mc), q.ctypes.data, out.ctypes.data), "spk_oriented_bounds")
     return out
+
+
+def posed_bounds(mesh: AcceptedMesh, translations_mm, quaternions_xyzw):
+    """validation_kernel::posed_bounds of each pose (validation_kernel.cpp:1000-1088):
+    (min (n, 3), max (n, 3), finite (n,) bool)."""
+    lib = _lib_ready()
+    mc, keep = _mesh_c(mesh)
+    t = _arr(translations_mm, np.float64).reshape(-1, 3)
+    q = _arr(quaternions_xyzw, np.float64).reshape(-1, 4)
+    n = len(t)
+    lo, hi = np.zeros((n, 3), np.float64), np.zeros((n, 3), np.float64)
+    finite = np.zeros(n, np.uint8)
+    _lib.check(lib.spk_posed_bounds(ctypes.byref(mc), t.ctypes.data, q.ctypes.data, n, lo.ctypes.data,
+                                    hi.ctypes.data, finite.ctypes.data), "spk_posed_bounds")
+    return lo, hi, finite.astype(bool)
+
+
+def broad_phase(bounds_min, bounds_max, finite, clearance_mm: float, proven=None,
+                context: Optional[Context] = None, capacity: Optional[int] = None) -> np.ndarray:
+    """The copy pairs the validator's outward-AABB test leaves unresolved
+    (validation.cpp:404-418), (count, 2) uint32 rows (first, second) in its
+    visiting order."""
+    lib = _lib_ready()
+    context = context or default_context()
+    lo = _arr(bounds_min, np.float64).reshape(-1, 3)
+    hi = _arr(bounds_max, np.float64).reshape(-1, 3)
+    n = len(lo)
+    fin = _arr(finite, np.uint8)
+    prv = None if proven is None else _arr(proven, np.uint8)
+    cap = n * (n - 1) // 2 if capacity is None else capacity
+    out = np.zeros((max(cap, 1), 2), np.uint32)
+    count = ctypes.c_uint64()
+    _lib.check(lib.spk_broad_phase(context.handle, lo.ctypes.data, hi.ctypes.data, fin.ctypes.data,
+                                   None if prv is None else prv.ctypes.data, n, clearance_mm, out.ctypes.data, cap,
+                                   ctypes.byref(count)), "spk_broad_phase")
+    return out[:count.value].copy()
 
 
 def environment_window(bounds_mm, origin_mm, pitch_mm):

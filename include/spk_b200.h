@@ -297,6 +297,35 @@ int spk_voxelize_placed(spk_context* context, const spk_mesh* object, const doub
  * max xyz of the rotated mesh.  Host only. */
 int spk_oriented_bounds(const spk_mesh* object, const double q_xyzw[4], double bounds_mm[6]);
 
+/* ---- validator broad phase ------------------------------------------------
+ * Replaces the posed-bounds part of geometry::validate's pair loop
+ * (engine/pack_geometry/src/validation.cpp:404-418, which calls
+ * validation_kernel::bounds_pair_certificate -> separated_conservative_bounds,
+ * validation_kernel.cpp:1245-1261) for every pair of copies at once.
+ *
+ * spk_posed_bounds: validation_kernel::posed_bounds (validation_kernel.cpp:
+ * 1000-1088) of `count` poses of `object` (translation in mm, XYZW
+ * quaternion): conservative min/max corners, count x 3 each; finite[i] = 0
+ * where the reference returns no bounds (invalid pose or interval overflow;
+ * the validator then rejects the layout as indeterminate).  Host code.
+ *
+ * spk_broad_phase: the pairs (first, second), second < first, that the
+ * outward-AABB test does not certify disjoint, in the validator's visiting
+ * order (first ascending, then second), skipping pairs whose copies are both
+ * proven (validate_incremental's `proven`, may be null).  They are written
+ * to pairs (2 x uint32 each) up to `capacity`; *unresolved receives their
+ * number.  The validator's remaining certificates and exact classification
+ * run only for these pairs.  SPK_SCRATCH_LIMIT (25) when *unresolved exceeds
+ * capacity; SPK_INVALID_ARGUMENT for a clearance that is negative or not
+ * finite (the reference then certifies nothing and reports
+ * KERNEL_CLEARANCE_INVALID) or more than 2^20 copies.  Device kernels; the
+ * call returns after the pairs are on the host. */
+int spk_posed_bounds(const spk_mesh* object, const double* translations_mm, const double* q_xyzw, uint64_t count,
+                     double* bounds_min, double* bounds_max, uint8_t* finite);
+int spk_broad_phase(spk_context* context, const double* bounds_min, const double* bounds_max, const uint8_t* finite,
+                    const uint8_t* proven, uint64_t copies, double clearance_mm, uint32_t* pairs, uint64_t capacity,
+                    uint64_t* unresolved);
+
 /* Environment window of a container's bounds (spectral_pipeline.cpp:107-140). */
 int spk_environment_window(const double bounds_mm[6], const double origin_mm[3], double pitch_mm,
                            int64_t first[3], uint32_t shape[3]);

@@ -86,6 +86,21 @@ class C:
         fn(_ptr(es), _ptr(ks), _ptr(ef), _ptr(kf), _ptr(e), _ptr(k), _ptr(out), _ptr(tf), _ptr(os_))
         return tf, os_, out
 
+    def broad_phase(self, lo, hi, finite, proven, clearance, capacity=None):
+        """oracle_broad_phase: the uncertified pairs, (count, 2) uint32, in visiting order."""
+        lo = np.ascontiguousarray(lo, np.float64).reshape(-1, 3)
+        hi = np.ascontiguousarray(hi, np.float64).reshape(-1, 3)
+        n = lo.shape[0]
+        fin = np.ascontiguousarray(finite, np.uint8)
+        prv = None if proven is None else np.ascontiguousarray(proven, np.uint8)
+        cap = n * (n - 1) // 2 if capacity is None else capacity
+        out = np.zeros((max(cap, 1), 2), np.uint32)
+        self.lib.oracle_broad_phase.restype = ctypes.c_int64
+        count = self.lib.oracle_broad_phase(_ptr(lo), _ptr(hi), _ptr(fin), None if prv is None else _ptr(prv),
+                                            ctypes.c_int64(n), ctypes.c_double(clearance), _ptr(out),
+                                            ctypes.c_int64(cap))
+        return out[:min(count, cap)].copy(), int(count)
+
     def build_proximity(self, shape, occupied):
         s = np.array(shape, np.uint32)
         occ = np.ascontiguousarray(occupied, dtype=np.uint8)
@@ -214,6 +229,12 @@ class RefAsset:
         if rc:
             raise RuntimeError(self.ref._error())
         return cells
+
+    def bounds_pair(self, t1, q1, t2, q2, clearance):
+        """validation_kernel::bounds_pair_certificate: 0 none, 1 outward-aabb, 2 other, 3 indeterminate."""
+        return self.ref.lib.spkref_bounds_pair(_P(self.handle), _ptr(np.array(t1, np.float64)),
+                                               _ptr(np.array(q1, np.float64)), _ptr(np.array(t2, np.float64)),
+                                               _ptr(np.array(q2, np.float64)), ctypes.c_double(clearance))
 
     def oriented_bounds(self, q):
         out = np.zeros(6, np.float64)

@@ -11,6 +11,7 @@
 //   solver::make_orientation_catalog                          orientations.hpp:41-42
 //   solver::detail::build_spectral_pipeline                   spectral_pipeline.hpp:94-99
 //   geometry::validate                                        validation.hpp:168
+//   validation_kernel::bounds_pair_certificate                validation_kernel.hpp:177-178
 // The greedy driver below follows the non-timed page-merge loop of
 // engine/pack_solver/src/spectral.cpp:1460-1591 (run_trial) without the
 // physical refinement that starts once every voxel page is exhausted.
@@ -29,6 +30,7 @@
 
 #include "field_proximity.hpp"
 #include "spectral_pipeline.hpp"
+#include "validation_kernel.hpp"
 #include "spectrapack/compute/correlation.hpp"
 #include "spectrapack/geometry/conservative_fields.hpp"
 #include "spectrapack/geometry/physical_bounds.hpp"
@@ -364,6 +366,32 @@ int spkref_oriented_bounds(void* handle, const double* q, double* out)
         out[3 + a] = b.max[a];
     }
     return 0;
+}
+
+namespace vk = spectrapack::geometry::detail::validation_kernel;
+
+// validation_kernel::bounds_pair_certificate of two poses of the asset:
+// 0 no certificate (the validator goes on to its other certificates), 1
+// certified by the outward AABBs ("outward-aabb"), 2 certified another way,
+// 3 indeterminate, -1 a pose without bounds.
+int spkref_bounds_pair(void* handle, const double* t1, const double* q1, const double* t2, const double* q2,
+                       double clearance)
+{
+    vk::Budget budget(kHuge, kHuge);
+    const auto& solid = static_cast<Asset*>(handle)->solid;
+    const auto a = vk::posed_bounds(solid, { t1[0], t1[1], t1[2] }, { q1[0], q1[1], q1[2], q1[3] }, budget);
+    const auto b = vk::posed_bounds(solid, { t2[0], t2[1], t2[2] }, { q2[0], q2[1], q2[2], q2[3] }, budget);
+    if (!a || !b) {
+        return -1;
+    }
+    const auto c = vk::bounds_pair_certificate(*a.bounds, *b.bounds, clearance, budget);
+    if (!c) {
+        return 0;
+    }
+    if (c->material_overlap == vk::Decision::indeterminate || c->surface_gap == vk::Threshold::indeterminate) {
+        return 3;
+    }
+    return c->method == "outward-aabb" ? 1 : 2;
 }
 
 // mode: 0 fixed, 1 cube, 4 catalog (g::OrientationMode values).

@@ -16,6 +16,8 @@
  *                              correctly rounded)
  *   oracle_build_proximity     engine/pack_solver/src/field_proximity.hpp:32-132
  *   oracle_fsum                correctly rounded sum (Shewchuk expansions)
+ *   oracle_broad_phase         engine/pack_geometry/src/validation.cpp:404-418 pair order with
+ *                              separated_conservative_bounds, validation_kernel.cpp:1245-1261
  */
 #include <math.h>
 #include <stdint.h>
@@ -430,5 +432,43 @@ int oracle_page(const int64_t* env_first, const uint32_t* es, const uint8_t* occ
     free(list);
     free(terms);
     free(ones);
+    return count;
+}
+
+/* ---- validator broad phase (validation.cpp:404-418) ----
+ * The validator's pair loop visits (first, second) for first = 0..n-1 and
+ * second = 0..first-1, skipping pairs whose poses are both proven.  A pair
+ * is certified disjoint by its posed conservative bounds when, on some axis,
+ * nextafter(max + clearance, +inf) of one copy lies below the other copy's
+ * min (validation_kernel.cpp:1252-1258); copies whose bounds are not finite
+ * certify nothing.  Writes the uncertified pairs in visiting order as
+ * (first, second) uint32 pairs, up to `capacity`, and returns their count. */
+static int oracle_separated(const double* lo, const double* hi, const uint8_t* finite, int64_t i, int64_t j,
+                            double clearance)
+{
+    if (!finite[i] || !finite[j]) return 0;
+    for (int a = 0; a < 3; ++a) {
+        const double x = nextafter(hi[3 * i + a] + clearance, INFINITY);
+        const double y = nextafter(hi[3 * j + a] + clearance, INFINITY);
+        if (x < lo[3 * j + a] || y < lo[3 * i + a]) return 1;
+    }
+    return 0;
+}
+
+int64_t oracle_broad_phase(const double* lo, const double* hi, const uint8_t* finite, const uint8_t* proven,
+                           int64_t n, double clearance, uint32_t* pairs, int64_t capacity)
+{
+    int64_t count = 0;
+    for (int64_t first = 0; first < n; ++first) {
+        for (int64_t second = 0; second < first; ++second) {
+            if (proven && proven[first] && proven[second]) continue;
+            if (oracle_separated(lo, hi, finite, first, second, clearance)) continue;
+            if (count < capacity) {
+                pairs[2 * count] = (uint32_t)first;
+                pairs[2 * count + 1] = (uint32_t)second;
+            }
+            ++count;
+        }
+    }
     return count;
 }
