@@ -351,6 +351,7 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, O)
+    broad = broad_phase_line(ctx, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     if rank == 0:
         config = reference_config(args.workload, world)
@@ -385,6 +386,7 @@ def run_ours(args, rank, world, local_rank):
                          "passes": passes},
             "e2e": e2e,
             "clocks": clocks.summary(),
+            "validator_broad_phase": broad,
         }
         if learned:
             line["proposal"] = {"k": k, "weights": os.path.relpath(weights, os.path.dirname(os.path.abspath(__file__))),
@@ -398,6 +400,31 @@ def run_ours(args, rank, world, local_rank):
         net.close()
     session.close()
     ctx.close()
+
+
+def broad_phase_line(ctx, with_cpu: bool, copies: int = 3580):
+    """The validator broad phase (spk_broad_phase) on a full fill's number of
+    copies of the bench item: pairs per second through the C ABI with host
+    buffers (bounds in, unresolved pairs out), and, as its CPU baseline, the
+    oracle's plain-C pair loop on one host core over the same bounds, whose
+    pair list must be the same."""
+    bp = pkg("broad_phase_bench")
+    lo, hi, fin = bp.layout(copies)
+    pairs = copies * (copies - 1) // 2
+    seconds, got = bp.time_device(lo, hi, fin, 0.0, 10, ctx)
+    line = {"metric": "copy pairs tested per second", "copies": copies, "pairs": pairs,
+            "unresolved_pairs": int(len(got)), "value": round(pairs / seconds, 1), "ms_per_call": round(seconds * 1e3, 3),
+            "path": "spk_posed_bounds on the host, spk_broad_phase with host buffers"}
+    if with_cpu:
+        from oracle.bindings import C
+
+        t0 = time.perf_counter()
+        want, count = C().broad_phase(lo, hi, fin, None, 0.0)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(pairs / cpu_s, 1), "unit": "pairs/s", "cores": 1, "kind": "port",
+                                "sample": f"all {pairs} pairs of the same layout (oracle_broad_phase)",
+                                "same_pairs": bool(np.array_equal(got, want))}
+    return line
 
 
 def _page_worker(workload, worker, orientations, warmup_orientations, barrier, queue):

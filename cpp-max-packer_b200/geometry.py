@@ -54,6 +54,7 @@ def _declare(lib):
     lib.spk_voxelize_placed.argtypes = [P, M, P, ctypes.c_double, P, P, P, P, ctypes.c_double, P]
     lib.spk_oriented_bounds.argtypes = [M, P, P]
     lib.spk_posed_bounds.argtypes = [M, P, P, ctypes.c_uint64, P, P, P]
+    lib.spk_export_stl.argtypes = [P, M, P, P, ctypes.c_uint64, P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64)]
     lib.spk_broad_phase.argtypes = [P, P, P, P, P, ctypes.c_uint64, ctypes.c_double, P, ctypes.c_uint64,
                                     ctypes.POINTER(ctypes.c_uint64)]
     lib.spk_environment_window.argtypes = [P, P, ctypes.c_double, P, P]
@@ -166,6 +167,22 @@ def broad_phase(bounds_min, bounds_max, finite, clearance_mm: float, proven=None
                                    None if prv is None else prv.ctypes.data, n, clearance_mm, out.ctypes.data, cap,
                                    ctypes.byref(count)), "spk_broad_phase")
     return out[:count.value].copy()
+
+
+def export_stl(mesh: AcceptedMesh, translations_mm, quaternions_xyzw, context: Optional[Context] = None) -> bytes:
+    """The binary STL of the posed copies (pack_io's write_stl_stage,
+    result_export.cpp:1034-1123), computed on the device."""
+    lib = _lib_ready()
+    context = context or default_context()
+    mc, keep = _mesh_c(mesh)
+    t = _arr(translations_mm, np.float64).reshape(-1, 3)
+    q = _arr(quaternions_xyzw, np.float64).reshape(-1, 4)
+    size = 84 + 50 * len(mesh.triangles) * len(t)
+    out = np.empty(size, np.uint8)
+    got = ctypes.c_uint64()
+    _lib.check(lib.spk_export_stl(context.handle, ctypes.byref(mc), t.ctypes.data, q.ctypes.data, len(t),
+                                  out.ctypes.data, size, ctypes.byref(got)), "spk_export_stl")
+    return out[:got.value].tobytes()
 
 
 def environment_window(bounds_mm, origin_mm, pitch_mm):

@@ -326,6 +326,22 @@ int spk_broad_phase(spk_context* context, const double* bounds_min, const double
                     const uint8_t* proven, uint64_t copies, double clearance_mm, uint32_t* pairs, uint64_t capacity,
                     uint64_t* unresolved);
 
+/* ---- STL export of a placement sequence -----------------------------------
+ * Replaces write_stl_stage (engine/pack_io/src/result_export.cpp:1034-1123):
+ * the binary STL of `copies` copies of `object`, copy c posed by
+ * translation_mm[3c..3c+2] and the XYZW quaternion q_xyzw[4c..4c+3]
+ * (RigidTransform::make / apply, rigid_transform.cpp:11-42), in copy order,
+ * each copy's triangles in mesh order: an 80-byte zero header, the uint32
+ * triangle count, then 50-byte records (float32 unit normal from the float32
+ * points, the three float32 points, a zero attribute).  *size receives the
+ * file size, 84 + 50 x triangles; `out` must hold it (SPK_SCRATCH_LIMIT
+ * otherwise).  SPK_INVALID_ARGUMENT with the reference's message for a pose
+ * without a rigid transform, a coordinate that is not a finite float32, or
+ * more than 2^32 - 1 triangles.  The records are computed on the device;
+ * the call returns after they are in `out`. */
+int spk_export_stl(spk_context* context, const spk_mesh* object, const double* translations_mm,
+                   const double* q_xyzw, uint64_t copies, uint8_t* out, uint64_t capacity, uint64_t* size);
+
 /* Environment window of a container's bounds (spectral_pipeline.cpp:107-140). */
 int spk_environment_window(const double bounds_mm[6], const double origin_mm[3], double pitch_mm,
                            int64_t first[3], uint32_t shape[3]);

@@ -230,6 +230,20 @@ class RefAsset:
             raise RuntimeError(self.ref._error())
         return cells
 
+    def export_stl(self, translations, quaternions) -> bytes:
+        """The reference's STL records of the posed copies (spkref_export_stl)."""
+        t = np.ascontiguousarray(translations, np.float64).reshape(-1, 3)
+        q = np.ascontiguousarray(quaternions, np.float64).reshape(-1, 4)
+        size = ctypes.c_uint64()
+        self.ref.lib.spkref_export_stl(_P(self.handle), _ptr(t), _ptr(q), ctypes.c_uint64(len(t)), None,
+                                       ctypes.c_uint64(0), ctypes.byref(size))
+        out = np.zeros(size.value, np.uint8)
+        rc = self.ref.lib.spkref_export_stl(_P(self.handle), _ptr(t), _ptr(q), ctypes.c_uint64(len(t)), _ptr(out),
+                                            ctypes.c_uint64(size.value), ctypes.byref(size))
+        if rc:
+            raise RuntimeError(f"spkref_export_stl failed ({rc})")
+        return out.tobytes()
+
     def bounds_pair(self, t1, q1, t2, q2, clearance):
         """validation_kernel::bounds_pair_certificate: 0 none, 1 outward-aabb, 2 other, 3 indeterminate."""
         return self.ref.lib.spkref_bounds_pair(_P(self.handle), _ptr(np.array(t1, np.float64)),

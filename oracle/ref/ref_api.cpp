@@ -12,6 +12,11 @@
 //   solver::detail::build_spectral_pipeline                   spectral_pipeline.hpp:94-99
 //   geometry::validate                                        validation.hpp:168
 //   validation_kernel::bounds_pair_certificate                validation_kernel.hpp:177-178
+//   geometry::RigidTransform::make / apply                    rigid_transform.hpp:15-18
+// spkref_export_stl follows the record loop of pack_io's write_stl_stage
+// (engine/pack_io/src/result_export.cpp:1034-1123; pack_io itself needs
+// nlohmann/json and is not built here) with the reference's RigidTransform
+// and the host libm's hypot.
 // The greedy driver below follows the non-timed page-merge loop of
 // engine/pack_solver/src/spectral.cpp:1460-1591 (run_trial) without the
 // physical refinement that starts once every voxel page is exhausted.
@@ -30,6 +35,7 @@
 
 #include "field_proximity.hpp"
 #include "spectral_pipeline.hpp"
+#include "spectrapack/geometry/rigid_transform.hpp"
 #include "validation_kernel.hpp"
 #include "spectrapack/compute/correlation.hpp"
 #include "spectrapack/geometry/conservative_fields.hpp"
@@ -392,6 +398,69 @@ int spkref_bounds_pair(void* handle, const double* t1, const double* q1, const d
         return 3;
     }
     return c->method == "outward-aabb" ? 1 : 2;
+}
+
+// The binary STL of `copies` posed copies of the asset (see the header
+// comment).  1 = a pose without a rigid transform, 2 = a coordinate that is
+// not a finite float32, 3 = out too small (*size is the file size).
+int spkref_export_stl(void* handle, const double* translations, const double* quaternions, std::uint64_t copies,
+                      std::uint8_t* out, std::uint64_t capacity, std::uint64_t* size)
+{
+    const auto mesh = static_cast<Asset*>(handle)->solid->mesh();
+    const std::uint64_t triangles = mesh.triangles.size() * copies;
+    *size = 84 + 50 * triangles;
+    if (capacity < *size) {
+        return 3;
+    }
+    std::memset(out, 0, 80);
+    const auto count32 = static_cast<std::uint32_t>(triangles);
+    std::memcpy(out + 80, &count32, 4);
+    std::uint8_t* at = out + 84;
+    for (std::uint64_t c = 0; c < copies; ++c) {
+        const double* t = translations + 3 * c;
+        const double* q = quaternions + 4 * c;
+        const auto transform = g::RigidTransform::make({ q[0], q[1], q[2], q[3] }, { t[0], t[1], t[2] });
+        if (!transform) {
+            return 1;
+        }
+        for (const auto& face : mesh.triangles) {
+            std::array<std::array<float, 3>, 3> points {};
+            for (std::size_t vertex = 0; vertex != 3; ++vertex) {
+                const auto point = transform->apply(mesh.vertices[face[vertex]]);
+                for (std::size_t axis = 0; axis != 3; ++axis) {
+                    if (!std::isfinite(point[axis]) || point[axis] > std::numeric_limits<float>::max() ||
+                        point[axis] < -std::numeric_limits<float>::max()) {
+                        return 2;
+                    }
+                    points[vertex][axis] = static_cast<float>(point[axis]);
+                }
+            }
+            const std::array<double, 3> ea { static_cast<double>(points[1][0]) - points[0][0],
+                                             static_cast<double>(points[1][1]) - points[0][1],
+                                             static_cast<double>(points[1][2]) - points[0][2] };
+            const std::array<double, 3> eb { static_cast<double>(points[2][0]) - points[0][0],
+                                             static_cast<double>(points[2][1]) - points[0][1],
+                                             static_cast<double>(points[2][2]) - points[0][2] };
+            std::array<double, 3> n { ea[1] * eb[2] - ea[2] * eb[1], ea[2] * eb[0] - ea[0] * eb[2],
+                                      ea[0] * eb[1] - ea[1] * eb[0] };
+            const auto length = std::hypot(std::hypot(n[0], n[1]), n[2]);
+            if (length != 0.0 && std::isfinite(length)) {
+                for (auto& v : n) {
+                    v /= length;
+                }
+            }
+            else {
+                n = {};
+            }
+            const std::array<float, 3> normal { static_cast<float>(n[0]), static_cast<float>(n[1]),
+                                                static_cast<float>(n[2]) };
+            std::memcpy(at, normal.data(), 12);
+            std::memcpy(at + 12, points.data(), 36);
+            at[48] = at[49] = 0;
+            at += 50;
+        }
+    }
+    return 0;
 }
 
 // mode: 0 fixed, 1 cube, 4 catalog (g::OrientationMode values).

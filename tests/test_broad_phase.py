@@ -121,12 +121,13 @@ def test_device_broad_phase_capacity(gpu_ctx, oracle_c):
 
 @pytest.mark.gpu
 def test_device_broad_phase_on_posed_layout(gpu_ctx, oracle_c, oracle_ref):
-    # Posed bounds of a packed layout: the GPU session's own placements.
+    # Posed bounds of a packed layout: the GPU session's own placements of
+    # blobs, whose bounds overlap where the copies nest.
     assets, geometry, session_mod, workloads = (package("assets"), package("geometry"), package("session"),
                                                 package("workloads"))
-    wl = workloads.box64_cuboid_cube24()
+    wl = workloads.rounded256_blob_hopf512(orientations=16)
     s = session_mod.Session(wl.obj, wl.container, wl.origin, wl.pitch, wl.catalog, context=gpu_ctx)
-    placed = s.greedy(40)
+    placed = s.greedy(24)
     s.close()
     t = np.array([[wl.origin[a] + wl.pitch * p.translation[a] for a in range(3)] for p in placed])
     q = np.array([wl.catalog[p.orientation_index] for p in placed])
