@@ -38,8 +38,9 @@ UNIT = "placements/s"
 PASSES = [
     ("pass_a256_batch_kernel", "spectral z: environment spectrum read once per batch of orientations, kernel z "
                                "finish, conjugate product, inverse z"),
-    ("pass_b1_256_kernel", "inverse y over the legal z planes"),
-    ("pass_b2_256_kernel", "inverse x with the fused threshold / score / top-k epilogue"),
+    ("pass_b1_256_batch_kernel", "inverse y over the legal z planes, a batch of orientations per launch"),
+    ("pass_b2_256_batch_kernel", "inverse x with the fused threshold / score / top-k epilogue, a batch of "
+                                 "orientations per launch"),
     ("merge_kernel + exact_kernel", "key merge and exact recount"),
 ]
 # DRAM read + write bytes per launch of each kernel on the 256^3 workload,
@@ -352,6 +353,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.workload, O)
     broad = broad_phase_line(ctx, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+    stl = stl_export_line(ctx, with_cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
     if rank == 0:
         config = reference_config(args.workload, world)
@@ -387,6 +389,7 @@ def run_ours(args, rank, world, local_rank):
             "e2e": e2e,
             "clocks": clocks.summary(),
             "validator_broad_phase": broad,
+            "stl_export": stl,
         }
         if learned:
             line["proposal"] = {"k": k, "weights": os.path.relpath(weights, os.path.dirname(os.path.abspath(__file__))),
@@ -424,6 +427,41 @@ def broad_phase_line(ctx, with_cpu: bool, copies: int = 3580):
         line["cpu_baseline"] = {"value": round(pairs / cpu_s, 1), "unit": "pairs/s", "cores": 1, "kind": "port",
                                 "sample": f"all {pairs} pairs of the same layout (oracle_broad_phase)",
                                 "same_pairs": bool(np.array_equal(got, want))}
+    return line
+
+
+def stl_export_line(ctx, with_cpu: bool, copies: int = 512, cpu_copies: int = 16):
+    """STL export of a placement sequence (spk_export_stl): triangles per
+    second through the C ABI with host buffers (poses in, the file's bytes
+    out), for `copies` posed copies of the bench item; as its CPU baseline,
+    the reference build's own record loop (RigidTransform, libm hypot) on one
+    host core over the first `cpu_copies` poses, whose bytes must match."""
+    bp, geometry = pkg("broad_phase_bench"), pkg("geometry")
+    obj, stl_bytes, t, q = bp.poses(copies)
+    triangles = copies * len(obj.triangles)
+    geometry.export_stl(obj, t[:2], q[:2], context=ctx)  # buffers and first-call costs
+    repeats = 3
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        data = geometry.export_stl(obj, t, q, context=ctx)
+    seconds = (time.perf_counter() - t0) / repeats
+    line = {"metric": "STL triangles exported per second", "copies": copies, "triangles": triangles,
+            "bytes": len(data), "value": round(triangles / seconds, 1), "ms_per_call": round(seconds * 1e3, 3),
+            "path": "spk_export_stl with host buffers"}
+    if with_cpu:
+        from oracle.bindings import Ref
+
+        asset = Ref().asset(stl_bytes)
+        t1 = time.perf_counter()
+        want = asset.export_stl(t[:cpu_copies], q[:cpu_copies])
+        cpu_s = time.perf_counter() - t1
+        sample = cpu_copies * len(obj.triangles)
+        head = geometry.export_stl(obj, t[:cpu_copies], q[:cpu_copies], context=ctx)
+        line["cpu_baseline"] = {"value": round(sample / cpu_s, 1), "unit": "triangles/s", "cores": 1,
+                                "kind": "reference",
+                                "sample": f"the first {cpu_copies} copies ({sample} triangles), record loop of "
+                                          "result_export.cpp:1034-1123 in the reference build",
+                                "same_bytes": head == want}
     return line
 
 

@@ -33,9 +33,10 @@ def pkg(name):
     return importlib.import_module("cpp-max-packer_b200." + name)
 
 
-def layout(copies: int, seed: int = 3):
-    """(posed bounds min, max, finite) of `copies` seeded poses of the bench item."""
-    geometry, workloads = pkg("geometry"), pkg("workloads")
+def poses(copies: int, seed: int = 3):
+    """(item mesh, its STL bytes, translations (copies, 3), quaternions
+    (copies, 4)): seeded poses of the bench item over a 256 mm cube."""
+    workloads = pkg("workloads")
     spec = workloads.SPECS["rounded256_blob_hopf512"]()
     obj = pkg("assets").accept_stl(spec.object_stl)
     rng = np.random.default_rng(seed)
@@ -43,7 +44,13 @@ def layout(copies: int, seed: int = 3):
     q /= np.linalg.norm(q, axis=1)[:, None]
     q[q[:, 3] < 0] *= -1
     t = rng.uniform(0.0, 256.0, size=(copies, 3))
-    return geometry.posed_bounds(obj, t, q)
+    return obj, spec.object_stl, t, q
+
+
+def layout(copies: int, seed: int = 3):
+    """(posed bounds min, max, finite) of `copies` seeded poses of the bench item."""
+    obj, _, t, q = poses(copies, seed)
+    return pkg("geometry").posed_bounds(obj, t, q)
 
 
 def time_device(lo, hi, fin, clearance: float, repeats: int, context):

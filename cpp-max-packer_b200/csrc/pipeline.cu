@@ -556,17 +556,15 @@ __global__ void __launch_bounds__(256) env_column256_kernel(float2* __restrict__
     }
 }
 
-__global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ inter, int legal_y,
-                                                         const float2* __restrict__ twiddles)
+// Inverse y of 16 columns kx of one legal z plane: block b of an
+// orientation covers plane b / 16, columns 16 (b % 16) ...
+__device__ __forceinline__ void b1_block256(float2* __restrict__ inter, int legal_y, const RegTwiddles& tw,
+                                            float2* lines, unsigned int block)
 {
-    __shared__ RegTwiddles tw;
-    __shared__ float2 lines[16 * kRegLine];
-    load_twiddles(tw, twiddles);
-    __syncthreads();
     const int j = threadIdx.x & 15;
     const int t = threadIdx.x >> 4;
-    const long long zz = blockIdx.x >> 4;
-    const long long col = ((blockIdx.x & 15) << 4) + j + 65536LL * zz;
+    const long long zz = block >> 4;
+    const long long col = ((block & 15) << 4) + j + 65536LL * zz;
     float2 v[16];
 #pragma unroll
     for (int n1 = 0; n1 < 16; ++n1) {
@@ -580,6 +578,37 @@ __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ i
             inter[col + 256LL * y] = v[m2];
         }
     }
+}
+
+__global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ inter, int legal_y,
+                                                         const float2* __restrict__ twiddles)
+{
+    __shared__ RegTwiddles tw;
+    __shared__ float2 lines[16 * kRegLine];
+    load_twiddles(tw, twiddles);
+    __syncthreads();
+    b1_block256(inter, legal_y, tw, lines, blockIdx.x);
+}
+
+// Slot of a batched launch that owns this block.
+__device__ __forceinline__ int batch_slot(const PassBBatch& b)
+{
+    int g = 0;
+    while (g + 1 < b.count && b.slot[g + 1].first_block <= static_cast<int>(blockIdx.x)) {
+        ++g;
+    }
+    return g;
+}
+
+__global__ void __launch_bounds__(256) pass_b1_256_batch_kernel(const __grid_constant__ PassBBatch b,
+                                                               const float2* __restrict__ twiddles)
+{
+    __shared__ RegTwiddles tw;
+    __shared__ float2 lines[16 * kRegLine];
+    load_twiddles(tw, twiddles);
+    __syncthreads();
+    const int g = batch_slot(b);
+    b1_block256(b.slot[g].inter, b.slot[g].legal_y, tw, lines, blockIdx.x - b.slot[g].first_block);
 }
 
 // Pass B2 on 256^3 grids: 16 rows per block, 16 threads per row.
@@ -1049,6 +1078,33 @@ __device__ __forceinline__ void b2_rows256(float2 (&v)[16], float2* lines, const
     }
 }
 
+// Inverse x of 16 legal rows of one orientation and the epilogue: block b
+// covers rows 16 b ... (row = y + legal_y zz).
+__device__ __forceinline__ void b2_block256(const float2* __restrict__ inter, int legal_x, int legal_y, int legal_z,
+                                            const RegTwiddles& tw, float2* lines, B2Shared& sh,
+                                            const double* __restrict__ t65, double inv_occ, int mode, float target,
+                                            double threshold, double cursor_floor,
+                                            unsigned long long* __restrict__ keys, unsigned int* __restrict__ count,
+                                            unsigned int cap, unsigned long long* __restrict__ tau,
+                                            unsigned long long* __restrict__ resid, unsigned int block)
+{
+    const int t = threadIdx.x & 15;
+    const int j = threadIdx.x >> 4;
+    const long long rows = static_cast<long long>(legal_y) * legal_z;
+    const long long row = static_cast<long long>(block) * 16 + j;
+    const bool valid = row < rows;
+    const int y = valid ? static_cast<int>(row % legal_y) : 0;
+    const int zz = valid ? static_cast<int>(row / legal_y) : 0;
+    const long long base = 256LL * (y + 256LL * zz);
+    float2 v[16];
+#pragma unroll
+    for (int n1 = 0; n1 < 16; ++n1) {
+        v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
+    }
+    b2_rows256(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, target, threshold, cursor_floor,
+               keys, count, cap, tau, resid);
+}
+
 __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restrict__ inter, int legal_x,
                                                          int legal_y, int legal_z,
                                                          const float2* __restrict__ twiddles,
@@ -1064,21 +1120,22 @@ __global__ void __launch_bounds__(256) pass_b2_256_kernel(const float2* __restri
     __shared__ B2Shared sh;
     load_twiddles(tw, twiddles);
     __syncthreads();
-    const int t = threadIdx.x & 15;
-    const int j = threadIdx.x >> 4;
-    const long long rows = static_cast<long long>(legal_y) * legal_z;
-    const long long row = static_cast<long long>(blockIdx.x) * 16 + j;
-    const bool valid = row < rows;
-    const int y = valid ? static_cast<int>(row % legal_y) : 0;
-    const int zz = valid ? static_cast<int>(row / legal_y) : 0;
-    const long long base = 256LL * (y + 256LL * zz);
-    float2 v[16];
-#pragma unroll
-    for (int n1 = 0; n1 < 16; ++n1) {
-        v[n1] = valid ? inter[base + 16 * n1 + t] : make_float2(0.f, 0.f);
-    }
-    b2_rows256(v, lines, tw, sh, valid, y, zz, legal_x, legal_y, t65, inv_occ, mode, target, threshold, cursor_floor,
-               keys, count, cap, tau, resid);
+    b2_block256(inter, legal_x, legal_y, legal_z, tw, lines, sh, t65, inv_occ, mode, target, threshold, cursor_floor,
+                keys, count, cap, tau, resid, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) pass_b2_256_batch_kernel(const __grid_constant__ PassBBatch b,
+                                                               const float2* __restrict__ twiddles)
+{
+    __shared__ RegTwiddles tw;
+    __shared__ float2 lines[16 * kRegLine];
+    __shared__ B2Shared sh;
+    load_twiddles(tw, twiddles);
+    __syncthreads();
+    const PassBSlot& s = b.slot[batch_slot(b)];
+    b2_block256(s.inter, s.legal_x, s.legal_y, s.legal_z, tw, lines, sh, s.t65, s.inv_occ, 0, s.target, 0.0,
+                s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid,
+                blockIdx.x - static_cast<unsigned int>(s.first_block));
 }
 
 // Passes B1 and B2 fused on 256^3 grids: one cluster of 8 CTAs per legal z
@@ -1811,6 +1868,50 @@ int Pipeline::run_a256_batch(const KernelSlot* const* slots, int count, float2* 
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
+int Pipeline::run_b256_batch(const KernelSlot* const* slots, int count, float2* const* inter,
+                             const PassBSlot* outputs)
+{
+    cudaStream_t st = ctx_->stream;
+    int status = kOk;
+    const auto* tw0 = twiddle_table<float>(ctx_, L_[0], status);
+    const auto* tw1 = twiddle_table<float>(ctx_, L_[1], status);
+    if (!tw0 || !tw1) {
+        return status;
+    }
+    PassBBatch b1 {}, b2 {};
+    b1.count = b2.count = count;
+    int blocks1 = 0, blocks2 = 0;
+    double bytes1 = 0.0, bytes2 = 0.0;
+    for (int g = 0; g < count; ++g) {
+        const KernelSlot& s = *slots[g];
+        PassBSlot slot = outputs[g];
+        slot.inter = inter[g];
+        slot.t65 = s.t65;
+        slot.inv_occ = 1.0 / static_cast<double>(s.occupied);
+        slot.legal_x = s.legal[0];
+        slot.legal_y = s.legal[1];
+        slot.legal_z = s.legal[2];
+        slot.first_block = blocks1;
+        b1.slot[g] = slot;
+        blocks1 += 16 * s.legal[2];
+        slot.first_block = blocks2;
+        b2.slot[g] = slot;
+        const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
+        blocks2 += static_cast<int>((rows + 15) / 16);
+        const double legal_rows = static_cast<double>(rows);
+        bytes1 += 8.0 * L_[0] * L_[1] * s.legal[2] + 8.0 * L_[0] * legal_rows;
+        bytes2 += 8.0 * L_[0] * legal_rows;
+    }
+    auto ev = pass_begin(ctx_);
+    pass_b1_256_batch_kernel<<<blocks1, 256, 0, st>>>(b1, tw1);
+    pass_end(ctx_, 1, ev, bytes1);
+    ev = pass_begin(ctx_);
+    pass_b2_256_batch_kernel<<<blocks2, 256, 0, st>>>(b2, tw0);
+    pass_end(ctx_, 2, ev, bytes2);
+    ctx_->launches += 2;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
 int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, float target, double threshold, double cursor_floor,
                        unsigned long long* keys, unsigned int* count, unsigned int cap, unsigned long long* tau,
                        unsigned long long* resid)
@@ -2054,6 +2155,23 @@ int Pipeline::ordinary_pages(const std::vector<PageRequest>& requests, std::vect
             }
             if ((status = run_a256_batch(group, n, outs))) {
                 return status;
+            }
+            if (!fused_b_) {
+                PassBSlot targets[kPassABatch] {};
+                for (int g = 0; g < n; ++g) {
+                    const int r = runnable[i0 + g];
+                    targets[g].keys = keys + static_cast<long long>(r) * cap;
+                    targets[g].count = count + r;
+                    targets[g].cap = cap;
+                    targets[g].tau = tau + r;
+                    targets[g].resid = resid + r;
+                    targets[g].target = static_cast<float>(requests[r].overlap);
+                    targets[g].cursor_floor = floor[r];
+                }
+                if ((status = run_b256_batch(group, n, outs, targets))) {
+                    return status;
+                }
+                continue;
             }
             for (int g = 0; g < n; ++g) {
                 const int r = runnable[i0 + g];

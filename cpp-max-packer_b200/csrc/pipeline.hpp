@@ -65,6 +65,26 @@ struct PassABatch {
     PassASlot slot[kPassABatch];
     int count;
 };
+// Passes B1 and B2 of a batch of orientations in one launch each: slot g
+// owns the blocks from first_block on.
+struct PassBSlot {
+    float2* inter;
+    const double* t65;
+    unsigned long long* keys;
+    unsigned int* count;
+    unsigned long long* tau;
+    unsigned long long* resid;
+    double inv_occ;
+    double cursor_floor;
+    float target;
+    unsigned int cap;
+    int legal_x, legal_y, legal_z;
+    int first_block;
+};
+struct PassBBatch {
+    PassBSlot slot[kPassABatch];
+    int count;
+};
 
 struct PageRequest {
     std::uint64_t slot {};
@@ -136,6 +156,8 @@ private:
     // Pass A for up to kPassABatch orientations in one launch (256^3 grids);
     // orientation i's legal-z intermediate goes to inter[i].
     int run_a256_batch(const KernelSlot* const* slots, int count, float2* const* inter);
+    // Passes B1 and B2 (mode 0) of the same batch, one launch each.
+    int run_b256_batch(const KernelSlot* const* slots, int count, float2* const* inter, const PassBSlot* outputs);
     double score(const KernelSlot& s, const std::int64_t* t, double p) const;
     double approx_epsilon(const KernelSlot& s) const;
 
