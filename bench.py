@@ -48,9 +48,9 @@ PASSES = [
 # (dram__bytes.sum.per_second x duration; each launch there does the same
 # work as in the 512-orientation workload).
 NCU_DRAM_BYTES = {
-    "pass_a256_batch_kernel": 2231196881,
-    "pass_b1_256_kernel": 182485494,
-    "pass_b2_256_kernel": 119751955,
+    "pass_a256_batch_kernel": 2231803888,
+    "pass_b1_256_batch_kernel": 3796430981,
+    "pass_b2_256_batch_kernel": 1862089123,
 }
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp-max-packer_b200", "weights",
                                "proposal_rounded256.npz")

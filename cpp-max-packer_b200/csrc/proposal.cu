@@ -62,31 +62,36 @@ struct ConvArgs {
     // log2 of the power-of-two extents and channel counts (every layer of the
     // network has them), so the gathers index with shifts and masks.
     int lg_s_in, lg_s_out, lg_cin, lg_cinp, lg_cout;
-    // Corner-box forward (kFwdBox): the GEMM rows are the voxels of the box
-    // [0, box_out) of every sample, row m = n * box_out_vol + (z * box_out[1]
-    // + y) * box_out[0] + x, and `out` / `out_f32` are laid out by row as
-    // always.  An input voxel inside [0, box_in) is read from x, laid out
-    // [n][box_in voxels][cin] the same way; any other input voxel is read
-    // from x_shared ([s_in^3][cin], one sample shared by all), or is zero
-    // when x_shared is null.
+    // Corner-box forward (kFwdBox): `out` / `out_f32` hold the box
+    // [0, box_out) of every sample, voxel (x, y, z) of sample n at row
+    // n * box_out_vol + (z * box_out[1] + y) * box_out[0] + x.  The GEMM rows
+    // are the voxels of the sub-box [region_first, region_first + region) of
+    // every sample (row m = n * region_vol + its place in the sub-box, x
+    // fastest), each written to its place in the box.  An input voxel inside
+    // [0, box_in) is read from x, laid out [n][box_in voxels][cin] the same
+    // way; any other input voxel is read from x_shared ([s_in^3][cin], one
+    // sample shared by all), or is zero when x_shared is null.
     const bf16* x_shared;
     int box_in[3], box_out[3];
     int box_in_vol, box_out_vol;
+    int region_first[3], region[3];
+    int region_vol;
 };
 
 struct Vox {
     int n, z, y, x;
 };
 
-// Voxel of row m of a corner-box GEMM (rows < 2^32).
-__device__ __forceinline__ Vox decode_box(unsigned m, const int (&box)[3], int vol)
+// Voxel of row m of a corner-box GEMM over the sub-box [first, first +
+// region) (rows < 2^32).
+__device__ __forceinline__ Vox decode_box(unsigned m, const int (&first)[3], const int (&region)[3], int vol)
 {
     Vox v;
     v.n = static_cast<int>(m / static_cast<unsigned>(vol));
     const int r = static_cast<int>(m % static_cast<unsigned>(vol));
-    v.x = r % box[0];
-    v.y = (r / box[0]) % box[1];
-    v.z = r / (box[0] * box[1]);
+    v.x = first[0] + r % region[0];
+    v.y = first[1] + (r / region[0]) % region[1];
+    v.z = first[2] + r / (region[0] * region[1]);
     return v;
 }
 
@@ -341,7 +346,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
         const long long m = m0 + tid;
         row_ok = m < a.m_total;
         if (MODE == kFwdBox) {
-            row_vox = decode_box(static_cast<unsigned>(row_ok ? m : 0), a.box_out, a.box_out_vol);
+            row_vox = decode_box(static_cast<unsigned>(row_ok ? m : 0), a.region_first, a.region, a.region_vol);
         }
         else {
             row_vox = decode_pow2(static_cast<unsigned>(row_ok ? m : 0), MODE == kFwd ? a.lg_s_out : a.lg_s_in);
@@ -408,9 +413,14 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
         atomicOr(a.error, 1u);
     }
 
-    // Epilogue: thread tid holds TMEM lane tid = tile row tid.
+    // Epilogue: thread tid holds TMEM lane tid = tile row tid, written to
+    // its output row (for kFwdBox, the voxel's place in the box).
     const std::uint32_t lane_addr = tmem + (static_cast<std::uint32_t>(warp * 32) << 16);
     const long long row = m0 + tid;
+    const long long out_row =
+        MODE == kFwdBox ? static_cast<long long>(row_vox.n) * a.box_out_vol +
+                              (row_vox.z * a.box_out[1] + row_vox.y) * a.box_out[0] + row_vox.x
+                        : row;
     for (int c0 = 0; c0 < N; c0 += 16) {
         float v[16];
         umma::tmem_load16(lane_addr + static_cast<std::uint32_t>(c0), v);
@@ -422,7 +432,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
         }
         if (fwd && a.out_f32) {
             if (row < a.m_total) {
-                float4* dst = reinterpret_cast<float4*>(a.out_f32 + row * a.cout + c0);
+                float4* dst = reinterpret_cast<float4*>(a.out_f32 + out_row * a.cout + c0);
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
                     dst[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
@@ -436,7 +446,7 @@ __global__ void __launch_bounds__(kThreads) conv_kernel(const ConvArgs a)
                 for (int i = 0; i < 16; ++i) {
                     h[i] = __float2bfloat16_rn(fmaxf(v[i] + a.bias[c0 + i], 0.f));
                 }
-                uint4* dst = reinterpret_cast<uint4*>(a.out + row * a.cout + c0);
+                uint4* dst = reinterpret_cast<uint4*>(a.out + out_row * a.cout + c0);
                 dst[0] = reinterpret_cast<const uint4*>(h)[0];
                 dst[1] = reinterpret_cast<const uint4*>(h)[1];
             }
@@ -695,19 +705,23 @@ __global__ void assemble_box_kernel(const bf16* __restrict__ items, int batch, i
 // ([32^3][cout]), with the expression of combine_first_kernel.
 __global__ void combine_box_kernel(const float* __restrict__ item_box, const float* __restrict__ crop_half,
                                    const float* __restrict__ bias, int batch, int cout, int b0, int b1, int b2,
-                                   bf16* __restrict__ act)
+                                   int f0, int f1, int f2, int r0, int r1, int r2, bf16* __restrict__ act)
 {
+    // Voxels of the sub-box [f, f + r) of the box [0, b) of every sample.
     const int groups = cout / 8;
     const int vol = b0 * b1 * b2;
-    const long long total = static_cast<long long>(batch) * vol * groups;
+    const int rvol = r0 * r1 * r2;
+    const long long total = static_cast<long long>(batch) * rvol * groups;
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
         const int g = static_cast<int>(i % groups);
-        const int r = static_cast<int>((i / groups) % vol);
-        const int vx = r % b0, vy = (r / b0) % b1, vz = r / (b0 * b1);
+        const int r = static_cast<int>((i / groups) % rvol);
+        const long long n = i / (static_cast<long long>(groups) * rvol);
+        const int vx = f0 + r % r0, vy = f1 + (r / r0) % r1, vz = f2 + r / (r0 * r1);
         const long long voxel = (vz * kProposalGrid + vy) * kProposalGrid + vx;
+        const long long at = (n * vol + (vz * b1 + vy) * b0 + vx) * groups + g;  // 8-channel group in the box
         const int c0 = g * 8;
-        const float4* a = reinterpret_cast<const float4*>(item_box + i * 8);
+        const float4* a = reinterpret_cast<const float4*>(item_box + at * 8);
         const float4* c = reinterpret_cast<const float4*>(crop_half + voxel * cout + c0);
         const float4 a0 = a[0], a1 = a[1], q0 = c[0], q1 = c[1];
         const float v[8] = { a0.x + q0.x, a0.y + q0.y, a0.z + q0.z, a0.w + q0.w,
@@ -717,7 +731,26 @@ __global__ void combine_box_kernel(const float* __restrict__ item_box, const flo
         for (int k = 0; k < 8; ++k) {
             h[k] = __float2bfloat16_rn(fmaxf(v[k] + bias[c0 + k], 0.f));
         }
-        reinterpret_cast<uint4*>(act)[i] = *reinterpret_cast<const uint4*>(h);
+        reinterpret_cast<uint4*>(act)[at] = *reinterpret_cast<const uint4*>(h);
+    }
+}
+
+// Bounding range of the voxels where two pooled layouts differ (bitwise):
+// box[0..2] = lowest x, y, z and box[3..5] = highest, updated atomically.
+__global__ void crop_dirty_kernel(const bf16* __restrict__ a, const bf16* __restrict__ b, int* __restrict__ box)
+{
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= kProposalVoxels) {
+        return;
+    }
+    if (__bfloat16_as_ushort(a[v]) != __bfloat16_as_ushort(b[v])) {
+        const int x = v % kProposalGrid, y = (v / kProposalGrid) % kProposalGrid, z = v / (kProposalGrid * kProposalGrid);
+        atomicMin(box, x);
+        atomicMin(box + 1, y);
+        atomicMin(box + 2, z);
+        atomicMax(box + 3, x);
+        atomicMax(box + 4, y);
+        atomicMax(box + 5, z);
     }
 }
 
@@ -854,6 +887,11 @@ struct ProposalNet {
     bf16* act_shared[kProposalLayers] {};
     bf16* box_last {};
     std::size_t box_last_capacity {};
+    // The layout channel the kept activations were computed from, and the
+    // changed-voxel range found against it.
+    bf16* prev_crop {};
+    int* dirty {};
+    bool trunk_valid {};
     // The layout-only layers run on a stream of their own, ahead of the
     // per-sample boxes that read them (one event per layer).
     cudaStream_t side {};
@@ -1003,7 +1041,8 @@ void launch_conv_forward(spk_context* ctx, ProposalNet* net, int l, std::uint32_
 // Forward layer l over the corner box `box_out` of every sample (kFwdBox).
 void launch_conv_box(spk_context* ctx, ProposalNet* net, int l, std::uint32_t batch, const bf16* x,
                      const int (&box_in)[3], const bf16* x_shared, const int (&box_out)[3], bf16* out,
-                     float* out_f32)
+                     float* out_f32, const int (&region_first)[3], const int (&region)[3],
+                     cudaStream_t stream = nullptr)
 {
     ConvArgs a = layer_args(net, l, batch);
     a.x = x;
@@ -1012,17 +1051,24 @@ void launch_conv_box(spk_context* ctx, ProposalNet* net, int l, std::uint32_t ba
     a.out_f32 = out_f32;
     a.box_in_vol = 1;
     a.box_out_vol = 1;
+    a.region_vol = 1;
     for (int i = 0; i < 3; ++i) {
         a.box_in[i] = box_in[i];
         a.box_out[i] = box_out[i];
         a.box_in_vol *= box_in[i];
         a.box_out_vol *= box_out[i];
+        a.region_first[i] = region_first[i];
+        a.region[i] = region[i];
+        a.region_vol *= region[i];
     }
-    a.m_total = static_cast<long long>(batch) * a.box_out_vol;
+    a.m_total = static_cast<long long>(batch) * a.region_vol;
     a.k_total = a.kw;
+    if (a.m_total == 0) {
+        return;
+    }
     const int blocks = static_cast<int>((a.m_total + kRows - 1) / kRows);
     const int smem = kStages * (kRows * kKC * 2 + a.cout * kKC * 2);
-    conv_kernel<kFwdBox><<<blocks, kThreads, smem, ctx->stream>>>(a);
+    conv_kernel<kFwdBox><<<blocks, kThreads, smem, stream ? stream : ctx->stream>>>(a);
     ctx->launches++;
 }
 
@@ -1159,6 +1205,14 @@ namespace {
 // box of layer l - 1.  The layers therefore run once on the layout alone
 // (one sample, item sums zero) and, per sample, only over their boxes,
 // reading the layout-only activations wherever a window leaves the box.
+//
+// Between calls only the layout channel changes (a session places a copy),
+// and the activations of both kinds are kept: a call compares the layout
+// with the previous one, and each layer recomputes only the voxels whose
+// window reaches the previous layer's changed voxels (a box per layer,
+// grown by the window and shrunk by the stride).  An unchanged layout
+// recomputes nothing before the head.
+//
 // Every output row is the same dot product in the same K order as in the
 // full forward, so the predictions equal the full split forward's.
 int predict_box(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const bf16* crops, const bf16* items,
@@ -1204,15 +1258,19 @@ int predict_box(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const b
                 items, static_cast<int>(batch), net->item_box[0], net->item_box[1], net->item_box[2], net->x_item);
             ctx->launches++;
         }
-        launch_conv_box(ctx, net, 0, batch, net->x_item, net->item_box, nullptr, net->box[0], nullptr,
-                        net->item_half);
+        const int origin[3] = { 0, 0, 0 };
+        launch_conv_box(ctx, net, 0, batch, net->x_item, net->item_box, nullptr, net->box[0], nullptr, net->item_half,
+                        origin, net->box[0]);
         net->item_half_tag = items_tag;
         net->item_half_batch = batch;
         net->item_half_version = net->version;
         net->item_half_box = true;
+        net->trunk_valid = false;
     }
     if ((!net->x_crop && (status = alloc(net, net->x_crop, static_cast<std::size_t>(kProposalVoxels) * 2))) ||
-        (!net->crop_half && (status = alloc(net, net->crop_half, static_cast<std::size_t>(kProposalVoxels) * c1)))) {
+        (!net->crop_half && (status = alloc(net, net->crop_half, static_cast<std::size_t>(kProposalVoxels) * c1))) ||
+        (!net->prev_crop && (status = alloc(net, net->prev_crop, static_cast<std::size_t>(kProposalVoxels)))) ||
+        (!net->dirty && (status = alloc(net, net->dirty, 6)))) {
         return status;
     }
     for (int l = 0; l < kProposalLayers; ++l) {
@@ -1230,21 +1288,6 @@ int predict_box(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const b
                           static_cast<std::size_t>(batch) * s3 * s3 * s3 * c3))) {
         return status;
     }
-    // The layout's first-layer sums (one sample, item channel zero).
-    assemble_kernel<<<grid_for(kProposalVoxels), 256, 0, ctx->stream>>>(crops, nullptr, nullptr, nullptr, 1,
-                                                                        net->x_crop);
-    launch_conv_forward(ctx, net, 0, 1, net->x_crop, nullptr, net->crop_half);
-    const float* bias0 = net->params + net->b_off[0];
-    combine_first_kernel<<<grid_for(static_cast<long long>(kProposalVoxels) * c1 / 8), 256, 0, ctx->stream>>>(
-        nullptr, net->crop_half, bias0, 1, c1, net->act_shared[0]);
-    ctx->launches += 2;
-    // A layer's layout-only activations are read only where its box does not
-    // cover it (boxes never shrink back once they cover their layer).
-    bool shared_needed[kProposalLayers];
-    for (int l = 0; l < kProposalLayers; ++l) {
-        const int so = out_side(kProposalSpec[l]);
-        shared_needed[l] = net->box[l][0] < so || net->box[l][1] < so || net->box[l][2] < so;
-    }
     if (!net->side) {
         if (cudaStreamCreateWithFlags(&net->side, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
@@ -1258,37 +1301,106 @@ int predict_box(spk_context* ctx, ProposalNet* net, std::uint32_t batch, const b
             }
         }
     }
-    cudaEventRecord(net->layer_done[0], ctx->stream);
-    cudaStreamWaitEvent(net->side, net->layer_done[0], 0);
-    for (int l = 1; l < kProposalLayers; ++l) {
-        if (shared_needed[l]) {
-            launch_conv_forward(ctx, net, l, 1, net->act_shared[l - 1], net->act_shared[l], nullptr, net->side);
+    // The layout voxels that changed since the activations were computed:
+    // lo / hi per axis, inclusive (hi < lo: none).
+    int lo[3] = { 0, 0, 0 }, hi[3] = { kProposalGrid - 1, kProposalGrid - 1, kProposalGrid - 1 };
+    if (net->trunk_valid) {
+        const int init[6] = { kProposalGrid, kProposalGrid, kProposalGrid, -1, -1, -1 };
+        int found[6] {};
+        cudaMemcpyAsync(net->dirty, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream);
+        crop_dirty_kernel<<<kProposalVoxels / 256, 256, 0, ctx->stream>>>(crops, net->prev_crop, net->dirty);
+        ctx->launches++;
+        if (cudaMemcpyAsync(found, net->dirty, sizeof(found), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+            cudaGetLastError();
+            return kCuda;
         }
-        cudaEventRecord(net->layer_done[l], net->side);
-    }
-    const long long box0 = static_cast<long long>(batch) * net->box[0][0] * net->box[0][1] * net->box[0][2];
-    combine_box_kernel<<<grid_for(box0 * c1 / 8), 256, 0, ctx->stream>>>(
-        net->item_half, net->crop_half, bias0, static_cast<int>(batch), c1, net->box[0][0], net->box[0][1],
-        net->box[0][2], net->act_box[0]);
-    ctx->launches++;
-    for (int l = 1; l < kProposalLayers; ++l) {
-        if (l >= 2) {
-            cudaStreamWaitEvent(ctx->stream, net->layer_done[l - 1], 0);
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = found[a];
+            hi[a] = found[3 + a];
         }
-        launch_conv_box(ctx, net, l, batch, net->act_box[l - 1], net->box[l - 1],
-                        shared_needed[l - 1] ? net->act_shared[l - 1] : nullptr, net->box[l], net->act_box[l],
-                        nullptr);
     }
-    // Joins the side stream (the next call rewrites what it read).
-    cudaStreamWaitEvent(ctx->stream, net->layer_done[kProposalLayers - 1], 0);
-    const int* b3 = net->box[kProposalLayers - 1];
-    expand_box_kernel<<<grid_for(static_cast<long long>(batch) * s3 * s3 * s3 * c3 / 8), 256, 0, ctx->stream>>>(
-        net->act_shared[kProposalLayers - 1], net->act_box[kProposalLayers - 1], static_cast<int>(batch), s3, c3,
-        b3[0], b3[1], b3[2], net->box_last);
+    const bool changed = hi[0] >= lo[0] && hi[1] >= lo[1] && hi[2] >= lo[2];
+    if (changed) {
+        cudaMemcpyAsync(net->prev_crop, crops, sizeof(bf16) * kProposalVoxels, cudaMemcpyDeviceToDevice,
+                        ctx->stream);
+        // A layer's layout-only activations are read only where its box does
+        // not cover it (boxes never shrink back once they cover their layer).
+        bool shared_needed[kProposalLayers];
+        for (int l = 0; l < kProposalLayers; ++l) {
+            const int so = out_side(kProposalSpec[l]);
+            shared_needed[l] = net->box[l][0] < so || net->box[l][1] < so || net->box[l][2] < so;
+        }
+        // Changed output voxels per layer: window o * stride - 1 .. o * stride
+        // + 1 meets the previous layer's changed range.
+        int first[kProposalLayers][3], region[kProposalLayers][3], box_first[kProposalLayers][3],
+            box_region[kProposalLayers][3];
+        for (int l = 0; l < kProposalLayers; ++l) {
+            const ProposalLayer& L = kProposalSpec[l];
+            const int so = out_side(L);
+            for (int a = 0; a < 3; ++a) {
+                const int pl = l == 0 ? lo[a] : first[l - 1][a];
+                const int ph = l == 0 ? hi[a] : first[l - 1][a] + region[l - 1][a] - 1;
+                int ol = (pl - 1 + L.stride - 1) / L.stride;  // ceil((pl - 1) / stride), pl >= 0
+                if (pl - 1 < 0) {
+                    ol = 0;
+                }
+                const int oh = std::min((ph + 1) / L.stride, so - 1);
+                first[l][a] = ol;
+                region[l][a] = std::max(0, oh - ol + 1);
+                box_first[l][a] = ol;
+                box_region[l][a] = std::max(0, std::min(oh, net->box[l][a] - 1) - ol + 1);
+            }
+        }
+        // The layout's first-layer sums (one sample, item channel zero).
+        assemble_kernel<<<grid_for(kProposalVoxels), 256, 0, ctx->stream>>>(crops, nullptr, nullptr, nullptr, 1,
+                                                                            net->x_crop);
+        launch_conv_forward(ctx, net, 0, 1, net->x_crop, nullptr, net->crop_half);
+        const float* bias0 = net->params + net->b_off[0];
+        combine_first_kernel<<<grid_for(static_cast<long long>(kProposalVoxels) * c1 / 8), 256, 0, ctx->stream>>>(
+            nullptr, net->crop_half, bias0, 1, c1, net->act_shared[0]);
+        ctx->launches += 2;
+        cudaEventRecord(net->layer_done[0], ctx->stream);
+        cudaStreamWaitEvent(net->side, net->layer_done[0], 0);
+        const int zero[3] = { 0, 0, 0 };
+        for (int l = 1; l < kProposalLayers; ++l) {
+            if (shared_needed[l]) {
+                const int so = out_side(kProposalSpec[l]);
+                const int whole[3] = { so, so, so };
+                launch_conv_box(ctx, net, l, 1, nullptr, zero, net->act_shared[l - 1], whole, net->act_shared[l],
+                                nullptr, first[l], region[l], net->side);
+            }
+            cudaEventRecord(net->layer_done[l], net->side);
+        }
+        const long long box0 = static_cast<long long>(batch) * box_region[0][0] * box_region[0][1] * box_region[0][2];
+        if (box0) {
+            combine_box_kernel<<<grid_for(box0 * c1 / 8), 256, 0, ctx->stream>>>(
+                net->item_half, net->crop_half, bias0, static_cast<int>(batch), c1, net->box[0][0], net->box[0][1],
+                net->box[0][2], box_first[0][0], box_first[0][1], box_first[0][2], box_region[0][0],
+                box_region[0][1], box_region[0][2], net->act_box[0]);
+            ctx->launches++;
+        }
+        for (int l = 1; l < kProposalLayers; ++l) {
+            if (l >= 2) {
+                cudaStreamWaitEvent(ctx->stream, net->layer_done[l - 1], 0);
+            }
+            launch_conv_box(ctx, net, l, batch, net->act_box[l - 1], net->box[l - 1],
+                            shared_needed[l - 1] ? net->act_shared[l - 1] : nullptr, net->box[l], net->act_box[l],
+                            nullptr, box_first[l], box_region[l]);
+        }
+        // Joins the side stream (the next call rewrites what it read).
+        cudaStreamWaitEvent(ctx->stream, net->layer_done[kProposalLayers - 1], 0);
+        const int* b3 = net->box[kProposalLayers - 1];
+        expand_box_kernel<<<grid_for(static_cast<long long>(batch) * s3 * s3 * s3 * c3 / 8), 256, 0, ctx->stream>>>(
+            net->act_shared[kProposalLayers - 1], net->act_box[kProposalLayers - 1], static_cast<int>(batch), s3,
+            c3, b3[0], b3[1], b3[2], net->box_last);
+        ctx->launches++;
+        net->trunk_valid = true;
+    }
     head_kernel<<<batch, 64, 0, ctx->stream>>>(net->box_last, net->params + net->head_w, net->params + net->head_b,
                                                 static_cast<int>(batch), nullptr, pred, nullptr, nullptr, nullptr,
                                                 nullptr);
-    ctx->launches += 2;
+    ctx->launches++;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 

@@ -199,26 +199,37 @@ def test_session_predictions_match_the_plain_forward(gpu_ctx, net):
 @pytest.mark.parametrize("workload", ["box64_cuboid_cube24", "rounded256_blob_hopf512"])
 def test_corner_box_trunk_equals_the_full_split_forward(gpu_ctx, net, workload):
     # The session path runs every layer once on the layout alone and, per
-    # orientation, only over the corner box its item reaches; its predictions
-    # must equal, value for value, the full split forward's
-    # (SPK_PROPOSAL_TRUNK=full), on later layouts and after a parameter change.
+    # orientation, only over the corner box its item reaches, and between
+    # calls recomputes only the voxels a layout change reaches.  Its
+    # predictions must equal, value for value, the full split forward's
+    # (SPK_PROPOSAL_TRUNK=full, on a second network with the same
+    # parameters): over successive placements, after a removal, on an
+    # unchanged layout, and after a parameter change.
     import os
 
     proposal, workloads, session_mod = package("proposal"), package("workloads"), package("session")
-    _set_oracle_parameters(net, 6)
+    full = proposal.Proposal(seed=11, context=gpu_ctx)
+    for n in (net, full):
+        _set_oracle_parameters(n, 6)
     kwargs = {"orientations": 24} if workload.startswith("rounded256") else {}
     wl = getattr(workloads, workload)(**kwargs)
     s = session_mod.Session(wl.obj, wl.container, wl.origin, wl.pitch, wl.catalog, context=gpu_ctx)
-    for step in range(3):
-        if step == 2:
-            _set_oracle_parameters(net, 7)
+    for step in range(6):
+        if step == 3:
+            s.remove_last()  # the layout goes back: a change the trunk must see
+        if step == 5:
+            for n in (net, full):
+                _set_oracle_parameters(n, 7)
         best, pred = proposal.propose(s, net, 4)
+        again_best, again = proposal.propose(s, net, 4)  # unchanged layout
         os.environ["SPK_PROPOSAL_TRUNK"] = "full"
         try:
-            best_full, pred_full = proposal.propose(s, net, 4)
+            best_full, pred_full = proposal.propose(s, full, 4)
         finally:
             os.environ.pop("SPK_PROPOSAL_TRUNK", None)
         assert np.array_equal(pred, pred_full), (step, np.abs(pred - pred_full).max())
-        assert np.array_equal(best, best_full)
-        s.greedy(1)
+        assert np.array_equal(again, pred) and np.array_equal(best, best_full)
+        if step != 2:
+            s.greedy(1)
     s.close()
+    full.close()
