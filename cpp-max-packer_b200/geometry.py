@@ -169,20 +169,23 @@ def broad_phase(bounds_min, bounds_max, finite, clearance_mm: float, proven=None
     return out[:count.value].copy()
 
 
-def export_stl(mesh: AcceptedMesh, translations_mm, quaternions_xyzw, context: Optional[Context] = None) -> bytes:
+def export_stl(mesh: AcceptedMesh, translations_mm, quaternions_xyzw, context: Optional[Context] = None,
+               out: Optional[np.ndarray] = None):
     """The binary STL of the posed copies (pack_io's write_stl_stage,
-    result_export.cpp:1034-1123), computed on the device."""
+    result_export.cpp:1034-1123), computed on the device: the file's bytes,
+    or, with `out` (a uint8 array at least as large), the file's size after
+    writing it there."""
     lib = _lib_ready()
     context = context or default_context()
     mc, keep = _mesh_c(mesh)
     t = _arr(translations_mm, np.float64).reshape(-1, 3)
     q = _arr(quaternions_xyzw, np.float64).reshape(-1, 4)
     size = 84 + 50 * len(mesh.triangles) * len(t)
-    out = np.empty(size, np.uint8)
+    buffer = np.empty(size, np.uint8) if out is None else out
     got = ctypes.c_uint64()
     _lib.check(lib.spk_export_stl(context.handle, ctypes.byref(mc), t.ctypes.data, q.ctypes.data, len(t),
-                                  out.ctypes.data, size, ctypes.byref(got)), "spk_export_stl")
-    return out[:got.value].tobytes()
+                                  buffer.ctypes.data, buffer.nbytes, ctypes.byref(got)), "spk_export_stl")
+    return buffer[:got.value].tobytes() if out is None else int(got.value)
 
 
 def environment_window(bounds_mm, origin_mm, pitch_mm):
