@@ -65,7 +65,8 @@ def main():
     ap.add_argument("--weights", default=os.path.join(HERE, "weights", "proposal_rounded256.npz"))
     ap.add_argument("--max-copies", type=int, default=100000)
     ap.add_argument("--report", default="")
-    ap.add_argument("--configs", default="", help="comma-separated learned configurations: k or k:min_feasible")
+    ap.add_argument("--configs", default="", help="comma-separated learned configurations: k, k:min_feasible, "
+                                                  "or m:k_min:k_max:margin")
     args = ap.parse_args()
     compute, session_mod, workloads, proposal = pkg("compute"), pkg("session"), pkg("workloads"), pkg("proposal")
     ctx = compute.Context(0)
@@ -89,14 +90,22 @@ def main():
         "learned": [],
     }
     for config in configs:
-        k, _, m = config.partition(":")
-        k, m = int(k), int(m or 0)
+        margin = None
+        if config.startswith("m:"):
+            _, k_min, k_max, margin = config.split(":")
+            k, m, k_max, margin = int(k_min), 0, int(k_max), float(margin)
+        else:
+            k, _, m = config.partition(":")
+            k, m = int(k), int(m or 0)
         s = open_session()
-        print(f"learned fill k={k} min_feasible={m}", flush=True)
+        print(f"learned fill k={k} min_feasible={m} margin={margin}", flush=True)
         widened = [0]
 
         def learned(n):
-            if m:
+            if margin is not None:
+                placed, fb, paged = proposal.greedy_proposed_margin(s, net, k, k_max, margin, n)
+                widened[0] += paged
+            elif m:
                 placed, fb, w = proposal.greedy_proposed_adaptive(s, net, k, m, n)
                 widened[0] += w
             else:
@@ -107,6 +116,8 @@ def main():
         ln_scores = [p.score for p in s.placements]
         s.close()
         entry = {"k": k, "min_feasible": m, "copies": ln[0], "fallback_steps": ln[1], "widenings": widened[0],
+                 "margin": margin, "k_max": k_max if margin is not None else None,
+                 "mean_paged": round(widened[0] / max(ln[0], 1), 2) if margin is not None else None,
                  "seconds": round(ln[2], 2), "placements_per_s": round(ln[0] / ln[2], 3),
                  "packed_count_ratio": round(ln[0] / ex[0], 4) if ex[0] else None,
                  "speed_over_exhaustive": round((ln[0] / ln[2]) / (ex[0] / ex[2]), 3) if ex[2] and ln[2] else None,

@@ -1299,6 +1299,74 @@ int spk_session_greedy_proposed(spk_context* ctx, spk_proposal* proposal, uint32
     }
 }
 
+int spk_session_greedy_proposed_margin(spk_context* ctx, spk_proposal* proposal, uint32_t k_min, uint32_t k_max,
+                                       float margin, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
+                                       int64_t* translations, double* scores, uint64_t* fallbacks, uint64_t* paged)
+{
+    try {
+        if (!ctx || !session_of(ctx) || !placed) {
+            return kNotReady;
+        }
+        ProposalNet* net = proposal_net(proposal);
+        if (!net || k_min == 0 || k_max < k_min || !(margin >= 0.f)) {
+            return kInvalidArgument;
+        }
+        auto& s = *session_of(ctx);
+        *placed = 0;
+        if (fallbacks) {
+            *fallbacks = 0;
+        }
+        if (paged) {
+            *paged = 0;
+        }
+        const std::size_t O = s.catalog.size();
+        std::vector<std::size_t> all(O);
+        for (std::size_t o = 0; o < O; ++o) {
+            all[o] = o;
+        }
+        std::vector<float> pred;
+        while (*placed < max_steps) {
+            int status = session_predict(ctx, s, net, pred);
+            if (status) {
+                return status;
+            }
+            const std::vector<std::size_t> ranked = top_k(pred, O);
+            // The k_min best, then every further orientation predicted within
+            // `margin` of the k_min-th, up to k_max.
+            std::size_t n = std::min<std::size_t>(k_min, O);
+            const float cut = pred[ranked[n - 1]] + margin;
+            while (n < std::min<std::size_t>(k_max, O) && pred[ranked[n]] <= cut) {
+                ++n;
+            }
+            const std::vector<std::size_t> subset(ranked.begin(), ranked.begin() + n);
+            if (paged) {
+                *paged += n;
+            }
+            std::optional<Candidate> chosen;
+            if ((status = greedy_step(ctx, s, subset, chosen))) {
+                return status;
+            }
+            if (!chosen) {
+                if ((status = greedy_step(ctx, s, all, chosen))) {
+                    return status;
+                }
+                if (!chosen) {
+                    break;
+                }
+                if (fallbacks) {
+                    ++*fallbacks;
+                }
+            }
+            record(*chosen, *placed, orientations, translations, scores);
+            ++*placed;
+        }
+        return kOk;
+    }
+    catch (...) {
+        return kAllocation;
+    }
+}
+
 int spk_session_greedy_proposed_adaptive(spk_context* ctx, spk_proposal* proposal, uint32_t k,
                                          uint32_t min_feasible, uint64_t max_steps, uint64_t* placed,
                                          uint64_t* orientations, int64_t* translations, double* scores,

@@ -59,6 +59,8 @@ def _declare(lib):
     lib.spk_session_features.argtypes = [P, P, P]
     lib.spk_session_propose.argtypes = [P, P, ctypes.c_uint32, P, P]
     lib.spk_session_greedy_proposed.argtypes = [P, P, ctypes.c_uint32, ctypes.c_uint64, P, P, P, P, P]
+    lib.spk_session_greedy_proposed_margin.argtypes = [P, P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                                       ctypes.c_uint64, P, P, P, P, P, P]
     lib.spk_session_greedy_proposed_adaptive.argtypes = [P, P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64, P,
                                                          P, P, P, P, P]
     lib._proposal_declared = True
@@ -230,6 +232,29 @@ def greedy_proposed(session, net: Proposal, k: int, max_steps: int):
     out = [Placement(int(ori[i]), tuple(int(v) for v in t[i]), float(scores[i])) for i in range(placed.value)]
     session.placements += out
     return out, int(fallbacks.value)
+
+
+def greedy_proposed_margin(session, net: Proposal, k_min: int, k_max: int, margin: float, max_steps: int):
+    """The proposed greedy paging the k_min best orientations and those
+    predicted within `margin` of the k_min-th (at most k_max); returns
+    (placements, fallback steps, orientations paged in all)."""
+    from .session import Placement
+
+    lib = _lib.lib()
+    _declare(lib)
+    n = max(max_steps, 1)
+    ori = np.zeros(n, np.uint64)
+    t = np.zeros((n, 3), np.int64)
+    scores = np.zeros(n, np.float64)
+    placed, fallbacks, paged = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    _lib.check(lib.spk_session_greedy_proposed_margin(session.context.handle, net.handle, k_min, k_max,
+                                                      ctypes.c_float(margin), max_steps, ctypes.byref(placed),
+                                                      ori.ctypes.data, t.ctypes.data, scores.ctypes.data,
+                                                      ctypes.byref(fallbacks), ctypes.byref(paged)),
+               "spk_session_greedy_proposed_margin")
+    out = [Placement(int(ori[i]), tuple(int(v) for v in t[i]), float(scores[i])) for i in range(placed.value)]
+    session.placements += out
+    return out, int(fallbacks.value), int(paged.value)
 
 
 def greedy_proposed_adaptive(session, net: Proposal, k: int, min_feasible: int, max_steps: int):

@@ -492,6 +492,15 @@ int spk_session_propose(spk_context* context, spk_proposal* proposal, uint32_t k
 int spk_session_greedy_proposed(spk_context* context, spk_proposal* proposal, uint32_t k, uint64_t max_steps,
                                 uint64_t* placed, uint64_t* orientations, int64_t* translations, double* scores,
                                 uint64_t* fallbacks);
+/* The proposed greedy with a margin: each step pages the k_min orientations
+ * the network ranks best and every further one whose prediction lies within
+ * `margin` of the k_min-th, at most k_max; the exhaustive fallback as in
+ * spk_session_greedy_proposed.  *paged receives the orientations paged over
+ * all steps (their mean is placed / paged).  No counterpart in the reference. */
+int spk_session_greedy_proposed_margin(spk_context* context, spk_proposal* proposal, uint32_t k_min, uint32_t k_max,
+                                       float margin, uint64_t max_steps, uint64_t* placed, uint64_t* orientations,
+                                       int64_t* translations, double* scores, uint64_t* fallbacks, uint64_t* paged);
+
 /* No counterpart in the reference.  The proposed greedy with widening: when
  * fewer than min_feasible of the k proposed orientations admit any copy, the
  * step pages the next k in the network's order, and so on, before choosing
