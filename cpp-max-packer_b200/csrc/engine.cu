@@ -118,7 +118,7 @@ int object_field(spk_context* ctx, const geo::Prepared& prepared, const double* 
 // edges) outside which every output cell is zero.
 int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Window& requested, const double* origin,
                  double pitch, const geo::Vec3& translation, const geo::Quat& q, double clearance,
-                 std::uint8_t* d_out, EdtBox* support = nullptr)
+                 std::uint8_t* d_out, EdtBox* support = nullptr, const std::uint32_t* d_tris = nullptr)
 {
     if (!geo::canonical_unit(q)) {
         return kFieldInput;
@@ -159,7 +159,7 @@ int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Win
     if (!raw) {
         return status;
     }
-    if ((status = raster_fill(ctx, placed, make_window(plan, origin, pitch), raw, false))) {
+    if ((status = raster_fill(ctx, placed, make_window(plan, origin, pitch), raw, false, nullptr, d_tris))) {
         return status;
     }
     return dilate_crop(ctx, raw, make_window(plan, origin, pitch), halo, clearance, false, d_out,
@@ -223,6 +223,7 @@ struct Session {
     std::uint8_t* mask {};
     std::uint32_t* counts {};
     std::uint8_t* occ {};
+    std::uint32_t* object_tris {};  // the item's triangle indices on the device (placed-copy rasters)
     std::vector<Copy> copies;
     bool dirty { true };
     __nv_bfloat16* items {};  // every orientation's kernel pooled to 32^3 (proposal input)
@@ -311,7 +312,7 @@ int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const
     }
     EdtBox support {};
     if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[orientation], s.pair,
-                               placed, &support))) {
+                               placed, &support, s.object_tris))) {
         return status;
     }
     if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), 1))) {
@@ -944,9 +945,13 @@ int spk_session_open(spk_context* ctx, const spk_session_desc* d, spk_session_in
         s->mask = static_cast<std::uint8_t*>(device_buffer(ctx, "session.mask", n, status));
         s->counts = static_cast<std::uint32_t*>(device_buffer(ctx, "session.counts", n * 4, status));
         s->occ = static_cast<std::uint8_t*>(device_buffer(ctx, "session.occ", n, status));
-        if (!s->mask || !s->counts || !s->occ) {
+        const std::size_t tri_bytes = s->object_mesh.triangles.size() * 12;
+        s->object_tris = static_cast<std::uint32_t*>(device_buffer(ctx, "session.object_tris", tri_bytes, status));
+        if (!s->mask || !s->counts || !s->occ || !s->object_tris) {
             return status;
         }
+        cudaMemcpyAsync(s->object_tris, s->object_mesh.triangles.data(), tri_bytes, cudaMemcpyHostToDevice,
+                        ctx->stream);
         cudaMemsetAsync(s->counts, 0, n * 4, ctx->stream);
         if ((status = container_field(ctx, s->box ? s->box_mm : nullptr, s->box ? nullptr : &s->container, s->env,
                                       s->origin, s->pitch, s->wall, s->mask))) {
@@ -1043,7 +1048,7 @@ int spk_session_remove_last(spk_context* ctx)
             return status;
         }
         if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[c.orientation],
-                                   s.pair, placed))) {
+                                   s.pair, placed, nullptr, s.object_tris))) {
             return status;
         }
         if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), -1))) {

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <vector>
 
 #include "context.hpp"
@@ -33,14 +34,126 @@ int blocks_for(long long n, int threads)
     return static_cast<int>(std::min<long long>(std::max<long long>(want, 1), 148LL * 32));
 }
 
+// Per-face candidate cell ranges on the device: face_ranges
+// (validation_kernel.cpp:3248-3340 cursor bounds) with the host's binary64
+// path, floor((v - origin) / pitch) when the quotient lies farther than
+// |q| 2^-48 + 2^-60 from every integer.  Nearer to an integer n the host
+// takes the floor of a long double quotient, which is n - 1 or n; here the
+// range takes n - 1 for its low end and n for its high end instead.  The
+// range is then at most one cell wider than the host's, and a cell it adds
+// lies outside the face's padded interval bounds, where the SAT's first
+// three axes separate it: the raster is the same.  Quotients of magnitude
+// 2^50 or more, or not finite, set bit 4 of error[0] (the host path then
+// runs).  counts[f] = the clipped range's cell count (0 when outside).
+__global__ void face_ranges_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint, int faces,
+                                   FieldWindow w, geo::FaceRange* __restrict__ ranges,
+                                   long long* __restrict__ counts, int* __restrict__ error)
+{
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= faces) {
+        return;
+    }
+    geo::FaceRange r;
+    r.outside = 0;
+    r.pad = 0;
+    bool host_needed = false;
+    for (int a = 0; a < 3; ++a) {
+        const IVec3& v0 = vint[tris[3 * f]];
+        double low = v0.v[a].low, high = v0.v[a].high;
+        for (int k = 1; k < 3; ++k) {
+            const IVec3& vk = vint[tris[3 * f + k]];
+            low = f_min(low, vk.v[a].low);
+            high = f_max(high, vk.v[a].high);
+        }
+        long long ends[2];
+        for (int e = 0; e < 2; ++e) {
+            const double q = f_div(f_sub(e == 0 ? low : high, w.origin[a]), w.pitch);
+            if (!(fabs(q) < 0x1p50)) {
+                host_needed = true;
+                ends[e] = 0;
+                continue;
+            }
+            const double fl = floor(q);
+            const double margin = f_add(f_mul(fabs(q), 0x1p-48), 0x1p-60);
+            if (f_sub(q, fl) > margin && f_sub(f_add(fl, 1.0), q) > margin) {
+                ends[e] = static_cast<long long>(fl);
+            }
+            else {
+                const long long n = static_cast<long long>(rint(q));
+                ends[e] = e == 0 ? n - 1 : n;
+            }
+        }
+        r.first[a] = ends[0] - 1;
+        r.last[a] = ends[1] + 1;
+        const long long wlast = w.first[a] + static_cast<long long>(w.shape[a] - 1);
+        if (r.last[a] < w.first[a] || r.first[a] > wlast) {
+            r.outside = 1;
+        }
+        r.first[a] = r.first[a] > w.first[a] ? r.first[a] : w.first[a];
+        r.last[a] = r.last[a] < wlast ? r.last[a] : wlast;
+    }
+    if (host_needed) {
+        atomicOr(error, 4);
+    }
+    ranges[f] = r;
+    long long cells = 0;
+    if (!r.outside && r.last[0] >= r.first[0] && r.last[1] >= r.first[1] && r.last[2] >= r.first[2]) {
+        cells = (r.last[0] - r.first[0] + 1) * (r.last[1] - r.first[1] + 1) * (r.last[2] - r.first[2] + 1);
+    }
+    counts[f] = cells;
+}
+
+// offsets[0] = 0, offsets[f + 1] = counts[0] + ... + counts[f], in place
+// over offsets[1..faces] (the counts); one block of 1024 threads.
+__global__ void __launch_bounds__(1024) face_offsets_kernel(long long* __restrict__ offsets, int faces)
+{
+    __shared__ long long warp_sums[32];
+    __shared__ long long carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        carry = 0;
+        offsets[0] = 0;
+    }
+    __syncthreads();
+    for (int start = 0; start < faces; start += 1024) {
+        const int i = start + threadIdx.x;
+        const long long v = i < faces ? offsets[1 + i] : 0;
+        long long inclusive = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long other = __shfl_up_sync(0xffffffffu, inclusive, o);
+            if (lane >= o) {
+                inclusive += other;
+            }
+        }
+        if (lane == 31) {
+            warp_sums[warp] = inclusive;
+        }
+        __syncthreads();
+        long long before = carry;
+        for (int k = 0; k < warp; ++k) {
+            before += warp_sums[k];
+        }
+        if (i < faces) {
+            offsets[1 + i] = before + inclusive;
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) {
+            carry = before + inclusive;
+        }
+        __syncthreads();
+    }
+}
+
 // One thread per (face, cell) pair.  `offsets` is the exclusive prefix sum of
 // the faces' clipped cell-range sizes (outside faces count 0), so small faces
 // pack densely into warps instead of leaving most lanes of a per-face warp idle.
+// The pair count is offsets[faces], read on the device.
 __global__ void __launch_bounds__(128, 6) raster_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint,
                               const geo::FaceRange* __restrict__ ranges, const long long* __restrict__ offsets,
-                              int faces, long long total, FieldWindow w, std::uint8_t* __restrict__ cells,
+                              int faces, FieldWindow w, std::uint8_t* __restrict__ cells,
                               int* __restrict__ error)
 {
+    const long long total = offsets[faces];
     for (long long item = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; item < total;
          item += static_cast<long long>(gridDim.x) * blockDim.x) {
         int lo = 0, hi = faces - 1;  // last face whose offset is <= item: the face that owns it
@@ -251,8 +364,11 @@ __global__ void occupancy_kernel(const std::uint8_t* __restrict__ mask, const st
 
 }  // namespace
 
-int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells, bool normalize,
-                std::uint64_t* uncertain_components)
+namespace {
+
+int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells,
+                     bool normalize, std::uint64_t* uncertain_components, const std::uint32_t* d_tris_kept,
+                     bool host_ranges)
 {
     cudaStream_t st = ctx->stream;
     const auto& mesh = *placed.prepared->mesh;
@@ -260,29 +376,12 @@ int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& 
     if (n >= (1LL << 31)) {
         return kCellLimit;
     }
-    geo::Window gw;
-    for (int a = 0; a < 3; ++a) {
-        gw.first[a] = w.first[a];
-        gw.shape[a] = w.shape[a];
-    }
-    std::vector<geo::FaceRange> ranges;
-    if (!geo::face_ranges(placed, gw, w.origin, w.pitch, ranges)) {
-        return kFieldIndexOverflow;
-    }
     const std::size_t F = mesh.triangles.size(), V = mesh.vertices.size();
-    std::vector<long long> offsets(F + 1, 0);
-    for (std::size_t f = 0; f < F; ++f) {
-        const auto& r = ranges[f];
-        long long cells = 0;
-        if (!r.outside && r.last[0] >= r.first[0] && r.last[1] >= r.first[1] && r.last[2] >= r.first[2]) {
-            cells = (r.last[0] - r.first[0] + 1) * (r.last[1] - r.first[1] + 1) * (r.last[2] - r.first[2] + 1);
-        }
-        offsets[f + 1] = offsets[f] + cells;
-    }
-    const long long total = offsets[F];
     int status = kOk;
-    auto* d_tris = static_cast<std::uint32_t*>(device_buffer(ctx, "field.tris", F * 12, status));
+    auto* d_tris = d_tris_kept ? const_cast<std::uint32_t*>(d_tris_kept)
+                               : static_cast<std::uint32_t*>(device_buffer(ctx, "field.tris", F * 12, status));
     auto* d_vint = static_cast<IVec3*>(device_buffer(ctx, "field.vint", V * sizeof(IVec3), status));
+    auto* h_vint = static_cast<IVec3*>(host_buffer(ctx, "field.vint", V * sizeof(IVec3), status));
     auto* d_ranges = static_cast<geo::FaceRange*>(device_buffer(ctx, "field.ranges", F * sizeof(geo::FaceRange), status));
     auto* d_offsets = static_cast<long long*>(device_buffer(ctx, "field.offsets", (F + 1) * sizeof(long long), status));
     auto* d_parent = static_cast<int*>(device_buffer(ctx, "field.parent", n * sizeof(int), status));
@@ -290,33 +389,75 @@ int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& 
     auto* d_misc = static_cast<int*>(device_buffer(ctx, "field.misc", 64, status));
     const unsigned int root_capacity = 1u << 20;
     auto* d_roots = static_cast<int*>(device_buffer(ctx, "field.roots", root_capacity * 4ULL, status));
-    if (!d_tris || !d_vint || !d_ranges || !d_offsets || !d_parent || !d_rootv || !d_misc || !d_roots) {
+    if (!d_tris || !d_vint || !h_vint || !d_ranges || !d_offsets || !d_parent || !d_rootv || !d_misc || !d_roots) {
         return status;
     }
-    cudaMemcpyAsync(d_tris, mesh.triangles.data(), F * 12, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_vint, placed.intervals.data(), V * sizeof(IVec3), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_ranges, ranges.data(), F * sizeof(geo::FaceRange), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(d_offsets, offsets.data(), (F + 1) * sizeof(long long), cudaMemcpyHostToDevice, st);
+    if (!d_tris_kept) {
+        cudaMemcpyAsync(d_tris, mesh.triangles.data(), F * 12, cudaMemcpyHostToDevice, st);
+    }
+    // The vertex intervals go through pinned memory (the previous call's
+    // copy finished at its synchronisation below).
+    std::memcpy(h_vint, placed.intervals.data(), V * sizeof(IVec3));
+    cudaMemcpyAsync(d_vint, h_vint, V * sizeof(IVec3), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_cells, 0, n, st);
     cudaMemsetAsync(d_misc, 0, 64, st);
     const int threads = 256;
-    if (total > 0) {
+    if (F > 0) {
+        if (host_ranges) {
+            geo::Window gw;
+            for (int a = 0; a < 3; ++a) {
+                gw.first[a] = w.first[a];
+                gw.shape[a] = w.shape[a];
+            }
+            std::vector<geo::FaceRange> ranges;
+            if (!geo::face_ranges(placed, gw, w.origin, w.pitch, ranges)) {
+                return kFieldIndexOverflow;
+            }
+            std::vector<long long> offsets(F + 1, 0);
+            for (std::size_t f = 0; f < F; ++f) {
+                const auto& r = ranges[f];
+                long long cells = 0;
+                if (!r.outside && r.last[0] >= r.first[0] && r.last[1] >= r.first[1] && r.last[2] >= r.first[2]) {
+                    cells = (r.last[0] - r.first[0] + 1) * (r.last[1] - r.first[1] + 1) * (r.last[2] - r.first[2] + 1);
+                }
+                offsets[f + 1] = offsets[f] + cells;
+            }
+            cudaMemcpyAsync(d_ranges, ranges.data(), F * sizeof(geo::FaceRange), cudaMemcpyHostToDevice, st);
+            cudaMemcpyAsync(d_offsets, offsets.data(), (F + 1) * sizeof(long long), cudaMemcpyHostToDevice, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) {  // the host vectors end with this scope
+                cudaGetLastError();
+                return kCuda;
+            }
+        }
+        else {
+            face_ranges_kernel<<<static_cast<unsigned>((F + 255) / 256), 256, 0, st>>>(
+                d_tris, d_vint, static_cast<int>(F), w, d_ranges, d_offsets + 1, d_misc);
+            face_offsets_kernel<<<1, 1024, 0, st>>>(d_offsets, static_cast<int>(F));
+        }
         // 128-thread blocks, six to an SM: the SAT's dependent FP64 chains need
         // the resident warps more than the registers that spill (measured).
-        raster_kernel<<<blocks_for(total, 128), 128, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets,
-                                                                      static_cast<int>(F), total, w, d_cells, d_misc);
+        // The pair count is on the device; a grid of four waves loops over it.
+        raster_kernel<<<148 * 6 * 4, 128, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets, static_cast<int>(F), w,
+                                                  d_cells, d_misc);
+        ctx->launches += 3;
     }
     ccl_init_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, n);
     ccl_union_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, w.shape[0], w.shape[1],
                                                                    w.shape[2], d_misc);
     auto* d_root_count = reinterpret_cast<unsigned int*>(d_misc + 4);
     ccl_compress_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_parent, n, d_roots, d_root_count, root_capacity);
-    ctx->launches += total > 0 ? 4 : 3;
+    ctx->launches += 3;
     int h_misc[8];
     cudaMemcpyAsync(h_misc, d_misc, 32, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) {
         cudaGetLastError();
         return kCuda;
+    }
+    if (h_misc[0] & 4) {
+        // A quotient the device's binary64 path does not cover: the host's
+        // face ranges (with their long double floors) decide, and the raster
+        // and labels run again from them.
+        return raster_fill_impl(ctx, placed, w, d_cells, normalize, uncertain_components, d_tris_kept, true);
     }
     if (h_misc[0] & 1) {
         return kFieldIndexOverflow;
@@ -360,6 +501,14 @@ int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& 
     fill_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, d_rootv, n, normalize ? 1 : 0);
     ctx->launches++;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+}  // namespace
+
+int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells, bool normalize,
+                std::uint64_t* uncertain_components, const std::uint32_t* d_tris_kept)
+{
+    return raster_fill_impl(ctx, placed, w, d_cells, normalize, uncertain_components, d_tris_kept, false);
 }
 
 int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,

@@ -31,8 +31,11 @@ inline FieldWindow make_window(const geo::Window& w, const double* origin, doubl
 
 // Raster + component fill of `placed` over window `w` into d_cells (u8,
 // values 0/1/2/3, or 0/1 when `normalize`).
+// d_tris_kept: the mesh's triangle indices already on the device (a
+// session keeps its item's), or null to upload them.
 int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells,
-                bool normalize, std::uint64_t* uncertain_components = nullptr);
+                bool normalize, std::uint64_t* uncertain_components = nullptr,
+                const std::uint32_t* d_tris_kept = nullptr);
 // Clearance dilation of a raw field into the requested window.
 int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,
                 double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req);
