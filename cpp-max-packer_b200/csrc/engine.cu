@@ -118,7 +118,8 @@ int object_field(spk_context* ctx, const geo::Prepared& prepared, const double* 
 // edges) outside which every output cell is zero.
 int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Window& requested, const double* origin,
                  double pitch, const geo::Vec3& translation, const geo::Quat& q, double clearance,
-                 std::uint8_t* d_out, EdtBox* support = nullptr, const std::uint32_t* d_tris = nullptr)
+                 std::uint8_t* d_out, EdtBox* support = nullptr, const std::uint32_t* d_tris = nullptr,
+                 const double* d_vertices = nullptr)
 {
     if (!geo::canonical_unit(q)) {
         return kFieldInput;
@@ -129,7 +130,15 @@ int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Win
     }
     const geo::Window work = expanded(requested, halo);
     geo::Placed placed;
-    if (!geo::place(prepared, translation, q, placed)) {
+    // With the item's vertices on the device, a non-cardinal pose's vertex
+    // intervals are computed there (the host reads back only their bounds).
+    bool on_device = false;
+    int status = kOk;
+    if (d_vertices && d_tris &&
+        (status = place_on_device(ctx, prepared, d_vertices, translation, q, placed, on_device))) {
+        return status;
+    }
+    if (!on_device && !geo::place(prepared, translation, q, placed)) {
         return kFieldInput;
     }
     geo::Window plan;
@@ -154,12 +163,12 @@ int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Win
             support->hi[a] = static_cast<int>(std::min(std::max(hi, -1LL), top + 1));
         }
     }
-    int status = kOk;
     auto* raw = static_cast<std::uint8_t*>(device_buffer(ctx, "placed.raw", cells_of(plan), status));
     if (!raw) {
         return status;
     }
-    if ((status = raster_fill(ctx, placed, make_window(plan, origin, pitch), raw, false, nullptr, d_tris))) {
+    if ((status = raster_fill(ctx, placed, make_window(plan, origin, pitch), raw, false, nullptr, d_tris,
+                              on_device))) {
         return status;
     }
     return dilate_crop(ctx, raw, make_window(plan, origin, pitch), halo, clearance, false, d_out,
@@ -224,6 +233,7 @@ struct Session {
     std::uint32_t* counts {};
     std::uint8_t* occ {};
     std::uint32_t* object_tris {};  // the item's triangle indices on the device (placed-copy rasters)
+    double* object_vertices {};     // and its vertices
     std::vector<Copy> copies;
     bool dirty { true };
     __nv_bfloat16* items {};  // every orientation's kernel pooled to 32^3 (proposal input)
@@ -312,7 +322,7 @@ int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const
     }
     EdtBox support {};
     if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[orientation], s.pair,
-                               placed, &support, s.object_tris))) {
+                               placed, &support, s.object_tris, s.object_vertices))) {
         return status;
     }
     if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), 1))) {
@@ -946,11 +956,15 @@ int spk_session_open(spk_context* ctx, const spk_session_desc* d, spk_session_in
         s->counts = static_cast<std::uint32_t*>(device_buffer(ctx, "session.counts", n * 4, status));
         s->occ = static_cast<std::uint8_t*>(device_buffer(ctx, "session.occ", n, status));
         const std::size_t tri_bytes = s->object_mesh.triangles.size() * 12;
+        const std::size_t vertex_bytes = s->object_mesh.vertices.size() * 24;
         s->object_tris = static_cast<std::uint32_t*>(device_buffer(ctx, "session.object_tris", tri_bytes, status));
-        if (!s->mask || !s->counts || !s->occ || !s->object_tris) {
+        s->object_vertices = static_cast<double*>(device_buffer(ctx, "session.object_vertices", vertex_bytes, status));
+        if (!s->mask || !s->counts || !s->occ || !s->object_tris || !s->object_vertices) {
             return status;
         }
         cudaMemcpyAsync(s->object_tris, s->object_mesh.triangles.data(), tri_bytes, cudaMemcpyHostToDevice,
+                        ctx->stream);
+        cudaMemcpyAsync(s->object_vertices, s->object_mesh.vertices.data(), vertex_bytes, cudaMemcpyHostToDevice,
                         ctx->stream);
         cudaMemsetAsync(s->counts, 0, n * 4, ctx->stream);
         if ((status = container_field(ctx, s->box ? s->box_mm : nullptr, s->box ? nullptr : &s->container, s->env,
@@ -1048,7 +1062,7 @@ int spk_session_remove_last(spk_context* ctx)
             return status;
         }
         if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[c.orientation],
-                                   s.pair, placed, nullptr, s.object_tris))) {
+                                   s.pair, placed, nullptr, s.object_tris, s.object_vertices))) {
             return status;
         }
         if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), -1))) {

@@ -34,6 +34,79 @@ int blocks_for(long long n, int threads)
     return static_cast<int>(std::min<long long>(std::max<long long>(want, 1), 148LL * 32));
 }
 
+// The placed copy's vertex intervals (place(), validation_kernel.cpp:
+// 805-943) on the device, for a rotation that is not cardinal: each
+// coordinate is transformed_interval_at, the code the host runs.  Each block
+// also reduces its vertices' bounds (lowest low, highest high per axis) into
+// partial[block]; error[0] is set when an interval is not valid.
+struct PoseIntervals {
+    Interval rotation[3][3];
+    double translation[3];
+};
+
+__global__ void __launch_bounds__(256) vertex_intervals_kernel(const double* __restrict__ vertices, int count,
+                                                              const PoseIntervals pose, IVec3* __restrict__ vint,
+                                                              double* __restrict__ partial, int* __restrict__ error)
+{
+    __shared__ double lows[3][256], highs[3][256];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = INFINITY;
+        hi[a] = -INFINITY;
+    }
+    if (i < count) {
+        const double point[3] = { vertices[3 * i], vertices[3 * i + 1], vertices[3 * i + 2] };
+        IVec3 out;
+        bool valid = true;
+        for (int a = 0; a < 3; ++a) {
+            out.v[a] = transformed_interval_at(point, pose.translation, pose.rotation, a);
+            valid = valid && out.v[a].valid;
+            lo[a] = out.v[a].low;
+            hi[a] = out.v[a].high;
+        }
+        vint[i] = out;
+        if (!valid) {
+            atomicOr(error, 1);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        lows[a][threadIdx.x] = lo[a];
+        highs[a][threadIdx.x] = hi[a];
+    }
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) {
+            for (int a = 0; a < 3; ++a) {
+                lows[a][threadIdx.x] = f_min(lows[a][threadIdx.x], lows[a][threadIdx.x + h]);
+                highs[a][threadIdx.x] = f_max(highs[a][threadIdx.x], highs[a][threadIdx.x + h]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; ++a) {
+            partial[6 * blockIdx.x + a] = lows[a][0];
+            partial[6 * blockIdx.x + 3 + a] = highs[a][0];
+        }
+    }
+}
+
+// The blocks' partial bounds reduced to out[0..5] (one thread).
+__global__ void vertex_bounds_kernel(const double* __restrict__ partial, int blocks, double* __restrict__ out)
+{
+    double b[6] = { INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY };
+    for (int k = 0; k < blocks; ++k) {
+        for (int a = 0; a < 3; ++a) {
+            b[a] = f_min(b[a], partial[6 * k + a]);
+            b[3 + a] = f_max(b[3 + a], partial[6 * k + 3 + a]);
+        }
+    }
+    for (int a = 0; a < 6; ++a) {
+        out[a] = b[a];
+    }
+}
+
 // Per-face candidate cell ranges on the device: face_ranges
 // (validation_kernel.cpp:3248-3340 cursor bounds) with the host's binary64
 // path, floor((v - origin) / pitch) when the quotient lies farther than
@@ -368,7 +441,7 @@ namespace {
 
 int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells,
                      bool normalize, std::uint64_t* uncertain_components, const std::uint32_t* d_tris_kept,
-                     bool host_ranges)
+                     bool device_intervals, bool host_ranges)
 {
     cudaStream_t st = ctx->stream;
     const auto& mesh = *placed.prepared->mesh;
@@ -395,10 +468,12 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
     if (!d_tris_kept) {
         cudaMemcpyAsync(d_tris, mesh.triangles.data(), F * 12, cudaMemcpyHostToDevice, st);
     }
-    // The vertex intervals go through pinned memory (the previous call's
-    // copy finished at its synchronisation below).
-    std::memcpy(h_vint, placed.intervals.data(), V * sizeof(IVec3));
-    cudaMemcpyAsync(d_vint, h_vint, V * sizeof(IVec3), cudaMemcpyHostToDevice, st);
+    if (!device_intervals) {
+        // The vertex intervals go through pinned memory (the previous call's
+        // copy finished at its synchronisation below).
+        std::memcpy(h_vint, placed.intervals.data(), V * sizeof(IVec3));
+        cudaMemcpyAsync(d_vint, h_vint, V * sizeof(IVec3), cudaMemcpyHostToDevice, st);
+    }
     cudaMemsetAsync(d_cells, 0, n, st);
     cudaMemsetAsync(d_misc, 0, 64, st);
     const int threads = 256;
@@ -409,8 +484,23 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
                 gw.first[a] = w.first[a];
                 gw.shape[a] = w.shape[a];
             }
+            // The host reads the vertex intervals; those made on the device
+            // come back first.
+            const geo::Placed* source = &placed;
+            geo::Placed with_intervals;
+            if (device_intervals) {
+                with_intervals = placed;
+                with_intervals.intervals.resize(V);
+                if (cudaMemcpyAsync(with_intervals.intervals.data(), d_vint, V * sizeof(IVec3), cudaMemcpyDeviceToHost,
+                                    st) != cudaSuccess ||
+                    cudaStreamSynchronize(st) != cudaSuccess) {
+                    cudaGetLastError();
+                    return kCuda;
+                }
+                source = &with_intervals;
+            }
             std::vector<geo::FaceRange> ranges;
-            if (!geo::face_ranges(placed, gw, w.origin, w.pitch, ranges)) {
+            if (!geo::face_ranges(*source, gw, w.origin, w.pitch, ranges)) {
                 return kFieldIndexOverflow;
             }
             std::vector<long long> offsets(F + 1, 0);
@@ -457,7 +547,8 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
         // A quotient the device's binary64 path does not cover: the host's
         // face ranges (with their long double floors) decide, and the raster
         // and labels run again from them.
-        return raster_fill_impl(ctx, placed, w, d_cells, normalize, uncertain_components, d_tris_kept, true);
+        return raster_fill_impl(ctx, placed, w, d_cells, normalize, uncertain_components, d_tris_kept,
+                                device_intervals, true);
     }
     if (h_misc[0] & 1) {
         return kFieldIndexOverflow;
@@ -506,9 +597,73 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
 }  // namespace
 
 int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells, bool normalize,
-                std::uint64_t* uncertain_components, const std::uint32_t* d_tris_kept)
+                std::uint64_t* uncertain_components, const std::uint32_t* d_tris_kept, bool device_intervals)
 {
-    return raster_fill_impl(ctx, placed, w, d_cells, normalize, uncertain_components, d_tris_kept, false);
+    return raster_fill_impl(ctx, placed, w, d_cells, normalize, uncertain_components, d_tris_kept, device_intervals,
+                            false);
+}
+
+int place_on_device(spk_context* ctx, const geo::Prepared& prepared, const double* d_vertices,
+                    const geo::Vec3& translation, const geo::Quat& q, geo::Placed& out, bool& done)
+{
+    done = false;
+    if (!geo::finite_pose(translation, q)) {
+        return kOk;  // the host's place() decides
+    }
+    const auto transform = geo::rotation_transform(q);
+    if (!transform || transform->exact_cardinal) {
+        return kOk;
+    }
+    const auto& mesh = *prepared.mesh;
+    const int V = static_cast<int>(mesh.vertices.size());
+    if (V == 0) {
+        return kOk;
+    }
+    cudaStream_t st = ctx->stream;
+    int status = kOk;
+    const int blocks = (V + 255) / 256;
+    auto* d_vint = static_cast<IVec3*>(device_buffer(ctx, "field.vint", V * sizeof(IVec3), status));
+    auto* d_partial = static_cast<double*>(device_buffer(ctx, "field.vpartial", (6 * blocks + 6) * 8, status));
+    auto* d_err = static_cast<int*>(device_buffer(ctx, "field.verr", 4, status));
+    auto* h_out = static_cast<double*>(host_buffer(ctx, "field.vbounds", 8 * 8, status));
+    if (!d_vint || !d_partial || !d_err || !h_out) {
+        return status;
+    }
+    PoseIntervals pose {};
+    geo::rotation_intervals(q, pose.rotation);
+    for (int a = 0; a < 3; ++a) {
+        pose.translation[a] = translation[a];
+    }
+    cudaMemsetAsync(d_err, 0, 4, st);
+    vertex_intervals_kernel<<<blocks, 256, 0, st>>>(d_vertices, V, pose, d_vint, d_partial, d_err);
+    vertex_bounds_kernel<<<1, 1, 0, st>>>(d_partial, blocks, d_partial + 6 * blocks);
+    ctx->launches += 2;
+    cudaMemcpyAsync(h_out, d_partial + 6 * blocks, 48, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(h_out + 6, d_err, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return kCuda;
+    }
+    int invalid = 0;
+    std::memcpy(&invalid, h_out + 6, 4);
+    if (invalid) {
+        return kOk;  // the host's place() decides (it returns false)
+    }
+    out = geo::Placed {};
+    out.prepared = &prepared;
+    out.translation = translation;
+    out.q = q;
+    out.is_cardinal = false;
+    for (int a = 0; a < 3; ++a) {
+        out.source_axis[a] = transform->source_axis[a];
+        out.sign[a] = transform->sign[a];
+        out.conservative.min[a] = h_out[a];
+        out.conservative.max[a] = h_out[3 + a];
+    }
+    out.finite = true;
+    out.world_exact = false;
+    done = true;
+    return kOk;
 }
 
 int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,

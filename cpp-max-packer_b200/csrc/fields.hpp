@@ -32,10 +32,21 @@ inline FieldWindow make_window(const geo::Window& w, const double* origin, doubl
 // Raster + component fill of `placed` over window `w` into d_cells (u8,
 // values 0/1/2/3, or 0/1 when `normalize`).
 // d_tris_kept: the mesh's triangle indices already on the device (a
-// session keeps its item's), or null to upload them.
+// session keeps its item's), or null to upload them.  device_intervals: the
+// vertex intervals are already in the context's "field.vint" buffer
+// (place_on_device), so placed.intervals is not read.
 int raster_fill(spk_context* ctx, const geo::Placed& placed, const FieldWindow& w, std::uint8_t* d_cells,
                 bool normalize, std::uint64_t* uncertain_components = nullptr,
-                const std::uint32_t* d_tris_kept = nullptr);
+                const std::uint32_t* d_tris_kept = nullptr, bool device_intervals = false);
+
+// place() for a rotation that is not cardinal, with the vertex intervals
+// computed on the device (d_vertices: the mesh's vertices there) into the
+// context's "field.vint" buffer; on the host `out` receives everything the
+// window plan and the witnesses read (conservative bounds, pose), not the
+// per-vertex vectors.  done = false: the pose is cardinal, not finite or
+// has an invalid interval, and the host's place() must run instead.
+int place_on_device(spk_context* ctx, const geo::Prepared& prepared, const double* d_vertices,
+                    const geo::Vec3& translation, const geo::Quat& q, geo::Placed& out, bool& done);
 // Clearance dilation of a raw field into the requested window.
 int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,
                 double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req);

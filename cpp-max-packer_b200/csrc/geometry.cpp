@@ -99,34 +99,12 @@ bool cardinal_rotation(const Quat& quaternion, int* source_axis, int* sign)
     return true;
 }
 
-// multiply_interval(a, point_interval(p)).  With a point operand the four
-// products are two, each computed twice, and the first-minimum / first-maximum
-// scan picks the same values from the pair, so the result is identical.
-Interval multiply_by_point(const Interval& a, double p)
-{
-    if (!a.valid || !f_finite(p)) {
-        return { 0, 0, false };
-    }
-    const double v0 = f_mul(a.low, p), v2 = f_mul(a.high, p);
-    if (!f_finite(v0) || !f_finite(v2)) {
-        return { 0, 0, false };
-    }
-    double lo = v0, hi = v0;
-    if (v2 < lo) lo = v2;
-    if (hi < v2) hi = v2;
-    return widened(lo, hi);
-}
-
 Interval transformed_interval(const Vec3& point, const Vec3& translation, const Interval rotation[3][3], int row)
 {
-    Interval value = point_interval(translation[row]);
-    for (int column = 0; column < 3; ++column) {
-        value = add_interval(value, multiply_by_point(rotation[row][column], point[column]));
-    }
-    return value;
+    return transformed_interval_at(point.data(), translation.data(), rotation, row);
 }
 
-bool finite_pose(const Vec3& translation, const Quat& q)
+bool finite_pose_in(const Vec3& translation, const Quat& q)
 {
     return finite3(translation) && std::isfinite(q[0]) && std::isfinite(q[1]) && std::isfinite(q[2]) &&
            std::isfinite(q[3]) && (q[0] != 0.0 || q[1] != 0.0 || q[2] != 0.0 || q[3] != 0.0);
@@ -371,6 +349,8 @@ Decision local_interval_point_in_material(const Placed& solid, const Bounds& wi)
 }
 
 }  // namespace
+
+bool finite_pose(const Vec3& translation, const Quat& q) { return finite_pose_in(translation, q); }
 
 Prepared prepare(const Mesh& mesh)
 {
@@ -650,7 +630,7 @@ void run_chunks(std::size_t n, std::size_t parts, const Body& body)
 
 bool place(const Prepared& prepared, const Vec3& translation, const Quat& q, Placed& out)
 {
-    if (!finite_pose(translation, q)) {
+    if (!finite_pose_in(translation, q)) {
         return false;
     }
     const auto transform = rotation_transform(q);
@@ -1054,7 +1034,7 @@ std::vector<std::array<std::int64_t, 3>> make_stencil(std::uint64_t halo, double
 
 bool oriented_bounds(const Mesh& mesh, const Quat& q, Bounds& out)
 {
-    if (!finite_pose({ 0, 0, 0 }, q)) {
+    if (!finite_pose_in({ 0, 0, 0 }, q)) {
         return false;
     }
     const auto transform = rotation_transform(q);
@@ -1105,7 +1085,7 @@ bool oriented_bounds(const Mesh& mesh, const Quat& q, Bounds& out)
 // intervals.  False where the reference returns no bounds.
 bool posed_bounds(const Mesh& mesh, const Vec3& translation, const Quat& q, Bounds& out)
 {
-    if (!finite_pose(translation, q)) {
+    if (!finite_pose_in(translation, q)) {
         return false;
     }
     const auto transform = rotation_transform(q);

@@ -75,6 +75,9 @@ struct Placed {
     bool world_exact {};
 };
 bool place(const Prepared& prepared, const Vec3& translation, const Quat& q, Placed& out);
+// finite_pose (validation_kernel.cpp): a finite translation and a finite,
+// non-zero quaternion.
+bool finite_pose(const Vec3& translation, const Quat& q);
 
 struct Window {
     std::int64_t first[3] {};

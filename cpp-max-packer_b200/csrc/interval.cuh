@@ -163,6 +163,37 @@ SPK_HD Interval multiply_interval(Interval a, Interval b)
     return widened(lo, hi);
 }
 
+// multiply_interval(a, point_interval(p)).  With a point operand the four
+// products are two, each computed twice, and the first-minimum / first-maximum
+// scan picks the same values from the pair, so the result is identical.
+SPK_HD Interval multiply_by_point(const Interval& a, double p)
+{
+    if (!a.valid || !f_finite(p)) {
+        return { 0, 0, false };
+    }
+    const double v0 = f_mul(a.low, p), v2 = f_mul(a.high, p);
+    if (!f_finite(v0) || !f_finite(v2)) {
+        return { 0, 0, false };
+    }
+    double lo = v0, hi = v0;
+    if (v2 < lo) lo = v2;
+    if (hi < v2) hi = v2;
+    return widened(lo, hi);
+}
+
+// transformed_interval (validation_kernel.cpp:805-943): row `row` of the
+// rotation intervals applied to a point, plus the translation, as intervals.
+// Host and device run this same code.
+SPK_HD Interval transformed_interval_at(const double* point, const double* translation, const Interval (*rotation)[3],
+                                        int row)
+{
+    Interval value = point_interval(translation[row]);
+    for (int column = 0; column < 3; ++column) {
+        value = add_interval(value, multiply_by_point(rotation[row][column], point[column]));
+    }
+    return value;
+}
+
 SPK_HD Interval divide_interval(Interval n, Interval d)
 {
     if (!n.valid || !d.valid || d.low <= 0.0) {
