@@ -165,6 +165,33 @@ def test_proposed_greedy_with_every_orientation_is_the_exhaustive_greedy(gpu_ctx
 
 
 @pytest.mark.gpu
+def test_margin_greedy_reduces_to_the_fixed_and_exhaustive_greedies(gpu_ctx, net):
+    # A zero margin with k_max = k_min pages exactly the k_min best, as the
+    # proposed greedy with k = k_min; k_min = every orientation is the
+    # exhaustive greedy.
+    proposal = package("proposal")
+    s, wl = _small_session(gpu_ctx)
+    want, _ = proposal.greedy_proposed(s, net, 5, 6)
+    s.close()
+    s, wl = _small_session(gpu_ctx)
+    got, fallbacks, paged = proposal.greedy_proposed_margin(s, net, 5, 5, 0.0, 6)
+    assert [(p.orientation_index, p.translation, p.score) for p in got] == \
+        [(p.orientation_index, p.translation, p.score) for p in want]
+    assert paged == 5 * len(got)
+    s.close()
+    s, wl = _small_session(gpu_ctx)
+    exhaustive = s.greedy(6)
+    s.close()
+    s, wl = _small_session(gpu_ctx)
+    O = len(wl.catalog)
+    got, fallbacks, paged = proposal.greedy_proposed_margin(s, net, O, O, 0.5, 6)
+    assert fallbacks == 0 and paged == O * len(got)
+    assert [(p.orientation_index, p.translation, p.score) for p in got] == \
+        [(p.orientation_index, p.translation, p.score) for p in exhaustive]
+    s.close()
+
+
+@pytest.mark.gpu
 def test_proposed_greedy_places_exact_copies(gpu_ctx, net):
     proposal = package("proposal")
     s, wl = _small_session(gpu_ctx)
