@@ -251,11 +251,16 @@ struct Session {
 
 Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
 
-int refresh(spk_context* ctx, Session& s)
+// Brings the occupancy up to date on the context's stream and queues the
+// pipeline's proximity and spectrum update on the pipeline's own stream
+// (refresh_begin), so that work that needs only the occupancy (the
+// proposal) runs beside it.
+int refresh_async(spk_context* ctx, Session& s)
 {
     if (!s.dirty) {
         return kOk;
     }
+    s.pipe->refresh_order();
     const long long n = static_cast<long long>(cells_of(s.env));
     int status = occupancy(ctx, s.mask, s.counts, s.occ, n);
     if (status) {
@@ -263,16 +268,26 @@ int refresh(spk_context* ctx, Session& s)
     }
     if (s.one_added) {
         auto* placed = static_cast<std::uint8_t*>(device_buffer(ctx, "session.placed", cells_of(s.env), status));
-        if (!placed || (status = s.pipe->add_occupied(s.occ, placed, s.added_support))) {
+        if (!placed || (status = s.pipe->refresh_begin(s.occ, placed, &s.added_support))) {
             return status ? status : kAllocation;
         }
     }
-    else if ((status = s.pipe->set_occupancy(s.occ))) {
+    else if ((status = s.pipe->refresh_begin(s.occ, nullptr, nullptr))) {
         return status;
     }
     s.dirty = false;
     s.one_added = false;
     return kOk;
+}
+
+// The same, then the context's stream waits for the update.
+int refresh(spk_context* ctx, Session& s)
+{
+    int status = refresh_async(ctx, s);
+    if (!status) {
+        s.pipe->refresh_order();
+    }
+    return status;
 }
 
 void to_c(const Candidate& c, spk_candidate& out)
@@ -312,6 +327,7 @@ int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const
     if (orientation >= s.catalog.size()) {
         return kCatalog;
     }
+    s.pipe->refresh_order();  // a queued update may still read the placed-copy buffer
     const geo::Vec3 translation { s.origin[0] + s.pitch * static_cast<double>(t[0]),
                                   s.origin[1] + s.pitch * static_cast<double>(t[1]),
                                   s.origin[2] + s.pitch * static_cast<double>(t[2]) };
@@ -606,7 +622,7 @@ int session_items(spk_context* ctx, Session& s)
 // Pools the current occupancy to the proposal grid.
 int session_crop(spk_context* ctx, Session& s, __nv_bfloat16*& crop)
 {
-    int status = refresh(ctx, s);
+    int status = refresh_async(ctx, s);
     if (status) {
         return status;
     }
@@ -1052,6 +1068,7 @@ int spk_session_remove_last(spk_context* ctx)
             return kNotReady;
         }
         auto& s = *session_of(ctx);
+        s.pipe->refresh_order();  // a queued update may still read the placed-copy buffer
         const Copy c = s.copies.back();
         const geo::Vec3 translation { s.origin[0] + s.pitch * static_cast<double>(c.t[0]),
                                       s.origin[1] + s.pitch * static_cast<double>(c.t[1]),

@@ -1388,6 +1388,12 @@ Pipeline::Pipeline(spk_context* ctx) : ctx_(ctx)
 
 Pipeline::~Pipeline()
 {
+    if (side_) {
+        cudaStreamSynchronize(side_);
+        cudaEventDestroy(ev_in_);
+        cudaEventDestroy(ev_done_);
+        cudaStreamDestroy(side_);
+    }
     for (auto& s : slots_) {
         cudaFree(s.partial);
         cudaFree(s.ones);
@@ -1672,17 +1678,68 @@ int Pipeline::update_spectrum()
             ctx_->launches++;
         }
     }
-    std::vector<double> host(blocks);
-    cudaMemcpyAsync(host.data(), partial, blocks * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (cudaStreamSynchronize(st) != cudaSuccess) {
+    // The partial sums of b^2 + p^2 come back to pinned memory; the host
+    // adds them up (finish_norm) only when a page needs the error bound, so
+    // nothing here waits for the device.
+    auto* host = static_cast<double*>(host_buffer(ctx_, "pipe.norm", blocks * sizeof(double), status));
+    if (!host) {
+        return status;
+    }
+    cudaMemcpyAsync(host, partial, blocks * sizeof(double), cudaMemcpyDeviceToHost, st);
+    norm_host_ = host;
+    norm_blocks_ = blocks;
+    norm_stream_ = st;
+    norm_pending_ = true;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int Pipeline::finish_norm()
+{
+    if (!norm_pending_) {
+        return kOk;
+    }
+    if (cudaStreamSynchronize(norm_stream_) != cudaSuccess) {
+        cudaGetLastError();
         return kCuda;
     }
     double sum = 0;
-    for (double v : host) {
-        sum += v;
+    for (int i = 0; i < norm_blocks_; ++i) {
+        sum += norm_host_[i];
     }
     z_norm_ = std::sqrt(sum);
+    norm_pending_ = false;
     return kOk;
+}
+
+int Pipeline::refresh_begin(const std::uint8_t* d_occupancy, const std::uint8_t* d_sites, const EdtBox* sites)
+{
+    refresh_order();
+    if (!side_) {
+        if (cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_in_, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&ev_done_, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return kCuda;
+        }
+    }
+    cudaStream_t main = ctx_->stream;
+    cudaEventRecord(ev_in_, main);
+    cudaStreamWaitEvent(side_, ev_in_, 0);
+    // Every launch of the update goes to the side stream while it is queued.
+    ctx_->stream = side_;
+    const int status = d_sites ? add_occupied(d_occupancy, d_sites, *sites) : set_occupancy(d_occupancy);
+    cudaEventRecord(ev_done_, side_);
+    ctx_->stream = main;
+    pending_ = true;
+    return status;
+}
+
+void Pipeline::refresh_order()
+{
+    if (pending_) {
+        cudaStreamWaitEvent(ctx_->stream, ev_done_, 0);
+        pending_ = false;
+    }
 }
 
 int Pipeline::add_kernel(std::uint64_t orientation, const std::int64_t* first, const std::uint32_t* shape,
@@ -1956,6 +2013,10 @@ int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, float targe
 
 int Pipeline::pages(const std::vector<PageRequest>& requests, std::vector<PageOutcome>& out, bool full)
 {
+    refresh_order();
+    if (int status = finish_norm()) {
+        return status;
+    }
     std::vector<std::size_t> ordinary;
     for (std::size_t r = 0; r < requests.size(); ++r) {
         if (!requests[r].low_overlap) {

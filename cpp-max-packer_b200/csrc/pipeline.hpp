@@ -125,6 +125,14 @@ public:
     // d_sites != 0 (all inside `sites`, window coordinates) became occupied:
     // the EDT is updated in place over the region they can affect.
     int add_occupied(const std::uint8_t* d_occupancy, const std::uint8_t* d_sites, const EdtBox& sites);
+    // The same updates queued on the pipeline's own stream, after the work
+    // already on the context's stream (d_sites null: set_occupancy), so that
+    // the context's stream can run other work (the proposal) meanwhile.
+    // refresh_order() makes the context's stream wait for it; pages() does
+    // so itself.  Until then nothing the update writes may be read, and
+    // nothing it reads (the occupancy, the sites) rewritten.
+    int refresh_begin(const std::uint8_t* d_occupancy, const std::uint8_t* d_sites, const EdtBox* sites);
+    void refresh_order();
     // Adds an oriented kernel field (host cells, X-fastest); returns the slot.
     int add_kernel(std::uint64_t orientation, const std::int64_t* first, const std::uint32_t* shape,
                    const std::uint8_t* cells, double max_z, std::uint64_t& slot);
@@ -151,6 +159,8 @@ private:
                  unsigned long long* resid);
     double pass_a_bytes(const KernelSlot& s) const;
     int update_spectrum();
+    // z_norm_ from the spectrum's partial sums, once the device has them.
+    int finish_norm();
     // Transform lengths per axis for the window (the autotuner); sets L_.
     int choose_lengths(const std::uint32_t* env_shape);
     // Pass A for up to kPassABatch orientations in one launch (256^3 grids);
@@ -178,6 +188,13 @@ private:
     bool fused_b_ {};  // 256^3: passes B1 and B2 as one cluster kernel (SPK_PASS_B=fused), else two passes
     const double* table_ {};
     double z_norm_ {};  // sqrt(sum over cells of b^2 + p^2)
+    const double* norm_host_ {};  // pinned partial sums of the last update_spectrum
+    int norm_blocks_ {};
+    cudaStream_t norm_stream_ {};
+    bool norm_pending_ {};
+    cudaStream_t side_ {};  // refresh_begin's stream
+    cudaEvent_t ev_in_ {}, ev_done_ {};
+    bool pending_ {};
     std::vector<KernelSlot> slots_;
 
 public:
