@@ -269,7 +269,9 @@ SPK_HD bool triangle_box_disjoint(const IVec3* tri, const IVec3& box)
         return true;
     }
     const IVec3 edges[3] = { first, second, ivec_sub(tri[2], tri[1]) };
-#pragma unroll
+    // The edge loop stays rolled: nine unrolled axis tests made the raster
+    // wait on instruction fetch (measured faster rolled, at six blocks per SM).
+#pragma unroll 1
     for (int e = 0; e < 3; ++e) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
