@@ -248,9 +248,9 @@ SPK_HD bool projection_separates(const IVec3* tri, const IVec3& box, const IVec3
 // 13-axis separating-axis test of a triangle (vertex intervals) and a box.
 SPK_HD bool triangle_box_disjoint(const IVec3* tri, const IVec3& box)
 {
-    // The loops are unrolled so that every array index is a constant and the
-    // intervals stay in registers; the operations and their order are as
-    // written.
+    // The axis loops are unrolled so that their array indices are constants
+    // and the intervals stay in registers; the operations and their order are
+    // as written.
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         double lo = tri[0].v[a].low, hi = tri[0].v[a].high;
