@@ -151,17 +151,20 @@ int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Win
         }
         return kOk;
     }
-    if (support) {
-        // The raster writes only inside `plan`; the clearance dilation reaches
-        // `halo` cells further.
-        for (int a = 0; a < 3; ++a) {
-            const long long h = static_cast<long long>(halo);
-            const long long lo = plan.first[a] - h - requested.first[a];
-            const long long hi = plan.first[a] + static_cast<long long>(plan.shape[a]) + h - requested.first[a];
-            const long long top = static_cast<long long>(requested.shape[a]);
+    // The raster writes only inside `plan`; the clearance dilation reaches
+    // `halo` cells further.  Outside that box the field is zero.
+    int box_lo[3], box_hi[3];
+    for (int a = 0; a < 3; ++a) {
+        const long long h = static_cast<long long>(halo);
+        const long long lo = plan.first[a] - h - requested.first[a];
+        const long long hi = plan.first[a] + static_cast<long long>(plan.shape[a]) + h - requested.first[a];
+        const long long top = static_cast<long long>(requested.shape[a]);
+        if (support) {
             support->lo[a] = static_cast<int>(std::min(std::max(lo, -1LL), top + 1));
             support->hi[a] = static_cast<int>(std::min(std::max(hi, -1LL), top + 1));
         }
+        box_lo[a] = static_cast<int>(std::min(std::max(lo, 0LL), top));
+        box_hi[a] = static_cast<int>(std::min(std::max(hi, 0LL), top));
     }
     auto* raw = static_cast<std::uint8_t*>(device_buffer(ctx, "placed.raw", cells_of(plan), status));
     if (!raw) {
@@ -172,7 +175,7 @@ int placed_field(spk_context* ctx, const geo::Prepared& prepared, const geo::Win
         return status;
     }
     return dilate_crop(ctx, raw, make_window(plan, origin, pitch), halo, clearance, false, d_out,
-                       make_window(requested, origin, pitch));
+                       make_window(requested, origin, pitch), box_lo, box_hi);
 }
 
 // voxelize_container into d_out over `requested` (device).
@@ -251,6 +254,16 @@ struct Session {
 
 Session* session_of(spk_context* ctx) { return static_cast<Session*>(ctx->session); }
 
+// The window box of a placed copy's support (its field is zero outside).
+void support_box(const Session& s, const EdtBox& support, int (&shape)[3], int (&lo)[3], int (&hi)[3])
+{
+    for (int a = 0; a < 3; ++a) {
+        shape[a] = static_cast<int>(s.env.shape[a]);
+        lo[a] = std::min(std::max(support.lo[a], 0), shape[a]);
+        hi[a] = std::min(std::max(support.hi[a], 0), shape[a]);
+    }
+}
+
 // Brings the occupancy up to date on the context's stream and queues the
 // pipeline's proximity and spectrum update on the pipeline's own stream
 // (refresh_begin), so that work that needs only the occupancy (the
@@ -262,7 +275,16 @@ int refresh_async(spk_context* ctx, Session& s)
     }
     s.pipe->refresh_order();
     const long long n = static_cast<long long>(cells_of(s.env));
-    int status = occupancy(ctx, s.mask, s.counts, s.occ, n);
+    int status = kOk;
+    if (s.one_added) {
+        // One copy added to an up-to-date occupancy: only its support changes.
+        int shape[3], lo[3], hi[3];
+        support_box(s, s.added_support, shape, lo, hi);
+        status = occupancy_box(ctx, s.mask, s.counts, s.occ, shape, lo, hi);
+    }
+    else {
+        status = occupancy(ctx, s.mask, s.counts, s.occ, n);
+    }
     if (status) {
         return status;
     }
@@ -322,6 +344,14 @@ bool rank_less(const Candidate& l, const Candidate& r)
     return std::tie(l.t[2], l.t[1], l.t[0]) < std::tie(r.t[2], r.t[1], r.t[0]);
 }
 
+// Copy counts +1 / -1 under a placed copy's field, over its support only.
+int stamp_support(spk_context* ctx, Session& s, const std::uint8_t* placed, const EdtBox& support, int direction)
+{
+    int shape[3], lo[3], hi[3];
+    support_box(s, support, shape, lo, hi);
+    return stamp_box(ctx, s.counts, placed, shape, lo, hi, direction);
+}
+
 int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const std::int64_t* t)
 {
     if (orientation >= s.catalog.size()) {
@@ -341,7 +371,7 @@ int session_place(spk_context* ctx, Session& s, std::uint64_t orientation, const
                                placed, &support, s.object_tris, s.object_vertices))) {
         return status;
     }
-    if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), 1))) {
+    if ((status = stamp_support(ctx, s, placed, support, 1))) {
         return status;
     }
     s.copies.push_back({ orientation, { t[0], t[1], t[2] } });
@@ -1078,11 +1108,12 @@ int spk_session_remove_last(spk_context* ctx)
         if (!placed) {
             return status;
         }
+        EdtBox support {};
         if ((status = placed_field(ctx, s.object, s.env, s.origin, s.pitch, translation, s.catalog[c.orientation],
-                                   s.pair, placed, nullptr, s.object_tris, s.object_vertices))) {
+                                   s.pair, placed, &support, s.object_tris, s.object_vertices))) {
             return status;
         }
-        if ((status = stamp(ctx, s.counts, placed, static_cast<long long>(cells_of(s.env)), -1))) {
+        if ((status = stamp_support(ctx, s, placed, support, -1))) {
             return status;
         }
         s.copies.pop_back();

@@ -376,15 +376,37 @@ __global__ void fill_kernel(std::uint8_t* __restrict__ cells, const int* __restr
 }
 
 // out[t] over `req` = OR over stencil deltas d of seed(raw[t - d]) inside `raw`.
+// A sub-box [lo, lo + extent) of a window (cell offsets from its first
+// cell); the box kernels visit its cells only.
+struct CellBox {
+    int lo[3];
+    int extent[3];
+};
+
+__device__ __forceinline__ long long box_cells(const CellBox& b)
+{
+    return static_cast<long long>(b.extent[0]) * b.extent[1] * b.extent[2];
+}
+
+// Offset (x, y, z) from the window's first cell of the box's cell i.
+__device__ __forceinline__ void box_cell(const CellBox& b, long long i, int (&c)[3])
+{
+    c[0] = b.lo[0] + static_cast<int>(i % b.extent[0]);
+    c[1] = b.lo[1] + static_cast<int>((i / b.extent[0]) % b.extent[1]);
+    c[2] = b.lo[2] + static_cast<int>(i / (static_cast<long long>(b.extent[0]) * b.extent[1]));
+}
+
 __global__ void dilate_kernel(const std::uint8_t* __restrict__ raw, FieldWindow rw,
                               const int* __restrict__ stencil, int stencil_count, int invert,
-                              std::uint8_t* __restrict__ out, FieldWindow req)
+                              std::uint8_t* __restrict__ out, FieldWindow req, CellBox box)
 {
-    const long long n = static_cast<long long>(req.shape[0]) * req.shape[1] * req.shape[2];
+    const long long n = box_cells(box);
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        const long long t[3] = { req.first[0] + i % req.shape[0], req.first[1] + (i / req.shape[0]) % req.shape[1],
-                                 req.first[2] + i / (static_cast<long long>(req.shape[0]) * req.shape[1]) };
+        int c[3];
+        box_cell(box, i, c);
+        const long long t[3] = { req.first[0] + c[0], req.first[1] + c[1], req.first[2] + c[2] };
+        const long long at = c[0] + static_cast<long long>(req.shape[0]) * (c[1] + static_cast<long long>(req.shape[1]) * c[2]);
         std::uint8_t value = 0;
         for (int s = 0; s < stencil_count && !value; ++s) {
             const long long sx = t[0] - stencil[3 * s] - rw.first[0];
@@ -396,7 +418,7 @@ __global__ void dilate_kernel(const std::uint8_t* __restrict__ raw, FieldWindow 
             const std::uint8_t v = raw[sx + rw.shape[0] * (sy + static_cast<long long>(rw.shape[1]) * sz)];
             value = invert ? (v != 1) : (v != 0);
         }
-        out[i] = value;
+        out[at] = value;
     }
 }
 
@@ -412,6 +434,34 @@ __global__ void box_mask_kernel(const std::uint8_t* __restrict__ ax, const std::
         const int y = static_cast<int>(r % sy);
         const int z = static_cast<int>(r / sy);
         mask[i] = (ax[x] && ay[y] && az[z]) ? 0 : 1;
+    }
+}
+
+__global__ void stamp_box_kernel(std::uint32_t* __restrict__ counts, const std::uint8_t* __restrict__ placed,
+                                 int sx, int sy, CellBox box, int direction)
+{
+    const long long n = box_cells(box);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        int c[3];
+        box_cell(box, i, c);
+        const long long at = c[0] + static_cast<long long>(sx) * (c[1] + static_cast<long long>(sy) * c[2]);
+        if (placed[at]) {
+            counts[at] += direction > 0 ? 1u : static_cast<std::uint32_t>(-1);
+        }
+    }
+}
+
+__global__ void occupancy_box_kernel(const std::uint8_t* __restrict__ mask, const std::uint32_t* __restrict__ counts,
+                                     std::uint8_t* __restrict__ occ, int sx, int sy, CellBox box)
+{
+    const long long n = box_cells(box);
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        int c[3];
+        box_cell(box, i, c);
+        const long long at = c[0] + static_cast<long long>(sx) * (c[1] + static_cast<long long>(sy) * c[2]);
+        occ[at] = (mask[at] != 0 || counts[at] != 0) ? 1 : 0;
     }
 }
 
@@ -667,7 +717,8 @@ int place_on_device(spk_context* ctx, const geo::Prepared& prepared, const doubl
 }
 
 int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,
-                double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req)
+                double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req, const int* box_lo,
+                const int* box_hi)
 {
     const auto stencil = geo::make_stencil(halo, req.pitch, clearance);
     std::vector<int> flat(3 * stencil.size());
@@ -684,9 +735,24 @@ int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& 
     }
     cudaMemcpyAsync(d_stencil, flat.data(), flat.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
     const long long n = static_cast<long long>(req.shape[0]) * req.shape[1] * req.shape[2];
-    dilate_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(d_raw, raw, d_stencil, static_cast<int>(stencil.size()),
-                                                               invert ? 1 : 0, d_out, req);
-    ctx->launches++;
+    CellBox box {};
+    for (int a = 0; a < 3; ++a) {
+        box.lo[a] = box_lo ? box_lo[a] : 0;
+        box.extent[a] = (box_hi ? box_hi[a] : req.shape[a]) - box.lo[a];
+        if (box.extent[a] <= 0) {
+            box.extent[a] = 0;
+        }
+    }
+    const long long m = static_cast<long long>(box.extent[0]) * box.extent[1] * box.extent[2];
+    if (m < n) {
+        cudaMemsetAsync(d_out, 0, n, ctx->stream);  // no stencil offset reaches the raw window from outside the box
+    }
+    if (m > 0) {
+        dilate_kernel<<<blocks_for(m, 256), 256, 0, ctx->stream>>>(d_raw, raw, d_stencil,
+                                                                   static_cast<int>(stencil.size()), invert ? 1 : 0,
+                                                                   d_out, req, box);
+        ctx->launches++;
+    }
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
@@ -727,6 +793,40 @@ int stamp(spk_context* ctx, std::uint32_t* d_counts, const std::uint8_t* d_place
 {
     stamp_kernel<<<blocks_for(n, 256), 256, 0, ctx->stream>>>(d_counts, d_placed, n, direction);
     ctx->launches++;
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int stamp_box(spk_context* ctx, std::uint32_t* d_counts, const std::uint8_t* d_placed, const int* shape,
+              const int* lo, const int* hi, int direction)
+{
+    CellBox box {};
+    for (int a = 0; a < 3; ++a) {
+        box.lo[a] = lo[a];
+        box.extent[a] = hi[a] > lo[a] ? hi[a] - lo[a] : 0;
+    }
+    const long long m = static_cast<long long>(box.extent[0]) * box.extent[1] * box.extent[2];
+    if (m > 0) {
+        stamp_box_kernel<<<blocks_for(m, 256), 256, 0, ctx->stream>>>(d_counts, d_placed, shape[0], shape[1], box,
+                                                                      direction);
+        ctx->launches++;
+    }
+    return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int occupancy_box(spk_context* ctx, const std::uint8_t* d_mask, const std::uint32_t* d_counts, std::uint8_t* d_occ,
+                  const int* shape, const int* lo, const int* hi)
+{
+    CellBox box {};
+    for (int a = 0; a < 3; ++a) {
+        box.lo[a] = lo[a];
+        box.extent[a] = hi[a] > lo[a] ? hi[a] - lo[a] : 0;
+    }
+    const long long m = static_cast<long long>(box.extent[0]) * box.extent[1] * box.extent[2];
+    if (m > 0) {
+        occupancy_box_kernel<<<blocks_for(m, 256), 256, 0, ctx->stream>>>(d_mask, d_counts, d_occ, shape[0], shape[1],
+                                                                          box);
+        ctx->launches++;
+    }
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 

@@ -49,11 +49,20 @@ int place_on_device(spk_context* ctx, const geo::Prepared& prepared, const doubl
                     const geo::Vec3& translation, const geo::Quat& q, geo::Placed& out, bool& done);
 // Clearance dilation of a raw field into the requested window.
 int dilate_crop(spk_context* ctx, const std::uint8_t* d_raw, const FieldWindow& raw, std::uint64_t halo,
-                double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req);
+                double clearance, bool invert, std::uint8_t* d_out, const FieldWindow& req,
+                const int* box_lo = nullptr, const int* box_hi = nullptr);
+// box_lo / box_hi (cell offsets in `req`, hi exclusive): the only cells the
+// dilation can set; the rest of d_out is cleared.  Null: the whole window.
 // Analytic box container blocker over window w (1 = blocked).
 int box_mask(spk_context* ctx, const double* dims, double clearance, const FieldWindow& w, std::uint8_t* d_mask);
 int stamp(spk_context* ctx, std::uint32_t* d_counts, const std::uint8_t* d_placed, long long n, int direction);
 int occupancy(spk_context* ctx, const std::uint8_t* d_mask, const std::uint32_t* d_counts, std::uint8_t* d_occ,
               long long n);
+// stamp / occupancy over the box [lo, hi) of a window of `shape` cells (the
+// cells a placed copy's field can set).
+int stamp_box(spk_context* ctx, std::uint32_t* d_counts, const std::uint8_t* d_placed, const int* shape,
+              const int* lo, const int* hi, int direction);
+int occupancy_box(spk_context* ctx, const std::uint8_t* d_mask, const std::uint32_t* d_counts, std::uint8_t* d_occ,
+                  const int* shape, const int* lo, const int* hi);
 
 }  // namespace spk
