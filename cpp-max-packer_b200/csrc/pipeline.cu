@@ -1254,6 +1254,42 @@ __global__ void merge_kernel(const unsigned long long* __restrict__ keys, long l
     }
 }
 
+// Second stage for large key ranges: request r's `lists` sorted lists of
+// `per` keys each (the first stage's chunk winners) merged into their `per`
+// smallest, ascending, by one warp-pair per request: thread c holds the head
+// of list c, and each round the smallest head (keys are distinct, empty
+// slots are kEmptyKey) is written out and its list advances.  The result is
+// the first `per` keys of the sorted union, as a full sort would give.
+__global__ void __launch_bounds__(64) merge_lists_kernel(const unsigned long long* __restrict__ partial, int lists,
+                                                        int per, unsigned long long* __restrict__ selected)
+{
+    __shared__ unsigned long long warp_min[2];
+    const int r = blockIdx.x, c = threadIdx.x, lane = c & 31, warp = c >> 5;
+    const unsigned long long* list = partial + (static_cast<long long>(r) * lists + c) * per;
+    int head = 0;
+    unsigned long long value = c < lists ? list[0] : kEmptyKey;
+    for (int i = 0; i < per; ++i) {
+        unsigned long long m = value;
+        for (int o = 16; o > 0; o >>= 1) {
+            const unsigned long long other = __shfl_xor_sync(kFull, m, o);
+            m = other < m ? other : m;
+        }
+        if (lane == 0) {
+            warp_min[warp] = m;
+        }
+        __syncthreads();
+        const unsigned long long best = warp_min[0] < warp_min[1] ? warp_min[0] : warp_min[1];
+        __syncthreads();
+        if (c == 0) {
+            selected[static_cast<long long>(r) * per + i] = best;
+        }
+        if (value == best && best != kEmptyKey) {
+            ++head;
+            value = head < per ? list[head] : kEmptyKey;
+        }
+    }
+}
+
 // First stage for large key ranges: chunk c (kKeyCapacity keys) of request r
 // keeps its smallest kExactPerOrientation + 1 keys in
 // partial[(r * chunks + c) * (kExactPerOrientation + 1) ...].
@@ -2258,16 +2294,9 @@ int Pipeline::ordinary_pages(const std::vector<PageRequest>& requests, std::vect
     cudaMemcpyAsync(jobs, host_jobs.data(), R * sizeof(ExactJob), cudaMemcpyHostToDevice, st);
     auto ev = pass_begin(ctx_);
     if (large) {
-        // The second stage sorts 64 x 65 keys padded to 8192: 64 KB of shared memory.
-        constexpr unsigned padded = 8192;
-        static_assert(kLargeKeyChunks * (kExactPerOrientation + 1) <= padded, "second merge stage exceeds its buffer");
-        static std::once_flag merge_configured[64];
-        once_per_device(merge_configured, [] {
-            cudaFuncSetAttribute(merge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, padded * 8);
-        });
         merge_chunk_kernel<<<dim3(kLargeKeyChunks, R), 1024, 0, st>>>(keys, cap, count, partial);
-        merge_kernel<<<R, 1024, padded * 8, st>>>(partial, static_cast<long long>(kLargeKeyChunks) * per, nullptr,
-                                                  kLargeKeyChunks * per, selected);
+        static_assert(kLargeKeyChunks <= 64, "merge_lists_kernel holds one list head per thread of 64");
+        merge_lists_kernel<<<R, 64, 0, st>>>(partial, kLargeKeyChunks, per, selected);
         ctx_->launches++;
     }
     else {
