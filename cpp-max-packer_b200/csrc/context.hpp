@@ -91,6 +91,22 @@ inline void* host_buffer(spk_context* ctx, const std::string& name, std::size_t 
     return p;
 }
 
+// Copies a host table into device memory and returns once the copy has
+// landed.  A plain cudaMemcpy from pageable memory may return before its DMA
+// reaches the device, and it runs on the legacy stream, which the context's
+// non-blocking streams do not wait for: a kernel launched right after it
+// could read the table half written.  Here the copy is ordered on the
+// context's stream and that stream is drained before returning.
+inline bool upload_table(spk_context* ctx, void* dst, const void* src, std::size_t bytes)
+{
+    if (cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return true;
+}
+
 // exp(-2 pi i m / L) for m < L, FP64-computed, stored as T.
 template <typename T>
 const cplx_t<T>* twiddle_table(spk_context* ctx, int L, int& status)
@@ -124,7 +140,11 @@ const cplx_t<T>* twiddle_table(spk_context* ctx, int L, int& status)
         status = kAllocation;
         return nullptr;
     }
-    cudaMemcpy(p, host.data(), sizeof(cplx_t<T>) * L, cudaMemcpyHostToDevice);
+    if (!upload_table(ctx, p, host.data(), sizeof(cplx_t<T>) * L)) {
+        cudaFree(p);
+        status = kCuda;
+        return nullptr;
+    }
     ctx->twiddles[key] = p;
     return static_cast<const cplx_t<T>*>(p);
 }

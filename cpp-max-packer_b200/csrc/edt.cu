@@ -623,7 +623,10 @@ const double* proximity_table(spk_context* ctx, std::int32_t max_d2, int& status
     if (!d) {
         return nullptr;
     }
-    cudaMemcpy(d, host.data(), want * sizeof(double), cudaMemcpyHostToDevice);
+    if (!upload_table(ctx, d, host.data(), want * sizeof(double))) {
+        status = kCuda;
+        return nullptr;
+    }
     return d;
 }
 
