@@ -287,30 +287,38 @@ def run_ours(args, rank, world, local_rank):
         return
 
     # Roofline of the page passes, timed with events on the context stream
-    # around each launch during two further exhaustive steps; the bench line's
-    # roofline is the pass with the largest share of that time.
-    lib.spk_context_set_profiling(ctx.handle, 1)
-    session.greedy(2)
-    launches_arr = np.zeros(4, np.uint64)
-    total_ms = np.zeros(4, np.float64)
-    lib.spk_context_pass_times(ctx.handle, launches_arr.ctypes.data, total_ms.ctypes.data, 4)
-    pass_bytes = np.zeros(4, np.float64)
-    lib.spk_context_pass_bytes(ctx.handle, pass_bytes.ctypes.data, 4)
-    lib.spk_context_set_profiling(ctx.handle, 0)
+    # around each launch: during six further steps of the headline path (the
+    # learned steps when the proposal is on), and during two further
+    # exhaustive steps.  The bench line's roofline is the pass with the
+    # largest share of the headline path's time.
     hbm, peak_kind = peaks()
     full256 = tuple(session.fft_shape) == (256, 256, 256)
-    passes = []
-    for i, (kernel, what) in enumerate(PASSES):
-        n = max(int(launches_arr[i]), 1)
-        avg_ms = total_ms[i] / n
-        per_launch = pass_bytes[i] / n
-        achieved_i = per_launch / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 and per_launch > 0 else None
-        passes.append({"kernel": kernel, "work": what, "launches": int(launches_arr[i]),
-                       "share": round(float(total_ms[i] / max(total_ms.sum(), 1e-9)), 3),
-                       "avg_launch_ms": round(avg_ms, 5), "algorithmic_bytes_per_launch": int(per_launch),
-                       "achieved_gbs": round(achieved_i, 1) if achieved_i else None,
-                       "frac": round(achieved_i / hbm, 4) if achieved_i else None,
-                       "traffic": NCU_DRAM_BYTES.get(kernel) if full256 else None})
+
+    def profile_passes(run_steps):
+        lib.spk_context_set_profiling(ctx.handle, 1)
+        run_steps()
+        launches_arr = np.zeros(4, np.uint64)
+        total_ms = np.zeros(4, np.float64)
+        lib.spk_context_pass_times(ctx.handle, launches_arr.ctypes.data, total_ms.ctypes.data, 4)
+        pass_bytes = np.zeros(4, np.float64)
+        lib.spk_context_pass_bytes(ctx.handle, pass_bytes.ctypes.data, 4)
+        lib.spk_context_set_profiling(ctx.handle, 0)
+        out = []
+        for i, (kernel, what) in enumerate(PASSES):
+            n = max(int(launches_arr[i]), 1)
+            avg_ms = total_ms[i] / n
+            per_launch = pass_bytes[i] / n
+            achieved_i = per_launch / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 and per_launch > 0 else None
+            out.append({"kernel": kernel, "work": what, "launches": int(launches_arr[i]),
+                        "share": round(float(total_ms[i] / max(total_ms.sum(), 1e-9)), 3),
+                        "avg_launch_ms": round(avg_ms, 5), "algorithmic_bytes_per_launch": int(per_launch),
+                        "achieved_gbs": round(achieved_i, 1) if achieved_i else None,
+                        "frac": round(achieved_i / hbm, 4) if achieved_i else None,
+                        "traffic": NCU_DRAM_BYTES.get(kernel) if full256 else None})
+        return out
+
+    passes_exhaustive = profile_passes(lambda: session.greedy(2))
+    passes = profile_passes(lambda: proposal.greedy_proposed(session, net, k, 6)) if learned else passes_exhaustive
     dominant = max(passes[:3], key=lambda p: p["share"])
 
     # End to end through the public API with host buffers: the proposal
@@ -385,7 +393,8 @@ def run_ours(args, rank, world, local_rank):
                          "unit": "GB/s", "frac": dominant["frac"], "traffic": dominant["traffic"],
                          "algorithmic_bytes_per_launch": dominant["algorithmic_bytes_per_launch"],
                          "avg_launch_ms": dominant["avg_launch_ms"], "share": dominant["share"],
-                         "passes": passes},
+                         "passes": passes, "passes_measured_on": "learned steps" if learned else "exhaustive steps",
+                         "passes_exhaustive": passes_exhaustive},
             "e2e": e2e,
             "clocks": clocks.summary(),
             "validator_broad_phase": broad,

@@ -6,7 +6,10 @@
 --configs runs one exhaustive fill and then a learned fill per entry: "k"
 pages the k proposed orientations, "k:m" also widens by k at a time while
 fewer than m paged orientations admit a copy
-(spk_session_greedy_proposed_adaptive).
+(spk_session_greedy_proposed_adaptive), "m:k_min:k_max:margin" pages every
+orientation predicted within the margin of the k_min-th best, and
+"s:k:n:k2" pages k proposed orientations for the first n copies and k2
+after them (k2 = 0: the exhaustive step).
 
 Both fills start from the empty container and run until no orientation
 admits a copy.
@@ -90,8 +93,11 @@ def main():
         "learned": [],
     }
     for config in configs:
-        margin = None
-        if config.startswith("m:"):
+        margin, switch_at, k_late = None, None, None
+        if config.startswith("s:"):
+            _, k, switch_at, k_late = config.split(":")
+            k, m, switch_at, k_late = int(k), 0, int(switch_at), int(k_late)
+        elif config.startswith("m:"):
             _, k_min, k_max, margin = config.split(":")
             k, m, k_max, margin = int(k_min), 0, int(k_max), float(margin)
         else:
@@ -102,6 +108,22 @@ def main():
         widened = [0]
 
         def learned(n):
+            if switch_at is not None:
+                total, fallbacks = 0, 0
+                while total < n:
+                    done = len(s.placements)
+                    want = min(n - total, switch_at - done) if done < switch_at else n - total
+                    if done < switch_at:
+                        placed, fb = proposal.greedy_proposed(s, net, k, want)
+                    elif k_late == 0:
+                        placed, fb = s.greedy(want), 0
+                    else:
+                        placed, fb = proposal.greedy_proposed(s, net, k_late, want)
+                    total += len(placed)
+                    fallbacks += fb
+                    if len(placed) < want:
+                        break
+                return total, fallbacks
             if margin is not None:
                 placed, fb, paged = proposal.greedy_proposed_margin(s, net, k, k_max, margin, n)
                 widened[0] += paged
@@ -117,6 +139,7 @@ def main():
         s.close()
         entry = {"k": k, "min_feasible": m, "copies": ln[0], "fallback_steps": ln[1], "widenings": widened[0],
                  "margin": margin, "k_max": k_max if margin is not None else None,
+                 "switch_at": switch_at, "k_late": k_late,
                  "mean_paged": round(widened[0] / max(ln[0], 1), 2) if margin is not None else None,
                  "seconds": round(ln[2], 2), "placements_per_s": round(ln[0] / ln[2], 3),
                  "packed_count_ratio": round(ln[0] / ex[0], 4) if ex[0] else None,
