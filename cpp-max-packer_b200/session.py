@@ -21,7 +21,7 @@ from . import _lib
 from .assets import AcceptedMesh
 from .compute import Context, default_context
 from .geometry import MeshC, _lib_ready
-from .pipeline import PAGE_SIZE, CandidateC, PageQueryC, PageReportC, RankedCandidate
+from .pipeline import PAGE_SIZE, CandidateC, PageQueryC, PageReportC, RankedCandidate, candidates_from_c
 
 P = ctypes.c_void_p
 POSE_ACCEPTED, POSE_REJECTED = 0, 1
@@ -151,7 +151,7 @@ class Session:
             reports.extend(dict(max_integer_residual=r.max_integer_residual, max_score_error=r.max_score_error,
                                 rescored=r.rescored, certified=bool(r.certified),
                                 threshold_pass=bool(r.threshold_pass)) for r in reps)
-        return [[RankedCandidate.from_c(pages[i * PAGE_SIZE + k]) for k in range(int(counts[i]))] for i in range(n)]
+        return candidates_from_c(pages, counts.tolist(), PAGE_SIZE)
 
     def greedy(self, max_steps: int) -> List[Placement]:
         ori = np.zeros(max(max_steps, 1), np.uint64)

@@ -68,3 +68,28 @@ def test_policy_layouts_merge_with_reindexed_crops():
     assert merged.sample_item.tolist() == [2, 0, 3, 4]
     assert np.allclose(merged.sample_label, [0.1, 0.2, 0.3, 0.4])
     assert train.merge_datasets(base, [], [], [], [], []) is base
+
+
+def test_page_arrays_convert_like_the_per_element_reader():
+    # candidates_from_c reads a CandidateC array column by column; it must
+    # give the values, types and hashes of RankedCandidate.from_c.
+    pipeline = package("pipeline")
+    rng = np.random.default_rng(5)
+    pages = (pipeline.CandidateC * (8 * pipeline.PAGE_SIZE))()
+    for c in pages:
+        for a in range(3):
+            c.translation[a] = int(rng.integers(-2**40, 2**40))
+        c.score = float(rng.normal())
+        c.direct_zero_overlap = int(rng.integers(0, 2))
+        c.orientation_index = int(rng.integers(0, 2**63))
+        c.binary_overlap = float(rng.integers(0, 100))
+    counts = [0, 1, 32, 17, 5, 32, 2, 9]
+    want = [[pipeline.RankedCandidate.from_c(pages[i * pipeline.PAGE_SIZE + k]) for k in range(n)]
+            for i, n in enumerate(counts)]
+    got = pipeline.candidates_from_c(pages, counts, pipeline.PAGE_SIZE)
+    assert got == want
+    for page_got, page_want in zip(got, want):
+        for a, b in zip(page_got, page_want):
+            assert hash(a) == hash(b)
+            assert type(a.translation[0]) is int and type(a.score) is float
+            assert type(a.direct_zero_overlap) is bool and type(a.orientation_index) is int
