@@ -409,29 +409,31 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
 }
 
 // Pass A over a batch of orientations on 256^3 grids: the environment
-// spectrum column is read once per block and kept in registers while each
-// orientation of the batch finishes its kernel column, multiplies and
-// inverts along z.  The spectrum (134 MB at 256^3) then crosses HBM once per
+// spectrum column is read once per block and kept in shared memory (32 KB,
+// [k2][thread]) while each orientation of the batch finishes its kernel
+// column, multiplies and inverts along z.  Out of registers, it leaves the
+// kernel at 80 registers: three blocks per SM instead of two.  The spectrum (134 MB at 256^3) then crosses HBM once per
 // batch instead of once per orientation.  The next orientation's kernel
 // planes are fetched before the current one's transforms.
-__global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
+constexpr std::size_t kPassASmem = sizeof(float2) * 16 * 256;
+__global__ void __launch_bounds__(256, 3) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
                                                              const PassABatch batch,
                                                              const float2* __restrict__ twiddles)
 {
     __shared__ RegTwiddles tw;
     __shared__ float2 lines[16 * kRegLine];
+    extern __shared__ float2 sp_s[];  // [k2][threadIdx.x]
     load_twiddles(tw, twiddles);
-    __syncthreads();
     const int j = threadIdx.x & 15;  // column within the group (coalesced direction)
     const int t = threadIdx.x >> 4;  // lane within the line
     const int ky = blockIdx.x >> 4;
     const long long col = ((blockIdx.x & 15) << 4) + j + 256LL * ky;
     const long long plane = 65536;
-    float2 sp[16];
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) {
-        sp[k2] = __ldcs(spectrum + col + plane * (t + 16 * k2));
+        sp_s[k2 * 256 + threadIdx.x] = __ldcs(spectrum + col + plane * (t + 16 * k2));
     }
+    __syncthreads();
     float2* line = lines + j * kRegLine;
     // Kernel planes z = t and z = 16 + t of the next orientation (almost
     // every kernel has K2 <= 32; deeper planes are read in the loop).
@@ -466,7 +468,7 @@ __global__ void __launch_bounds__(256) pass_a256_batch_kernel(const float2* __re
         }
 #pragma unroll
         for (int k2 = 0; k2 < 16; ++k2) {
-            const float2 sv = sp[k2];
+            const float2 sv = sp_s[k2 * 256 + threadIdx.x];
             v[k2] = make_float2(sv.x * v[k2].x + sv.y * v[k2].y, sv.y * v[k2].x - sv.x * v[k2].y);
         }
         fft256<true>(v, line, t, tw);  // v[m2] = w(z = t + 16 m2)
@@ -1955,7 +1957,12 @@ int Pipeline::run_a256_batch(const KernelSlot* const* slots, int count, float2* 
         bytes += pass_a_bytes(*slots[i]) - spectrum_bytes;
     }
     auto ev = pass_begin(ctx_);
-    pass_a256_batch_kernel<<<16 * 256, 256, 0, ctx_->stream>>>(spectrum_, batch, tw2);
+    static std::once_flag a_configured[64];
+    once_per_device(a_configured, [] {
+        cudaFuncSetAttribute(pass_a256_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kPassASmem));
+    });
+    pass_a256_batch_kernel<<<16 * 256, 256, kPassASmem, ctx_->stream>>>(spectrum_, batch, tw2);
     pass_end(ctx_, 0, ev, bytes);
     ctx_->launches++;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
