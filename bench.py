@@ -42,15 +42,17 @@ PASSES = [
     ("pass_b2_256_batch_kernel", "inverse x with the fused threshold / score / top-k epilogue, a batch of "
                                  "orientations per launch"),
     ("merge_kernel + exact_kernel", "key merge and exact recount"),
+    ("pass_stage256_kernel", "pipelined stage: pass A of one batch of 16 orientations with B1 and B2 of the two "
+                             "batches before it, their blocks interleaved in one launch"),
 ]
 # DRAM read + write bytes per launch of each kernel on the 256^3 workload,
 # from the ncu capture summarised in profiles/page_passes_rounded256_o16.md
 # (dram__bytes.sum.per_second x duration; each launch there does the same
 # work as in the 512-orientation workload).
 NCU_DRAM_BYTES = {
-    "pass_a256_batch_kernel": 2231803888,
-    "pass_b1_256_batch_kernel": 3796430981,
-    "pass_b2_256_batch_kernel": 1862089123,
+    "pass_a256_batch_kernel": 2231207392,
+    "pass_b1_256_batch_kernel": 3797132958,
+    "pass_b2_256_batch_kernel": 1862176554,
 }
 DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cpp-max-packer_b200", "weights",
                                "proposal_rounded256.npz")
@@ -297,11 +299,11 @@ def run_ours(args, rank, world, local_rank):
     def profile_passes(run_steps):
         lib.spk_context_set_profiling(ctx.handle, 1)
         run_steps()
-        launches_arr = np.zeros(4, np.uint64)
-        total_ms = np.zeros(4, np.float64)
-        lib.spk_context_pass_times(ctx.handle, launches_arr.ctypes.data, total_ms.ctypes.data, 4)
-        pass_bytes = np.zeros(4, np.float64)
-        lib.spk_context_pass_bytes(ctx.handle, pass_bytes.ctypes.data, 4)
+        launches_arr = np.zeros(len(PASSES), np.uint64)
+        total_ms = np.zeros(len(PASSES), np.float64)
+        lib.spk_context_pass_times(ctx.handle, launches_arr.ctypes.data, total_ms.ctypes.data, len(PASSES))
+        pass_bytes = np.zeros(len(PASSES), np.float64)
+        lib.spk_context_pass_bytes(ctx.handle, pass_bytes.ctypes.data, len(PASSES))
         lib.spk_context_set_profiling(ctx.handle, 0)
         out = []
         for i, (kernel, what) in enumerate(PASSES):
@@ -319,7 +321,8 @@ def run_ours(args, rank, world, local_rank):
 
     passes_exhaustive = profile_passes(lambda: session.greedy(2))
     passes = profile_passes(lambda: proposal.greedy_proposed(session, net, k, 6)) if learned else passes_exhaustive
-    dominant = max(passes[:3], key=lambda p: p["share"])
+    # The candidates for the roofline: every pass but the merge and recount.
+    dominant = max((p for i, p in enumerate(passes) if i != 3 and p["launches"]), key=lambda p: p["share"])
 
     # End to end through the public API with host buffers: the proposal
     # (predictions out), page queries in, pages out, the chosen copy placed.

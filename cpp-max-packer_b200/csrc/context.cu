@@ -71,7 +71,7 @@ int spk_context_set_profiling(spk_context* ctx, int enabled)
     }
     spk::pass_collect(ctx);
     ctx->profiling = enabled != 0;
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < spk_context::kPasses; ++i) {
         ctx->pass_launches[i] = 0;
         ctx->pass_ms[i] = 0;
         ctx->pass_bytes[i] = 0;
@@ -84,7 +84,7 @@ int spk_context_pass_bytes(const spk_context* ctx, double* bytes, uint32_t capac
     if (!ctx || !bytes) {
         return spk::kInvalidArgument;
     }
-    for (uint32_t i = 0; i < capacity && i < 4; ++i) {
+    for (uint32_t i = 0; i < capacity && i < static_cast<uint32_t>(spk_context::kPasses); ++i) {
         bytes[i] = ctx->pass_bytes[i];
     }
     return spk::kOk;
@@ -96,7 +96,7 @@ int spk_context_pass_times(const spk_context* ctx, uint64_t* launches, double* t
         return spk::kInvalidArgument;
     }
     spk::pass_collect(const_cast<spk_context*>(ctx));
-    for (uint32_t i = 0; i < capacity && i < 4; ++i) {
+    for (uint32_t i = 0; i < capacity && i < static_cast<uint32_t>(spk_context::kPasses); ++i) {
         launches[i] = ctx->pass_launches[i];
         total_ms[i] = ctx->pass_ms[i];
     }

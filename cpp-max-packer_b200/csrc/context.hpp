@@ -32,9 +32,10 @@ struct spk_context {
     std::map<std::pair<int, int>, void*> twiddles;  // (sizeof scalar, L) -> table
     void* session {};                              // placement session (engine.cpp)
     bool profiling {};
-    std::uint64_t pass_launches[4] {};
-    double pass_ms[4] {};
-    double pass_bytes[4] {};  // algorithmic bytes of the profiled launches
+    static constexpr int kPasses = 5;  // A, B1, B2, merge + exact, the pipelined A/B1/B2 stage
+    std::uint64_t pass_launches[kPasses] {};
+    double pass_ms[kPasses] {};
+    double pass_bytes[kPasses] {};  // algorithmic bytes of the profiled launches
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> pending;  // (pass, events)
     const char* message { "" };  // static text of the last correlation failure on this context
 };

@@ -411,23 +411,23 @@ __global__ void __launch_bounds__(256) pass_a256_kernel(const float2* __restrict
 // Pass A over a batch of orientations on 256^3 grids: the environment
 // spectrum column is read once per block and kept in shared memory (32 KB,
 // [k2][thread]) while each orientation of the batch finishes its kernel
-// column, multiplies and inverts along z.  Out of registers, it leaves the
-// kernel at 80 registers: three blocks per SM instead of two.  The spectrum (134 MB at 256^3) then crosses HBM once per
-// batch instead of once per orientation.  The next orientation's kernel
-// planes are fetched before the current one's transforms.
+// column, multiplies and inverts along z.  The spectrum (134 MB at 256^3)
+// then crosses HBM once per batch instead of once per orientation.  Held in
+// shared memory rather than registers, it leaves the kernel at 80
+// registers: three blocks per SM instead of two.  The next orientation's
+// kernel planes are fetched before the current one's transforms.
 constexpr std::size_t kPassASmem = sizeof(float2) * 16 * 256;
-__global__ void __launch_bounds__(256, 3) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
-                                                             const PassABatch batch,
-                                                             const float2* __restrict__ twiddles)
+
+// Block `block` of a batched pass A; `sp_s` is kPassASmem bytes of shared
+// memory.  The caller has loaded `tw` (no barrier needed after it: the
+// spectrum staging below ends with one).
+__device__ __forceinline__ void a_block256(const float2* __restrict__ spectrum, const PassABatch& batch,
+                                           const RegTwiddles& tw, float2* lines, float2* sp_s, unsigned int block)
 {
-    __shared__ RegTwiddles tw;
-    __shared__ float2 lines[16 * kRegLine];
-    extern __shared__ float2 sp_s[];  // [k2][threadIdx.x]
-    load_twiddles(tw, twiddles);
     const int j = threadIdx.x & 15;  // column within the group (coalesced direction)
     const int t = threadIdx.x >> 4;  // lane within the line
-    const int ky = blockIdx.x >> 4;
-    const long long col = ((blockIdx.x & 15) << 4) + j + 256LL * ky;
+    const int ky = static_cast<int>(block >> 4);
+    const long long col = ((block & 15) << 4) + j + 256LL * ky;
     const long long plane = 65536;
 #pragma unroll
     for (int k2 = 0; k2 < 16; ++k2) {
@@ -480,6 +480,17 @@ __global__ void __launch_bounds__(256, 3) pass_a256_batch_kernel(const float2* _
             }
         }
     }
+}
+
+__global__ void __launch_bounds__(256, 3) pass_a256_batch_kernel(const float2* __restrict__ spectrum,
+                                                                const PassABatch batch,
+                                                                const float2* __restrict__ twiddles)
+{
+    __shared__ RegTwiddles tw;
+    __shared__ float2 lines[16 * kRegLine];
+    extern __shared__ float2 sp_s[];  // [k2][threadIdx.x]
+    load_twiddles(tw, twiddles);
+    a_block256(spectrum, batch, tw, lines, sp_s, blockIdx.x);
 }
 
 // Environment spectrum on 256^3 grids, register four-step FFTs (see
@@ -593,10 +604,10 @@ __global__ void __launch_bounds__(256) pass_b1_256_kernel(float2* __restrict__ i
 }
 
 // Slot of a batched launch that owns this block.
-__device__ __forceinline__ int batch_slot(const PassBBatch& b)
+__device__ __forceinline__ int batch_slot(const PassBBatch& b, unsigned int block)
 {
     int g = 0;
-    while (g + 1 < b.count && b.slot[g + 1].first_block <= static_cast<int>(blockIdx.x)) {
+    while (g + 1 < b.count && b.slot[g + 1].first_block <= static_cast<int>(block)) {
         ++g;
     }
     return g;
@@ -609,7 +620,7 @@ __global__ void __launch_bounds__(256) pass_b1_256_batch_kernel(const __grid_con
     __shared__ float2 lines[16 * kRegLine];
     load_twiddles(tw, twiddles);
     __syncthreads();
-    const int g = batch_slot(b);
+    const int g = batch_slot(b, blockIdx.x);
     b1_block256(b.slot[g].inter, b.slot[g].legal_y, tw, lines, blockIdx.x - b.slot[g].first_block);
 }
 
@@ -1134,11 +1145,66 @@ __global__ void __launch_bounds__(256) pass_b2_256_batch_kernel(const __grid_con
     __shared__ B2Shared sh;
     load_twiddles(tw, twiddles);
     __syncthreads();
-    const PassBSlot& s = b.slot[batch_slot(b)];
+    const PassBSlot& s = b.slot[batch_slot(b, blockIdx.x)];
     b2_block256(s.inter, s.legal_x, s.legal_y, s.legal_z, tw, lines, sh, s.t65, s.inv_occ, 0, s.target, 0.0,
                 s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid,
                 blockIdx.x - static_cast<unsigned int>(s.first_block));
 }
+
+// One stage of the software-pipelined page passes on 256^3 grids: pass A of
+// batch k, pass B1 of batch k - 1 and pass B2 of batch k - 2 in one launch,
+// each batch on its own intermediate (three in rotation).  Pass B1 streams
+// HBM at the copy peak while passes A and B2 are bound by instruction issue;
+// run as separate launches, each leaves the other resource idle.  Here the
+// three roles' blocks are interleaved through the grid in proportion to
+// their counts (block b takes role A when floor((b + 1) nA / n) passes an
+// integer, and the rest split the same way between B1 and B2), so every SM
+// holds a mix of them throughout the launch.  Each block runs the same code
+// as the corresponding block of the separate kernels.
+//
+// Measured slower than the separate launches (1.16 ms per stage launch; a
+// 32-orientation step's passes took 4.6 ms against 3.7 ms), so it runs only
+// under SPK_PAGE_SCHEDULE=staged: with three blocks per SM for every role,
+// the B1 blocks on an SM keep too few loads in flight to stream HBM, and
+// the long pass A blocks dispatched last leave a tail.
+struct PassStage {
+    const float2* spectrum;
+    PassABatch a;
+    PassBBatch b1, b2;
+    unsigned int blocks_a, blocks_b1;
+};
+
+__global__ void __launch_bounds__(256, 3) pass_stage256_kernel(const __grid_constant__ PassStage p,
+                                                              const float2* __restrict__ twiddles)
+{
+    __shared__ RegTwiddles tw;
+    __shared__ float2 lines[16 * kRegLine];
+    // Pass A: the spectrum column (kPassASmem bytes); pass B2: its B2Shared.
+    extern __shared__ __align__(16) unsigned char stage_smem[];
+    load_twiddles(tw, twiddles);
+    const unsigned long long b = blockIdx.x, n = gridDim.x;
+    const unsigned long long a_before = b * p.blocks_a / n, a_upto = (b + 1) * p.blocks_a / n;
+    if (a_upto > a_before) {
+        a_block256(p.spectrum, p.a, tw, lines, reinterpret_cast<float2*>(stage_smem),
+                   static_cast<unsigned int>(a_before));
+        return;
+    }
+    __syncthreads();
+    const unsigned long long q = b - a_before, m = n - p.blocks_a;
+    const unsigned long long b1_before = q * p.blocks_b1 / m, b1_upto = (q + 1) * p.blocks_b1 / m;
+    if (b1_upto > b1_before) {
+        const unsigned int block = static_cast<unsigned int>(b1_before);
+        const PassBSlot& s = p.b1.slot[batch_slot(p.b1, block)];
+        b1_block256(s.inter, s.legal_y, tw, lines, block - static_cast<unsigned int>(s.first_block));
+        return;
+    }
+    const unsigned int block = static_cast<unsigned int>(q - b1_before);
+    const PassBSlot& s = p.b2.slot[batch_slot(p.b2, block)];
+    b2_block256(s.inter, s.legal_x, s.legal_y, s.legal_z, tw, lines, *reinterpret_cast<B2Shared*>(stage_smem), s.t65,
+                s.inv_occ, 0, s.target, 0.0, s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid,
+                block - static_cast<unsigned int>(s.first_block));
+}
+static_assert(sizeof(B2Shared) <= kPassASmem, "pass B2's shared state must fit the stage kernel's dynamic buffer");
 
 // Passes B1 and B2 fused on 256^3 grids: one cluster of 8 CTAs per legal z
 // plane.  CTA c inverts along y the 32 columns kx = 32c..32c+31 of the plane
@@ -1422,6 +1488,8 @@ Pipeline::Pipeline(spk_context* ctx) : ctx_(ctx)
 {
     const char* mode = std::getenv("SPK_PASS_B");
     fused_b_ = mode && std::strcmp(mode, "fused") == 0;
+    const char* schedule = std::getenv("SPK_PAGE_SCHEDULE");
+    staged_ = schedule && std::strcmp(schedule, "staged") == 0;
 }
 
 Pipeline::~Pipeline()
@@ -1941,6 +2009,50 @@ double Pipeline::pass_a_bytes(const KernelSlot& s) const
     return plane * L_[2] + plane * (s.K[2] + s.legal[2]);
 }
 
+double Pipeline::fill_a256(const KernelSlot* const* slots, int count, float2* const* inter, PassABatch& batch) const
+{
+    batch = {};
+    batch.count = count;
+    const double spectrum_bytes = static_cast<double>(L_[0]) * L_[1] * L_[2] * sizeof(float2);
+    double bytes = spectrum_bytes;
+    for (int i = 0; i < count; ++i) {
+        batch.slot[i] = { slots[i]->partial, inter[i], slots[i]->K[2], slots[i]->legal[2] };
+        bytes += pass_a_bytes(*slots[i]) - spectrum_bytes;
+    }
+    return bytes;
+}
+
+void Pipeline::fill_b256(const KernelSlot* const* slots, int count, float2* const* inter, const PassBSlot* outputs,
+                         PassBBatch& b1, PassBBatch& b2, int& blocks1, int& blocks2, double& bytes1,
+                         double& bytes2) const
+{
+    b1 = {};
+    b2 = {};
+    b1.count = b2.count = count;
+    blocks1 = blocks2 = 0;
+    bytes1 = bytes2 = 0.0;
+    for (int g = 0; g < count; ++g) {
+        const KernelSlot& s = *slots[g];
+        PassBSlot slot = outputs[g];
+        slot.inter = inter[g];
+        slot.t65 = s.t65;
+        slot.inv_occ = 1.0 / static_cast<double>(s.occupied);
+        slot.legal_x = s.legal[0];
+        slot.legal_y = s.legal[1];
+        slot.legal_z = s.legal[2];
+        slot.first_block = blocks1;
+        b1.slot[g] = slot;
+        blocks1 += 16 * s.legal[2];
+        slot.first_block = blocks2;
+        b2.slot[g] = slot;
+        const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
+        blocks2 += static_cast<int>((rows + 15) / 16);
+        const double legal_rows = static_cast<double>(rows);
+        bytes1 += 8.0 * L_[0] * L_[1] * s.legal[2] + 8.0 * L_[0] * legal_rows;
+        bytes2 += 8.0 * L_[0] * legal_rows;
+    }
+}
+
 int Pipeline::run_a256_batch(const KernelSlot* const* slots, int count, float2* const* inter)
 {
     int status = kOk;
@@ -1949,13 +2061,7 @@ int Pipeline::run_a256_batch(const KernelSlot* const* slots, int count, float2* 
         return status;
     }
     PassABatch batch {};
-    batch.count = count;
-    const double spectrum_bytes = static_cast<double>(L_[0]) * L_[1] * L_[2] * sizeof(float2);
-    double bytes = spectrum_bytes;
-    for (int i = 0; i < count; ++i) {
-        batch.slot[i] = { slots[i]->partial, inter[i], slots[i]->K[2], slots[i]->legal[2] };
-        bytes += pass_a_bytes(*slots[i]) - spectrum_bytes;
-    }
+    const double bytes = fill_a256(slots, count, inter, batch);
     auto ev = pass_begin(ctx_);
     static std::once_flag a_configured[64];
     once_per_device(a_configured, [] {
@@ -1979,29 +2085,9 @@ int Pipeline::run_b256_batch(const KernelSlot* const* slots, int count, float2* 
         return status;
     }
     PassBBatch b1 {}, b2 {};
-    b1.count = b2.count = count;
     int blocks1 = 0, blocks2 = 0;
     double bytes1 = 0.0, bytes2 = 0.0;
-    for (int g = 0; g < count; ++g) {
-        const KernelSlot& s = *slots[g];
-        PassBSlot slot = outputs[g];
-        slot.inter = inter[g];
-        slot.t65 = s.t65;
-        slot.inv_occ = 1.0 / static_cast<double>(s.occupied);
-        slot.legal_x = s.legal[0];
-        slot.legal_y = s.legal[1];
-        slot.legal_z = s.legal[2];
-        slot.first_block = blocks1;
-        b1.slot[g] = slot;
-        blocks1 += 16 * s.legal[2];
-        slot.first_block = blocks2;
-        b2.slot[g] = slot;
-        const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
-        blocks2 += static_cast<int>((rows + 15) / 16);
-        const double legal_rows = static_cast<double>(rows);
-        bytes1 += 8.0 * L_[0] * L_[1] * s.legal[2] + 8.0 * L_[0] * legal_rows;
-        bytes2 += 8.0 * L_[0] * legal_rows;
-    }
+    fill_b256(slots, count, inter, outputs, b1, b2, blocks1, blocks2, bytes1, bytes2);
     auto ev = pass_begin(ctx_);
     pass_b1_256_batch_kernel<<<blocks1, 256, 0, st>>>(b1, tw1);
     pass_end(ctx_, 1, ev, bytes1);
@@ -2010,6 +2096,72 @@ int Pipeline::run_b256_batch(const KernelSlot* const* slots, int count, float2* 
     pass_end(ctx_, 2, ev, bytes2);
     ctx_->launches += 2;
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
+}
+
+int Pipeline::run_stages256(const std::vector<StageBatch>& batches, float2* const* inter, std::size_t stride)
+{
+    int status = kOk;
+    const auto* tw = twiddle_table<float>(ctx_, 256, status);
+    if (!tw) {
+        return status;
+    }
+    static std::once_flag configured[64];
+    once_per_device(configured, [] {
+        cudaFuncSetAttribute(pass_stage256_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kPassASmem));
+    });
+    const std::size_t nb = batches.size();
+    // Intermediates of batch k: inter[k % 3] + g * stride for its orientation g.
+    auto outs_of = [&](std::size_t k, float2** outs) {
+        for (int g = 0; g < batches[k].count; ++g) {
+            outs[g] = inter[k % 3] + g * stride;
+        }
+    };
+    for (std::size_t stage = 0; stage < nb + 2; ++stage) {
+        PassStage p {};
+        p.spectrum = spectrum_;
+        double bytes = 0.0;
+        int blocks_b1 = 0, blocks_b2 = 0;
+        float2* outs[kPassABatch];
+        if (stage < nb) {
+            outs_of(stage, outs);
+            bytes += fill_a256(batches[stage].slots, batches[stage].count, outs, p.a);
+            p.blocks_a = 16 * 256;
+        }
+        if (stage >= 1 && stage - 1 < nb) {
+            const StageBatch& sb = batches[stage - 1];
+            PassBBatch unused {};
+            int unused_blocks = 0;
+            double b1_bytes = 0.0, unused_bytes = 0.0;
+            outs_of(stage - 1, outs);
+            fill_b256(sb.slots, sb.count, outs, sb.outputs, p.b1, unused, blocks_b1, unused_blocks, b1_bytes,
+                      unused_bytes);
+            bytes += b1_bytes;
+        }
+        if (stage >= 2) {
+            const StageBatch& sb = batches[stage - 2];
+            PassBBatch unused {};
+            int unused_blocks = 0;
+            double b2_bytes = 0.0, unused_bytes = 0.0;
+            outs_of(stage - 2, outs);
+            fill_b256(sb.slots, sb.count, outs, sb.outputs, unused, p.b2, unused_blocks, blocks_b2, unused_bytes,
+                      b2_bytes);
+            bytes += b2_bytes;
+        }
+        p.blocks_b1 = static_cast<unsigned int>(blocks_b1);
+        const unsigned int blocks = p.blocks_a + p.blocks_b1 + static_cast<unsigned int>(blocks_b2);
+        if (!blocks) {
+            continue;
+        }
+        auto ev = pass_begin(ctx_);
+        pass_stage256_kernel<<<blocks, 256, kPassASmem, ctx_->stream>>>(p, tw);
+        pass_end(ctx_, 4, ev, bytes);
+        ctx_->launches++;
+        if (cudaGetLastError() != cudaSuccess) {
+            return kCuda;
+        }
+    }
+    return kOk;
 }
 
 int Pipeline::run_b256(const KernelSlot& s, float2* inter, int mode, float target, double threshold, double cursor_floor,
@@ -2239,11 +2391,49 @@ int Pipeline::ordinary_pages(const std::vector<PageRequest>& requests, std::vect
         floor[r] = requests[r].has_cursor ? requests[r].cursor.score - eps_s[r] : -INFINITY;
         runnable.push_back(r);
     }
-    if (large) {
+    // The pipelined schedule holds up to three batches' intermediates at once;
+    // where the device memory cap does not allow that, the passes run one
+    // launch each on one batch's intermediate.
+    const std::size_t stride = static_cast<std::size_t>(L_[0]) * L_[1] * L_[2];
+    const std::size_t batch_size = std::min<std::size_t>(kPassABatch, runnable.size());
+    const std::size_t batches = (runnable.size() + kPassABatch - 1) / kPassABatch;
+    float2* staged_inter = nullptr;
+    const std::size_t copies = std::min<std::size_t>(batches, 3);
+    if (large && staged_ && !fused_b_ && batches) {
+        int alloc_status = kOk;
+        staged_inter = static_cast<float2*>(device_buffer(
+            ctx_, "pipe.inter_batch", copies * batch_size * stride * sizeof(float2), alloc_status));
+    }
+    if (staged_inter) {
+        std::vector<StageBatch> work(batches);
+        for (std::size_t k = 0; k < work.size(); ++k) {
+            StageBatch& sb = work[k];
+            sb = {};
+            sb.count = static_cast<int>(std::min<std::size_t>(kPassABatch, runnable.size() - k * kPassABatch));
+            for (int g = 0; g < sb.count; ++g) {
+                const int r = runnable[k * kPassABatch + g];
+                sb.slots[g] = &slots_[requests[r].slot];
+                PassBSlot& t = sb.outputs[g];
+                t.keys = keys + static_cast<long long>(r) * cap;
+                t.count = count + r;
+                t.cap = cap;
+                t.tau = tau + r;
+                t.resid = resid + r;
+                t.target = static_cast<float>(requests[r].overlap);
+                t.cursor_floor = floor[r];
+            }
+        }
+        float2* rotation[3] = { nullptr, nullptr, nullptr };
+        for (std::size_t c = 0; c < copies; ++c) {
+            rotation[c] = staged_inter + c * batch_size * stride;
+        }
+        if ((status = run_stages256(work, rotation, stride))) {
+            return status;
+        }
+    }
+    else if (large) {
         // Pass A in batches of kPassABatch orientations, each batch followed by
         // the batch's B passes.
-        const std::size_t stride = static_cast<std::size_t>(L_[0]) * L_[1] * L_[2];
-        const std::size_t batch_size = std::min<std::size_t>(kPassABatch, runnable.size());
         auto* inter = static_cast<float2*>(
             device_buffer(ctx_, "pipe.inter_batch", batch_size * stride * sizeof(float2), status));
         if (!inter) {

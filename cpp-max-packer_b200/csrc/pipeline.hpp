@@ -168,6 +168,21 @@ private:
     int run_a256_batch(const KernelSlot* const* slots, int count, float2* const* inter);
     // Passes B1 and B2 (mode 0) of the same batch, one launch each.
     int run_b256_batch(const KernelSlot* const* slots, int count, float2* const* inter, const PassBSlot* outputs);
+    // The launch arguments of a batched pass A; returns its algorithmic bytes.
+    double fill_a256(const KernelSlot* const* slots, int count, float2* const* inter, PassABatch& batch) const;
+    // The launch arguments of batched passes B1 and B2: block counts and
+    // algorithmic bytes of each.
+    void fill_b256(const KernelSlot* const* slots, int count, float2* const* inter, const PassBSlot* outputs,
+                   PassBBatch& b1, PassBBatch& b2, int& blocks1, int& blocks2, double& bytes1, double& bytes2) const;
+    // Ordinary pages' passes A, B1 and B2 over `count` batches as a software
+    // pipeline: launch k runs pass A of batch k, B1 of batch k - 1 and B2 of
+    // batch k - 2 (pass_stage256_kernel).  Batch k uses inter[k % 3].
+    struct StageBatch {
+        const KernelSlot* slots[kPassABatch];
+        PassBSlot outputs[kPassABatch];
+        int count;
+    };
+    int run_stages256(const std::vector<StageBatch>& batches, float2* const* inter, std::size_t stride);
     double score(const KernelSlot& s, const std::int64_t* t, double p) const;
     double approx_epsilon(const KernelSlot& s) const;
 
@@ -186,6 +201,7 @@ private:
     float2* inter_ {};
     std::size_t inter_bytes_ {};
     bool fused_b_ {};  // 256^3: passes B1 and B2 as one cluster kernel (SPK_PASS_B=fused), else two passes
+    bool staged_ {};  // 256^3 ordinary pages: pipelined stage launches (SPK_PAGE_SCHEDULE=staged), else one per pass
     const double* table_ {};
     double z_norm_ {};  // sqrt(sum over cells of b^2 + p^2)
     const double* norm_host_ {};  // pinned partial sums of the last update_spectrum

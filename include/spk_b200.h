@@ -109,7 +109,10 @@ uint64_t spk_context_launches(const spk_context* context);
 void* spk_context_stream(const spk_context* context);
 /* Per-pass device timing of the page pipeline (CUDA events around each pass
  * launch when enabled): fills up to `capacity` entries of {launches, total_ms}
- * for passes 0 spectrum-A, 1 inverse-y, 2 inverse-x+epilogue, 3 merge+exact. */
+ * for passes 0 spectrum-A, 1 inverse-y, 2 inverse-x+epilogue, 3 merge+exact,
+ * 4 the pipelined stage (pass A of one batch of orientations with B1 and B2
+ * of the two batches before it, in one launch; only under
+ * SPK_PAGE_SCHEDULE=staged). */
 int spk_context_set_profiling(spk_context* context, int enabled);
 int spk_context_pass_times(const spk_context* context, uint64_t* launches, double* total_ms, uint32_t capacity);
 /* Algorithmic HBM bytes of the profiled launches of each pass (pass 0: the
