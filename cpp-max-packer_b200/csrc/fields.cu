@@ -221,7 +221,23 @@ __global__ void __launch_bounds__(1024) face_offsets_kernel(long long* __restric
 // the faces' clipped cell-range sizes (outside faces count 0), so small faces
 // pack densely into warps instead of leaving most lanes of a per-face warp idle.
 // The pair count is offsets[faces], read on the device.
-__global__ void __launch_bounds__(128, 6) raster_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint,
+// The triangle-only part of each face's separating-axis test (face_sat),
+// once per face before the raster.
+__global__ void face_sat_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint, int faces,
+                                FaceSat* __restrict__ sats)
+{
+    const int face = blockIdx.x * blockDim.x + threadIdx.x;
+    if (face >= faces) {
+        return;
+    }
+    IVec3 tri[3];
+    for (int k = 0; k < 3; ++k) {
+        tri[k] = vint[tris[3 * face + k]];
+    }
+    face_sat(tri, sats[face]);
+}
+
+__global__ void __launch_bounds__(128, 6) raster_kernel(const FaceSat* __restrict__ sats,
                               const geo::FaceRange* __restrict__ ranges, const long long* __restrict__ offsets,
                               int faces, FieldWindow w, std::uint8_t* __restrict__ cells,
                               int* __restrict__ error)
@@ -257,11 +273,7 @@ __global__ void __launch_bounds__(128, 6) raster_kernel(const std::uint32_t* __r
             atomicOr(error, 1);
             continue;
         }
-        IVec3 tri[3];
-        for (int k = 0; k < 3; ++k) {
-            tri[k] = vint[tris[3 * face + k]];
-        }
-        if (!triangle_box_disjoint(tri, box)) {
+        if (!face_sat_disjoint(sats[face], box)) {
             cells[flat] = 2;
         }
     }
@@ -507,12 +519,14 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
     auto* h_vint = static_cast<IVec3*>(host_buffer(ctx, "field.vint", V * sizeof(IVec3), status));
     auto* d_ranges = static_cast<geo::FaceRange*>(device_buffer(ctx, "field.ranges", F * sizeof(geo::FaceRange), status));
     auto* d_offsets = static_cast<long long*>(device_buffer(ctx, "field.offsets", (F + 1) * sizeof(long long), status));
+    auto* d_sats = static_cast<FaceSat*>(device_buffer(ctx, "field.sats", F * sizeof(FaceSat), status));
     auto* d_parent = static_cast<int*>(device_buffer(ctx, "field.parent", n * sizeof(int), status));
     auto* d_rootv = static_cast<std::uint8_t*>(device_buffer(ctx, "field.rootv", n, status));
     auto* d_misc = static_cast<int*>(device_buffer(ctx, "field.misc", 64, status));
     const unsigned int root_capacity = 1u << 20;
     auto* d_roots = static_cast<int*>(device_buffer(ctx, "field.roots", root_capacity * 4ULL, status));
-    if (!d_tris || !d_vint || !h_vint || !d_ranges || !d_offsets || !d_parent || !d_rootv || !d_misc || !d_roots) {
+    if (!d_tris || !d_vint || !h_vint || !d_ranges || !d_offsets || !d_sats || !d_parent || !d_rootv || !d_misc ||
+        !d_roots) {
         return status;
     }
     if (!d_tris_kept) {
@@ -577,9 +591,11 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
         // 128-thread blocks, six to an SM: the SAT's dependent FP64 chains need
         // the resident warps more than the registers that spill (measured).
         // The pair count is on the device; a grid of four waves loops over it.
-        raster_kernel<<<148 * 6 * 4, 128, 0, st>>>(d_tris, d_vint, d_ranges, d_offsets, static_cast<int>(F), w,
-                                                  d_cells, d_misc);
-        ctx->launches += 3;
+        face_sat_kernel<<<static_cast<unsigned>((F + 127) / 128), 128, 0, st>>>(d_tris, d_vint, static_cast<int>(F),
+                                                                             d_sats);
+        raster_kernel<<<148 * 6 * 4, 128, 0, st>>>(d_sats, d_ranges, d_offsets, static_cast<int>(F), w, d_cells,
+                                                  d_misc);
+        ctx->launches += 4;
     }
     ccl_init_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, n);
     ccl_union_kernel<<<blocks_for(n, threads), threads, 0, st>>>(d_cells, d_parent, w.shape[0], w.shape[1],

@@ -285,6 +285,88 @@ SPK_HD bool triangle_box_disjoint(const IVec3* tri, const IVec3& box)
     return false;
 }
 
+// The parts of triangle_box_disjoint that depend on the triangle alone, for
+// rasterising one triangle against many cells: the triangle's bounds on the
+// three box axes, the ten remaining axes (normal, then edge e x unit axis a
+// for e, a = 0..2, the test order) and the triangle's projection on each.
+// face_sat_disjoint(f, box) with f from face_sat(tri, f) returns exactly
+// triangle_box_disjoint(tri, box): every value is the same expression
+// computed once instead of once per cell.
+struct FaceSat {
+    double lo[3], hi[3];
+    IVec3 axis[10];
+    double tp_low[10], tp_high[10];
+    unsigned int usable;  // bit i: axis i can separate (all three vertex projections valid)
+};
+
+SPK_HD void face_sat(const IVec3* tri, FaceSat& f)
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        double lo = tri[0].v[a].low, hi = tri[0].v[a].high;
+#pragma unroll
+        for (int k = 1; k < 3; ++k) {
+            lo = f_min(lo, tri[k].v[a].low);
+            hi = f_max(hi, tri[k].v[a].high);
+        }
+        f.lo[a] = lo;
+        f.hi[a] = hi;
+    }
+    const IVec3 first = ivec_sub(tri[1], tri[0]);
+    const IVec3 second = ivec_sub(tri[2], tri[0]);
+    f.axis[0] = ivec_cross(first, second);
+    const IVec3 edges[3] = { first, second, ivec_sub(tri[2], tri[1]) };
+    for (int e = 0; e < 3; ++e) {
+        for (int a = 0; a < 3; ++a) {
+            IVec3 unit = { { point_interval(0.0), point_interval(0.0), point_interval(0.0) } };
+            unit.v[a] = point_interval(1.0);
+            f.axis[1 + 3 * e + a] = ivec_cross(edges[e], unit);
+        }
+    }
+    f.usable = 0;
+    for (int i = 0; i < 10; ++i) {
+        // projection_separates' triangle side: false whenever a vertex
+        // projection is invalid, whatever the box.
+        Interval tp = ivec_dot(tri[0], f.axis[i]);
+        bool usable = tp.valid;
+        for (int k = 1; k < 3; ++k) {
+            const Interval p = ivec_dot(tri[k], f.axis[i]);
+            if (!p.valid) {
+                usable = false;
+                break;
+            }
+            tp.low = f_min(tp.low, p.low);
+            tp.high = f_max(tp.high, p.high);
+        }
+        f.tp_low[i] = tp.low;
+        f.tp_high[i] = tp.high;
+        if (usable) {
+            f.usable |= 1u << i;
+        }
+    }
+}
+
+SPK_HD bool face_sat_disjoint(const FaceSat& f, const IVec3& box)
+{
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (f.hi[a] < box.v[a].low || box.v[a].high < f.lo[a]) {
+            return true;
+        }
+    }
+#pragma unroll 1
+    for (int i = 0; i < 10; ++i) {
+        if (!((f.usable >> i) & 1u)) {
+            continue;
+        }
+        const Interval bp = ivec_dot(box, f.axis[i]);
+        if (bp.valid && (f.tp_high[i] < bp.low || bp.high < f.tp_low[i])) {
+            return true;
+        }
+    }
+    return false;
+}
+
 // Outward enclosure of the closed cell `index` on the lattice; false when an
 // index is not exactly representable (|index| >= 2^53) or arithmetic overflows.
 SPK_HD bool grid_cell_interval(const double* origin, double pitch, const std::int64_t* index, IVec3& out)
