@@ -222,19 +222,27 @@ __global__ void __launch_bounds__(1024) face_offsets_kernel(long long* __restric
 // pack densely into warps instead of leaving most lanes of a per-face warp idle.
 // The pair count is offsets[faces], read on the device.
 // The triangle-only part of each face's separating-axis test (face_sat),
-// once per face before the raster.
+// once per face before the raster: 16 threads per face, thread i < 10
+// computing axis i and thread 10 the box-axis bounds.
 __global__ void face_sat_kernel(const std::uint32_t* __restrict__ tris, const IVec3* __restrict__ vint, int faces,
                                 FaceSat* __restrict__ sats)
 {
-    const int face = blockIdx.x * blockDim.x + threadIdx.x;
-    if (face >= faces) {
+    const long long thread = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long long face = thread >> 4;
+    const int i = static_cast<int>(thread & 15);
+    if (face >= faces || i > 10) {
         return;
     }
     IVec3 tri[3];
     for (int k = 0; k < 3; ++k) {
         tri[k] = vint[tris[3 * face + k]];
     }
-    face_sat(tri, sats[face]);
+    if (i == 10) {
+        face_sat_bounds(tri, sats[face]);
+    }
+    else {
+        face_sat_axis(tri, i, sats[face]);
+    }
 }
 
 __global__ void __launch_bounds__(128, 6) raster_kernel(const FaceSat* __restrict__ sats,
@@ -591,8 +599,8 @@ int raster_fill_impl(spk_context* ctx, const geo::Placed& placed, const FieldWin
         // 128-thread blocks, six to an SM: the SAT's dependent FP64 chains need
         // the resident warps more than the registers that spill (measured).
         // The pair count is on the device; a grid of four waves loops over it.
-        face_sat_kernel<<<static_cast<unsigned>((F + 127) / 128), 128, 0, st>>>(d_tris, d_vint, static_cast<int>(F),
-                                                                             d_sats);
+        face_sat_kernel<<<static_cast<unsigned>((16 * F + 127) / 128), 128, 0, st>>>(d_tris, d_vint,
+                                                                                  static_cast<int>(F), d_sats);
         raster_kernel<<<148 * 6 * 4, 128, 0, st>>>(d_sats, d_ranges, d_offsets, static_cast<int>(F), w, d_cells,
                                                   d_misc);
         ctx->launches += 4;

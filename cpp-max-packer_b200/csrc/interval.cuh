@@ -296,10 +296,11 @@ struct FaceSat {
     double lo[3], hi[3];
     IVec3 axis[10];
     double tp_low[10], tp_high[10];
-    unsigned int usable;  // bit i: axis i can separate (all three vertex projections valid)
+    unsigned char usable[10];  // axis i can separate (all three vertex projections valid)
 };
 
-SPK_HD void face_sat(const IVec3* tri, FaceSat& f)
+// FaceSat's box-axis bounds.
+SPK_HD void face_sat_bounds(const IVec3* tri, FaceSat& f)
 {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -312,37 +313,50 @@ SPK_HD void face_sat(const IVec3* tri, FaceSat& f)
         f.lo[a] = lo;
         f.hi[a] = hi;
     }
-    const IVec3 first = ivec_sub(tri[1], tri[0]);
-    const IVec3 second = ivec_sub(tri[2], tri[0]);
-    f.axis[0] = ivec_cross(first, second);
-    const IVec3 edges[3] = { first, second, ivec_sub(tri[2], tri[1]) };
-    for (int e = 0; e < 3; ++e) {
-        for (int a = 0; a < 3; ++a) {
-            IVec3 unit = { { point_interval(0.0), point_interval(0.0), point_interval(0.0) } };
-            unit.v[a] = point_interval(1.0);
-            f.axis[1 + 3 * e + a] = ivec_cross(edges[e], unit);
-        }
+}
+
+// FaceSat's axis i (0: the normal first x second; 1 + 3 e + a: edge e x
+// unit axis a, with edges first = v1 - v0, second = v2 - v0, v2 - v1) and the
+// triangle's projection on it.  Each axis is independent of the others, so a
+// device launch gives each its own thread.
+SPK_HD void face_sat_axis(const IVec3* tri, int i, FaceSat& f)
+{
+    IVec3 axis;
+    if (i == 0) {
+        axis = ivec_cross(ivec_sub(tri[1], tri[0]), ivec_sub(tri[2], tri[0]));
     }
-    f.usable = 0;
+    else {
+        const int e = (i - 1) / 3, a = (i - 1) % 3;
+        const IVec3 edge = e == 0 ? ivec_sub(tri[1], tri[0]) : e == 1 ? ivec_sub(tri[2], tri[0])
+                                                                       : ivec_sub(tri[2], tri[1]);
+        IVec3 unit = { { point_interval(0.0), point_interval(0.0), point_interval(0.0) } };
+        unit.v[a] = point_interval(1.0);
+        axis = ivec_cross(edge, unit);
+    }
+    f.axis[i] = axis;
+    // projection_separates' triangle side: false whenever a vertex
+    // projection is invalid, whatever the box.
+    Interval tp = ivec_dot(tri[0], axis);
+    bool usable = tp.valid;
+    for (int k = 1; k < 3 && usable; ++k) {
+        const Interval p = ivec_dot(tri[k], axis);
+        if (!p.valid) {
+            usable = false;
+            break;
+        }
+        tp.low = f_min(tp.low, p.low);
+        tp.high = f_max(tp.high, p.high);
+    }
+    f.tp_low[i] = tp.low;
+    f.tp_high[i] = tp.high;
+    f.usable[i] = usable ? 1 : 0;
+}
+
+SPK_HD void face_sat(const IVec3* tri, FaceSat& f)
+{
+    face_sat_bounds(tri, f);
     for (int i = 0; i < 10; ++i) {
-        // projection_separates' triangle side: false whenever a vertex
-        // projection is invalid, whatever the box.
-        Interval tp = ivec_dot(tri[0], f.axis[i]);
-        bool usable = tp.valid;
-        for (int k = 1; k < 3; ++k) {
-            const Interval p = ivec_dot(tri[k], f.axis[i]);
-            if (!p.valid) {
-                usable = false;
-                break;
-            }
-            tp.low = f_min(tp.low, p.low);
-            tp.high = f_max(tp.high, p.high);
-        }
-        f.tp_low[i] = tp.low;
-        f.tp_high[i] = tp.high;
-        if (usable) {
-            f.usable |= 1u << i;
-        }
+        face_sat_axis(tri, i, f);
     }
 }
 
@@ -356,7 +370,7 @@ SPK_HD bool face_sat_disjoint(const FaceSat& f, const IVec3& box)
     }
 #pragma unroll 1
     for (int i = 0; i < 10; ++i) {
-        if (!((f.usable >> i) & 1u)) {
+        if (!f.usable[i]) {
             continue;
         }
         const Interval bp = ivec_dot(box, f.axis[i]);
