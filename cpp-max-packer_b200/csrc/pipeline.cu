@@ -613,6 +613,19 @@ __device__ __forceinline__ int batch_slot(const PassBBatch& b, unsigned int bloc
     return g;
 }
 
+// The slot of block `block` of a batch and the block's index within it
+// (PassBBatch's block order).
+__device__ __forceinline__ int batch_block(const PassBBatch& b, unsigned int block, unsigned int& local)
+{
+    if (block < static_cast<unsigned int>(b.interleaved)) {
+        local = block / static_cast<unsigned int>(b.count);
+        return static_cast<int>(block % static_cast<unsigned int>(b.count));
+    }
+    const int g = batch_slot(b, block);
+    local = static_cast<unsigned int>(b.min_blocks) + block - static_cast<unsigned int>(b.slot[g].first_block);
+    return g;
+}
+
 __global__ void __launch_bounds__(256) pass_b1_256_batch_kernel(const __grid_constant__ PassBBatch b,
                                                                const float2* __restrict__ twiddles)
 {
@@ -1145,10 +1158,10 @@ __global__ void __launch_bounds__(256) pass_b2_256_batch_kernel(const __grid_con
     __shared__ B2Shared sh;
     load_twiddles(tw, twiddles);
     __syncthreads();
-    const PassBSlot& s = b.slot[batch_slot(b, blockIdx.x)];
+    unsigned int local = 0;
+    const PassBSlot& s = b.slot[batch_block(b, blockIdx.x, local)];
     b2_block256(s.inter, s.legal_x, s.legal_y, s.legal_z, tw, lines, sh, s.t65, s.inv_occ, 0, s.target, 0.0,
-                s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid,
-                blockIdx.x - static_cast<unsigned int>(s.first_block));
+                s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid, local);
 }
 
 // One stage of the software-pipelined page passes on 256^3 grids: pass A of
@@ -1198,11 +1211,10 @@ __global__ void __launch_bounds__(256, 3) pass_stage256_kernel(const __grid_cons
         b1_block256(s.inter, s.legal_y, tw, lines, block - static_cast<unsigned int>(s.first_block));
         return;
     }
-    const unsigned int block = static_cast<unsigned int>(q - b1_before);
-    const PassBSlot& s = p.b2.slot[batch_slot(p.b2, block)];
+    unsigned int local = 0;
+    const PassBSlot& s = p.b2.slot[batch_block(p.b2, static_cast<unsigned int>(q - b1_before), local)];
     b2_block256(s.inter, s.legal_x, s.legal_y, s.legal_z, tw, lines, *reinterpret_cast<B2Shared*>(stage_smem), s.t65,
-                s.inv_occ, 0, s.target, 0.0, s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid,
-                block - static_cast<unsigned int>(s.first_block));
+                s.inv_occ, 0, s.target, 0.0, s.cursor_floor, s.keys, s.count, s.cap, s.tau, s.resid, local);
 }
 static_assert(sizeof(B2Shared) <= kPassASmem, "pass B2's shared state must fit the stage kernel's dynamic buffer");
 
@@ -2043,13 +2055,29 @@ void Pipeline::fill_b256(const KernelSlot* const* slots, int count, float2* cons
         slot.first_block = blocks1;
         b1.slot[g] = slot;
         blocks1 += 16 * s.legal[2];
-        slot.first_block = blocks2;
         b2.slot[g] = slot;
         const long long rows = static_cast<long long>(s.legal[1]) * s.legal[2];
         blocks2 += static_cast<int>((rows + 15) / 16);
         const double legal_rows = static_cast<double>(rows);
         bytes1 += 8.0 * L_[0] * L_[1] * s.legal[2] + 8.0 * L_[0] * legal_rows;
         bytes2 += 8.0 * L_[0] * legal_rows;
+    }
+    // Pass B2 visits the orientations round-robin: each orientation's
+    // pruning bound (tau) is lowered by its first blocks to finish, and
+    // slot-by-slot order would start every orientation with a full wave of
+    // blocks that run before any bound exists.
+    int min_blocks = count ? 1 << 30 : 0;
+    for (int g = 0; g < count; ++g) {
+        const long long rows = static_cast<long long>(slots[g]->legal[1]) * slots[g]->legal[2];
+        min_blocks = std::min(min_blocks, static_cast<int>((rows + 15) / 16));
+    }
+    b2.min_blocks = min_blocks;
+    b2.interleaved = count * min_blocks;
+    int first = b2.interleaved;
+    for (int g = 0; g < count; ++g) {
+        const long long rows = static_cast<long long>(slots[g]->legal[1]) * slots[g]->legal[2];
+        b2.slot[g].first_block = first;
+        first += static_cast<int>((rows + 15) / 16) - min_blocks;
     }
 }
 

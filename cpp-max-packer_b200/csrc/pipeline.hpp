@@ -81,9 +81,16 @@ struct PassBSlot {
     int legal_x, legal_y, legal_z;
     int first_block;
 };
+// Block order: the first `interleaved` blocks go round-robin over the
+// slots (block b: slot b % count, the slot's block b / count), covering the
+// first `min_blocks` blocks of every slot; the rest follow slot by slot from
+// each slot's first_block, as its blocks min_blocks and up.  With
+// interleaved = min_blocks = 0 the order is slot by slot.
 struct PassBBatch {
     PassBSlot slot[kPassABatch];
     int count;
+    int interleaved;
+    int min_blocks;
 };
 
 struct PageRequest {
