@@ -97,6 +97,7 @@ def _declare(h):
                                             ctypes.POINTER(CorrelationResultC)]
     h.spk_build_proximity.argtypes = [P, P, P, P]
     h.spk_build_proximity_static.argtypes = [P, P, P, P]
+    h.spk_check_bounded_wait.argtypes = [P, ctypes.c_uint32]
 
 
 def status_code(status: int) -> str:

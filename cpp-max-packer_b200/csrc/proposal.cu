@@ -1152,6 +1152,26 @@ int pack_all(spk_context* ctx, ProposalNet* net)
     return cudaGetLastError() == cudaSuccess ? kOk : kCuda;
 }
 
+// The bounded wait's expiry path on its own: one CTA initialises an
+// mbarrier that expects one arrival, which never comes, and waits on it with
+// bar_wait for `spins` polls.  The expired wait sets *error; the barrier is
+// invalidated before the CTA exits.
+__global__ void bounded_wait_check_kernel(std::uint32_t spins, unsigned* __restrict__ error)
+{
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        umma::bar_init(&bar, 1);
+        umma::bar_init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (!umma::bar_wait(&bar, 0, spins)) {
+            atomicOr(error, 1u);
+        }
+        asm volatile("mbarrier.inval.shared::cta.b64 [%0];" : : "r"(umma::smem_addr(&bar)) : "memory");
+    }
+}
+
 int check_error(spk_context* ctx, ProposalNet* net)
 {
     unsigned err = 0;
@@ -1523,6 +1543,31 @@ ProposalNet* net_of(spk_proposal* p) { return p ? &p->net : nullptr; }
 extern "C" {
 
 uint64_t spk_proposal_parameter_count(void) { return spk::proposal_parameter_count(); }
+
+int spk_check_bounded_wait(spk_context* ctx, uint32_t spins)
+{
+    if (!ctx) {
+        return spk::kNotReady;
+    }
+    if (spins == 0 || spins > (1u << 22)) {
+        return spk::kInvalidArgument;
+    }
+    int status = spk::kOk;
+    auto* error = static_cast<unsigned*>(spk::device_buffer(ctx, "wait.check", sizeof(unsigned), status));
+    if (!error) {
+        return status;
+    }
+    unsigned host = 0;
+    cudaMemsetAsync(error, 0, sizeof(unsigned), ctx->stream);
+    spk::bounded_wait_check_kernel<<<1, 32, 0, ctx->stream>>>(spins, error);
+    ctx->launches++;
+    if (cudaMemcpyAsync(&host, error, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return spk::kCuda;
+    }
+    return host ? spk::fail(ctx, spk::kKernelWait, "A bounded device wait expired.") : spk::kOk;
+}
 
 int spk_proposal_create(spk_context* ctx, uint64_t seed, spk_proposal** out)
 {

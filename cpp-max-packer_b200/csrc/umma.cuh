@@ -108,9 +108,10 @@ __device__ __forceinline__ bool bar_try_wait(unsigned long long* bar, std::uint3
 
 // Bounded wait for the phase with `parity` to complete; false when the limit
 // ran out (the caller records an error and carries on without hanging).
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, std::uint32_t parity)
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, std::uint32_t parity,
+                                         std::uint32_t limit = 1u << 22)
 {
-    for (std::uint32_t spin = 0; spin < (1u << 22); ++spin) {
+    for (std::uint32_t spin = 0; spin < limit; ++spin) {
         if (bar_try_wait(bar, parity)) {
             return true;
         }

@@ -463,6 +463,13 @@ typedef struct spk_proposal_dataset {
     uint64_t sample_count;
 } spk_proposal_dataset;
 
+/* The expiry path of the library's bounded device waits (the tcgen05
+ * convolutions' mbarrier waits), on its own: one CTA waits `spins` polls
+ * (1 .. 2^22) on an mbarrier that nothing arrives at.  Returns
+ * SPK_DEVICE_WAIT_LIMIT, the status those kernels report when a wait runs
+ * out; the context stays usable.  For tests of the error path. */
+int spk_check_bounded_wait(spk_context* context, uint32_t spins);
+
 uint64_t spk_proposal_parameter_count(void);
 /* He-initialised parameters from `seed`. */
 int spk_proposal_create(spk_context* context, uint64_t seed, spk_proposal** out);
