@@ -173,9 +173,19 @@ __device__ __forceinline__ void fft256(float2 (&v)[16], float2* line, int t, con
 __device__ __forceinline__ void fft256_first32(float2 a, float2 b, float2 (&v)[16], float2* line, int t,
                                                const RegTwiddles& tw)
 {
+    // w16^k1 = w256^(16 k1) as immediates (the table's values: FP32 roundings
+    // of cos and sin at multiples of pi/8, exact at the quarter points).
+    constexpr float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    constexpr float r2 = 0.70710678118654752440f;
+    const float2 w16[16] = { make_float2(1.f, 0.f),  make_float2(c1, -s1),  make_float2(r2, -r2),
+                             make_float2(s1, -c1),   make_float2(0.f, -1.f), make_float2(-s1, -c1),
+                             make_float2(-r2, -r2),  make_float2(-c1, -s1), make_float2(-1.f, 0.f),
+                             make_float2(-c1, s1),   make_float2(-r2, r2),  make_float2(-s1, c1),
+                             make_float2(0.f, 1.f),  make_float2(s1, c1),   make_float2(r2, r2),
+                             make_float2(c1, s1) };
 #pragma unroll
     for (int k1 = 0; k1 < 16; ++k1) {
-        const float2 w = tw.root[16 * k1];  // w16^k1 = w256^(16 k1)
+        const float2 w = w16[k1];
         v[k1] = make_float2(a.x + b.x * w.x - b.y * w.y, a.y + b.x * w.y + b.y * w.x);
     }
     twiddle_row<false>(v, tw, t);
