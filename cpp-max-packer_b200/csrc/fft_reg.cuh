@@ -20,12 +20,12 @@ namespace spk {
 constexpr int kRegLine = 273;  // shared complex slots per line (16 x 17 + 1: bank spread)
 constexpr int kTwRow = 18;     // complex slots per twiddle row (16 + 2: bank spread of 16-byte reads)
 
-// Shared twiddles of the register FFT: the 256 roots w256^m and, for each
-// lane-in-line t, the row w256^(t k) for k < 16.  A thread reads its row
-// two roots at a time (16-byte loads); with rows 144 bytes apart, the eight
-// threads of a quarter warp that hold different t read distinct banks.
+// Shared twiddles of the register FFT: for each lane-in-line t, the row
+// w256^(t k) for k < 16 (the 16-point DFTs' own roots are immediates).  A
+// thread reads its row two roots at a time (16-byte loads); with rows 144
+// bytes apart, the eight threads of a quarter warp that hold different t
+// read distinct banks.
 struct RegTwiddles {
-    float2 root[256];
     __align__(16) float2 row[16 * kTwRow];
 };
 
@@ -34,7 +34,6 @@ struct RegTwiddles {
 __device__ __forceinline__ void load_twiddles(RegTwiddles& tw, const float2* __restrict__ twiddles)
 {
     const int i = threadIdx.x, t = i >> 4, k = i & 15;
-    tw.root[i] = twiddles[i];
     tw.row[t * kTwRow + k] = twiddles[(t * k) & 255];
 }
 
